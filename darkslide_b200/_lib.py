@@ -1,0 +1,180 @@
+"""ctypes binding of libdsgpu.so (the C ABI in include/dsgpu.h).
+
+The library is built in-tree (``python -m darkslide_b200.build``). There is no
+CPU fallback: if the library or a CUDA device is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdsgpu.so")
+
+DSGPU_OK = 0
+DSGPU_ERR_ARG = -1
+DSGPU_ERR_CFA = -2
+DSGPU_ERR_SIZE = -3
+DSGPU_ERR_NOMEM = -4
+DSGPU_ERR_CUDA = -5
+DSGPU_ERR_NODEV = -6
+DSGPU_ERR_TIMEOUT = -7
+DSGPU_ERR_UNSUPPORTED = -8
+DSGPU_HOST = 1
+DSGPU_ASYNC = 2
+DSGPU_QUALITY_DRAFT = 0
+DSGPU_QUALITY_FULL = 1
+DSGPU_STAGE_DEMOSAIC = 0
+DSGPU_STAGE_NLM = 1
+DSGPU_STAGE_COPY = 2
+
+# every symbol include/dsgpu.h and include/dsgpu_scene.h declare
+EXPORTS = [
+    "dsgpu_strerror", "dsgpu_abi_version", "dsgpu_create", "dsgpu_destroy", "dsgpu_set_stream",
+    "dsgpu_get_stream", "dsgpu_synchronize", "dsgpu_trim", "dsgpu_last_error", "dsgpu_normalize_u16",
+    "dsgpu_clip_plane", "dsgpu_mhc", "dsgpu_rcd", "dsgpu_demosaic", "dsgpu_box_blur", "dsgpu_nlm",
+    "dsgpu_develop_u16", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
+    "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render",
+]
+
+
+class DsgpuError(RuntimeError):
+    def __init__(self, status: int, where: str = "", detail: str = ""):
+        self.status = status
+        msg = f"{where}: {strerror(status)} ({status})"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint64),
+        ("w", ctypes.c_int),
+        ("h", ctypes.c_int),
+        ("cfa", ctypes.c_uint8 * 4),
+        ("black", ctypes.c_int),
+        ("white", ctypes.c_int),
+        ("gain_e_per_dn", ctypes.c_float),
+        ("read_sigma_dn", ctypes.c_float),
+    ]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m darkslide_b200.build`")
+            L = ctypes.CDLL(LIB_PATH)
+            vp, i, f, u, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_uint, ctypes.c_size_t
+            L.dsgpu_strerror.restype = ctypes.c_char_p
+            L.dsgpu_strerror.argtypes = [i]
+            L.dsgpu_abi_version.restype = i
+            L.dsgpu_create.argtypes = [i, ctypes.POINTER(vp)]
+            L.dsgpu_destroy.argtypes = [vp]
+            L.dsgpu_set_stream.argtypes = [vp, vp]
+            L.dsgpu_get_stream.argtypes = [vp]
+            L.dsgpu_get_stream.restype = vp
+            L.dsgpu_synchronize.argtypes = [vp]
+            L.dsgpu_trim.argtypes = [vp]
+            L.dsgpu_last_error.argtypes = [vp]
+            L.dsgpu_last_error.restype = ctypes.c_char_p
+            L.dsgpu_normalize_u16.argtypes = [vp, vp, i, i, sz, vp, f, vp, vp, u]
+            L.dsgpu_clip_plane.argtypes = [vp, vp, i, i, vp, u]
+            L.dsgpu_mhc.argtypes = [vp, vp, i, i, vp, vp, vp, u]
+            L.dsgpu_rcd.argtypes = [vp, vp, i, i, vp, vp, vp, u]
+            L.dsgpu_demosaic.argtypes = [vp, vp, i, i, vp, vp, i, vp, vp, u]
+            L.dsgpu_box_blur.argtypes = [vp, vp, i, i, i, vp, u]
+            L.dsgpu_nlm.argtypes = [vp, vp, i, i, i, f, i, i, vp, u]
+            L.dsgpu_develop_u16.argtypes = [vp, vp, i, i, sz, vp, f, vp, vp, f, i, i, vp, vp, u]
+            L.dsgpu_profile.argtypes = [vp, i]
+            L.dsgpu_stage_ms.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i)]
+            L.dsgpu_launch_count.argtypes = [vp]
+            L.dsgpu_measure_peaks.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+            L.dsgpu_scene_render_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
+            L.dsgpu_scene_truth_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
+            L.dsgpu_scene_render.argtypes = [vp, ctypes.POINTER(SceneDesc), vp, u]
+            for name in EXPORTS:
+                if name not in ("dsgpu_strerror", "dsgpu_get_stream", "dsgpu_last_error", "dsgpu_launch_count"):
+                    getattr(L, name).restype = i
+            L.dsgpu_launch_count.restype = ctypes.c_ulonglong
+            _lib = L
+    return _lib
+
+
+def strerror(status: int) -> str:
+    return lib().dsgpu_strerror(int(status)).decode()
+
+
+class Context:
+    """One dsgpu context: a device, a stream and cached scratch (dsgpu_create)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        st = lib().dsgpu_create(int(device), ctypes.byref(h))
+        if st != DSGPU_OK:
+            raise DsgpuError(st, "dsgpu_create")
+        self.handle = h
+        self.device = int(device)
+
+    def check(self, status: int, where: str) -> None:
+        if status != DSGPU_OK:
+            detail = lib().dsgpu_last_error(self.handle)
+            raise DsgpuError(status, where, detail.decode() if detail else "")
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self.check(lib().dsgpu_set_stream(self.handle, ctypes.c_void_p(stream_ptr or 0)), "dsgpu_set_stream")
+
+    def synchronize(self) -> None:
+        self.check(lib().dsgpu_synchronize(self.handle), "dsgpu_synchronize")
+
+    def profile(self, enable: bool) -> None:
+        self.check(lib().dsgpu_profile(self.handle, int(bool(enable))), "dsgpu_profile")
+
+    def stage_ms(self, stage: int) -> tuple[float, int]:
+        t, n = ctypes.c_double(), ctypes.c_int()
+        self.check(lib().dsgpu_stage_ms(self.handle, int(stage), ctypes.byref(t), ctypes.byref(n)), "dsgpu_stage_ms")
+        return t.value, n.value
+
+    def launch_count(self) -> int:
+        return int(lib().dsgpu_launch_count(self.handle))
+
+    def measure_peaks(self) -> tuple[float, float]:
+        f, e = ctypes.c_double(), ctypes.c_double()
+        self.check(lib().dsgpu_measure_peaks(self.handle, ctypes.byref(f), ctypes.byref(e)), "dsgpu_measure_peaks")
+        return f.value, e.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and _lib is not None:
+            lib().dsgpu_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+_default: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    ctx = _default.get(device)
+    if ctx is None:
+        ctx = _default[device] = Context(device)
+    return ctx

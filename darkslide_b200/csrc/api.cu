@@ -1,0 +1,561 @@
+// C ABI of libdsgpu: argument checks, context, scratch and host staging,
+// and dispatch to the kernels. See include/dsgpu.h for the contract.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "internal.cuh"
+#include "scene.h"
+#include "../../include/dsgpu_scene.h"
+
+ds_scene ds_scene_make(const dsgpu_scene_desc* d);
+cudaError_t ds_launch_scene(cudaStream_t st, const ds_scene& s, uint16_t* out);
+void ds_scene_host(const ds_scene& s, int x0, int y0, int cw, int ch, uint16_t* out);
+void ds_scene_truth(const ds_scene& s, int x0, int y0, int cw, int ch, float* out);
+cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s);
+
+namespace {
+
+enum Slot { S_IN = 0, S_OUT, S_OUT2, S_CFA, S_RGB, S_TMP, S_COUNT };
+
+}  // namespace
+
+struct ds_mark {
+  int stage;
+  cudaEvent_t a, b;
+};
+
+struct dsgpu_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  void* slot[S_COUNT] = {};
+  size_t slot_bytes[S_COUNT] = {};
+  char last_error[256] = {};
+  unsigned long long launches = 0;  // kernels this context has launched
+  bool profiling = false;
+  std::vector<ds_mark> marks;       // stage events recorded while profiling
+  std::vector<cudaEvent_t> pool;    // idle events
+};
+
+namespace {
+
+// Makes ctx->device current for the duration of a call and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+int map_cuda(dsgpu_ctx* ctx, cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return DSGPU_OK;
+  if (ctx) snprintf(ctx->last_error, sizeof(ctx->last_error), "%s: %s", where, cudaGetErrorString(e));
+  cudaGetLastError();  // clear a non-sticky error
+  return e == cudaErrorMemoryAllocation ? DSGPU_ERR_NOMEM : DSGPU_ERR_CUDA;
+}
+
+#define DS_TRY(expr)                                 \
+  do {                                               \
+    cudaError_t _e = (expr);                         \
+    if (_e != cudaSuccess) return map_cuda(ctx, _e, #expr); \
+  } while (0)
+
+#define DS_CHECK(expr)          \
+  do {                          \
+    int _s = (expr);            \
+    if (_s != DSGPU_OK) return _s; \
+  } while (0)
+
+// grow-only device scratch
+int scratch(dsgpu_ctx* ctx, Slot s, size_t bytes, void** out) {
+  if (bytes == 0) bytes = 16;
+  if (ctx->slot_bytes[s] < bytes) {
+    if (ctx->slot[s]) cudaFreeAsync(ctx->slot[s], ctx->stream);
+    ctx->slot[s] = nullptr;
+    ctx->slot_bytes[s] = 0;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+    if (e != cudaSuccess) return map_cuda(ctx, e, "cudaMallocAsync");
+    ctx->slot[s] = p;
+    ctx->slot_bytes[s] = bytes;
+  }
+  *out = ctx->slot[s];
+  return DSGPU_OK;
+}
+
+// Stage timing (the analogue of the reference's Lap stage timer,
+// pipeline/mod.rs:106-137): with profiling on, each stage of a call is
+// bracketed by CUDA events on the context stream.
+cudaEvent_t take_event(dsgpu_ctx* ctx) {
+  cudaEvent_t e = nullptr;
+  if (!ctx->pool.empty()) {
+    e = ctx->pool.back();
+    ctx->pool.pop_back();
+  } else if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return e;
+}
+
+struct StageMark {
+  dsgpu_ctx* ctx;
+  int stage;
+  cudaEvent_t a = nullptr;
+  StageMark(dsgpu_ctx* c, int st) : ctx(c), stage(st) {
+    if (ctx->profiling && (a = take_event(ctx))) cudaEventRecord(a, ctx->stream);
+  }
+  ~StageMark() {
+    if (!a) return;
+    cudaEvent_t b = take_event(ctx);
+    if (!b) {
+      ctx->pool.push_back(a);
+      return;
+    }
+    cudaEventRecord(b, ctx->stream);
+    ctx->marks.push_back({stage, a, b});
+  }
+};
+
+int check_dims(int w, int h) {
+  if (w < 0 || h < 0) return DSGPU_ERR_ARG;
+  if (w > DSGPU_MAX_DIM || h > DSGPU_MAX_DIM) return DSGPU_ERR_SIZE;
+  return DSGPU_OK;
+}
+
+int check_pat(const uint8_t* cfa, ds_pat* pat) {
+  if (!cfa) return DSGPU_ERR_ARG;
+  pat->packed = 0;
+  for (int i = 0; i < 4; i++) {
+    if (cfa[i] > 2) return DSGPU_ERR_CFA;
+    pat->packed |= (uint32_t)cfa[i] << (8 * i);
+  }
+  return DSGPU_OK;
+}
+
+// Input staging: with DSGPU_HOST, copy host data into a scratch slot and
+// return the device pointer; otherwise the pointer is used as is.
+int stage_in(dsgpu_ctx* ctx, unsigned flags, Slot s, const void* p, size_t bytes, const void** dev) {
+  if (!(flags & DSGPU_HOST)) {
+    *dev = p;
+    return DSGPU_OK;
+  }
+  void* d = nullptr;
+  DS_CHECK(scratch(ctx, s, bytes, &d));
+  StageMark mark(ctx, DSGPU_STAGE_COPY);
+  if (bytes) DS_TRY(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  *dev = d;
+  return DSGPU_OK;
+}
+
+int stage_out_ptr(dsgpu_ctx* ctx, unsigned flags, Slot s, void* p, size_t bytes, void** dev) {
+  if (!(flags & DSGPU_HOST)) {
+    *dev = p;
+    return DSGPU_OK;
+  }
+  return scratch(ctx, s, bytes, dev);
+}
+
+int finish(dsgpu_ctx* ctx, unsigned flags, void* host_dst, const void* dev_src, size_t bytes, void* host_dst2 = nullptr,
+           const void* dev_src2 = nullptr, size_t bytes2 = 0) {
+  if (flags & DSGPU_HOST) {
+    StageMark mark(ctx, DSGPU_STAGE_COPY);
+    if (host_dst && bytes) DS_TRY(cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    if (host_dst2 && bytes2) DS_TRY(cudaMemcpyAsync(host_dst2, dev_src2, bytes2, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (flags & DSGPU_HOST) {
+    DS_TRY(cudaStreamSynchronize(ctx->stream));
+  } else if (!(flags & DSGPU_ASYNC)) {
+    DS_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  return DSGPU_OK;
+}
+
+int nlm_args_ok(int channels, int search, int patch) {
+  if (channels < 1 || channels > 4) return DSGPU_ERR_ARG;
+  if (patch < 0 || patch > DSGPU_NLM_MAX_PATCH) return DSGPU_ERR_ARG;
+  if (search > DSGPU_NLM_MAX_SEARCH) return DSGPU_ERR_ARG;
+  return DSGPU_OK;
+}
+
+// NLM on device buffers; a negative search radius yields an empty offset set
+// and therefore 0 / max(0, 1e-12) = 0 (enhance.rs:41, :71).
+int run_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h_param, int search, int patch,
+            float* out) {
+  const size_t n = (size_t)w * h * channels;
+  if (n == 0) return DSGPU_OK;
+  StageMark mark(ctx, DSGPU_STAGE_NLM);
+  if (search < 0) {
+    DS_TRY(cudaMemsetAsync(out, 0, n * sizeof(float), ctx->stream));
+    return DSGPU_OK;
+  }
+  DS_TRY(ds_launch_nlm(ctx->stream, in, w, h, channels, h_param, search, patch, out));
+  ctx->launches += 1;
+  return DSGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dsgpu_strerror(int status) {
+  switch (status) {
+    case DSGPU_OK: return "ok";
+    case DSGPU_ERR_ARG: return "invalid argument";
+    case DSGPU_ERR_CFA: return "invalid CFA pattern";
+    case DSGPU_ERR_SIZE: return "image too large";
+    case DSGPU_ERR_NOMEM: return "out of memory";
+    case DSGPU_ERR_CUDA: return "CUDA error";
+    case DSGPU_ERR_NODEV: return "no usable sm_100 device";
+    case DSGPU_ERR_TIMEOUT: return "device wait timed out";
+    case DSGPU_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+int dsgpu_abi_version(void) { return DSGPU_ABI_VERSION; }
+
+int dsgpu_create(int device, dsgpu_ctx** out) {
+  if (!out) return DSGPU_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return DSGPU_ERR_NODEV;
+  }
+  if (device < 0 || device >= n) return DSGPU_ERR_ARG;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return DSGPU_ERR_NODEV;
+  DeviceGuard g(device);
+  if (!g.ok) return DSGPU_ERR_NODEV;
+  dsgpu_ctx* ctx = new (std::nothrow) dsgpu_ctx();
+  if (!ctx) return DSGPU_ERR_NOMEM;
+  ctx->device = device;
+  if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return DSGPU_ERR_CUDA;
+  }
+  ctx->stream = ctx->own;
+  *out = ctx;
+  return DSGPU_OK;
+}
+
+int dsgpu_destroy(dsgpu_ctx* ctx) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (int i = 0; i < S_COUNT; i++)
+    if (ctx->slot[i]) cudaFreeAsync(ctx->slot[i], ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& m : ctx->marks) {
+    cudaEventDestroy(m.a);
+    cudaEventDestroy(m.b);
+  }
+  for (auto e : ctx->pool) cudaEventDestroy(e);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+  return DSGPU_OK;
+}
+
+int dsgpu_set_stream(dsgpu_ctx* ctx, void* stream) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  return DSGPU_OK;
+}
+
+void* dsgpu_get_stream(dsgpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int dsgpu_synchronize(dsgpu_ctx* ctx) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  return DSGPU_OK;
+}
+
+int dsgpu_trim(dsgpu_ctx* ctx) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  for (int i = 0; i < S_COUNT; i++) {
+    if (ctx->slot[i]) cudaFreeAsync(ctx->slot[i], ctx->stream);
+    ctx->slot[i] = nullptr;
+    ctx->slot_bytes[i] = 0;
+  }
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  return DSGPU_OK;
+}
+
+const char* dsgpu_last_error(dsgpu_ctx* ctx) { return ctx ? ctx->last_error : "no context"; }
+
+unsigned long long dsgpu_launch_count(dsgpu_ctx* ctx) { return ctx ? ctx->launches : 0ull; }
+
+int dsgpu_profile(dsgpu_ctx* ctx, int enable) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  for (auto& m : ctx->marks) {
+    ctx->pool.push_back(m.a);
+    ctx->pool.push_back(m.b);
+  }
+  ctx->marks.clear();
+  ctx->profiling = enable != 0;
+  return DSGPU_OK;
+}
+
+int dsgpu_stage_ms(dsgpu_ctx* ctx, int stage, double* total_ms, int* count) {
+  if (!ctx || !total_ms) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  double t = 0.0;
+  int n = 0;
+  for (auto& m : ctx->marks) {
+    if (m.stage != stage) continue;
+    float ms = 0.f;
+    DS_TRY(cudaEventElapsedTime(&ms, m.a, m.b));
+    t += ms;
+    n++;
+  }
+  *total_ms = t;
+  if (count) *count = n;
+  return DSGPU_OK;
+}
+
+int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops, double* ex2_per_s) {
+  if (!ctx || !ffma_flops || !ex2_per_s) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  DS_TRY(ds_measure_peaks(ctx->stream, ctx->device, ffma_flops, ex2_per_s));
+  ctx->launches += 4;
+  return DSGPU_OK;
+}
+
+int dsgpu_normalize_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t pitch, const uint8_t cfa[4],
+                        float black, const float white[3], float* out, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  ds_pat pat;
+  DS_CHECK(check_pat(cfa, &pat));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!raw || !out || !white || pitch < (size_t)w) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  DS_CHECK(stage_in(ctx, flags, S_IN, raw, ((size_t)(h - 1) * pitch + w) * sizeof(uint16_t), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, n * sizeof(float), &dout));
+  DS_TRY(ds_launch_normalize_u16(ctx->stream, (const uint16_t*)din, w, h, pitch, pat, black, white, (float*)dout));
+  ctx->launches += 1;
+  return finish(ctx, flags, out, dout, n * sizeof(float));
+}
+
+int dsgpu_clip_plane(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, float* out, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!cfa_data || !out) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  DS_CHECK(stage_in(ctx, flags, S_IN, cfa_data, n * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, n * sizeof(float), &dout));
+  DS_TRY(ds_launch_clip_plane(ctx->stream, (const float*)din, w, h, (float*)dout));
+  ctx->launches += 1;
+  return finish(ctx, flags, out, dout, n * sizeof(float));
+}
+
+int dsgpu_mhc(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, const uint8_t cfa[4], const float mul[3],
+              float* out_rgb, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  ds_pat pat;
+  DS_CHECK(check_pat(cfa, &pat));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!cfa_data || !out_rgb || !mul) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  DS_CHECK(stage_in(ctx, flags, S_IN, cfa_data, n * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &dout));
+  DS_TRY(ds_launch_mhc(ctx->stream, (const float*)din, w, h, pat, mul, (float*)dout));
+  ctx->launches += 1;
+  return finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float));
+}
+
+// rcd_bayer (demosaic.rs:147-151): MHC below 16 pixels in either direction.
+static int rcd_dev(dsgpu_ctx* ctx, const float* din, int w, int h, ds_pat pat, const float mul[3], float* drgb,
+                   float* dclip) {
+  StageMark mark(ctx, DSGPU_STAGE_DEMOSAIC);
+  if (w < 16 || h < 16) {
+    DS_TRY(ds_launch_mhc(ctx->stream, din, w, h, pat, mul, drgb));
+    ctx->launches += 1;
+    if (dclip) DS_TRY(ds_launch_clip_plane(ctx->stream, din, w, h, dclip));
+    if (dclip) ctx->launches += 1;
+    return DSGPU_OK;
+  }
+  DS_TRY(ds_launch_rcd_f32(ctx->stream, ds_src_f32{din, w}, w, h, pat, mul, drgb, dclip));
+  ctx->launches += 1;
+  return DSGPU_OK;
+}
+
+int dsgpu_rcd(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, const uint8_t cfa[4], const float mul[3],
+              float* out_rgb, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  ds_pat pat;
+  DS_CHECK(check_pat(cfa, &pat));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!cfa_data || !out_rgb || !mul) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  DS_CHECK(stage_in(ctx, flags, S_IN, cfa_data, n * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &dout));
+  DS_CHECK(rcd_dev(ctx, (const float*)din, w, h, pat, mul, (float*)dout, nullptr));
+  return finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float));
+}
+
+int dsgpu_demosaic(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, const uint8_t cfa[4], const float mul[3],
+                   int quality, float* out_rgb, float* out_clip, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  ds_pat pat;
+  DS_CHECK(check_pat(cfa, &pat));
+  if (quality != DSGPU_QUALITY_FULL && quality != DSGPU_QUALITY_DRAFT) return DSGPU_ERR_ARG;
+  const size_t n = (size_t)w * h;
+  const size_t on = quality == DSGPU_QUALITY_FULL ? n : (size_t)(w / 2) * (h / 2);
+  if (n == 0) return DSGPU_OK;
+  if (!cfa_data || !out_rgb || !mul) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void *drgb, *dclip = nullptr;
+  DS_CHECK(stage_in(ctx, flags, S_IN, cfa_data, n * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, on * 3 * sizeof(float), &drgb));
+  if (out_clip) DS_CHECK(stage_out_ptr(ctx, flags, S_OUT2, out_clip, on * sizeof(float), &dclip));
+  if (quality == DSGPU_QUALITY_FULL) {
+    DS_CHECK(rcd_dev(ctx, (const float*)din, w, h, pat, mul, (float*)drgb, (float*)dclip));
+  } else {
+    DS_TRY(ds_launch_superpixel(ctx->stream, (const float*)din, w, h, pat, mul, (float*)drgb, (float*)dclip));
+    ctx->launches += 1;
+  }
+  return finish(ctx, flags, out_rgb, drgb, on * 3 * sizeof(float), out_clip, dclip, on * sizeof(float));
+}
+
+int dsgpu_box_blur(dsgpu_ctx* ctx, const float* in, int w, int h, int r, float* out, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  if (r < 0) return DSGPU_ERR_ARG;
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!in || !out) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  void* tmp;
+  DS_CHECK(stage_in(ctx, flags, S_IN, in, n * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, n * sizeof(float), &dout));
+  if (r == 0) {  // image.rs:270-272: a copy
+    DS_TRY(cudaMemcpyAsync(dout, din, n * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    DS_CHECK(scratch(ctx, S_TMP, n * sizeof(float), &tmp));
+    DS_TRY(ds_launch_box_blur(ctx->stream, (const float*)din, w, h, r, (float*)tmp, (float*)dout));
+    ctx->launches += 2;
+  }
+  return finish(ctx, flags, out, dout, n * sizeof(float));
+}
+
+int dsgpu_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h_param, int search, int patch,
+              float* out, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  DS_CHECK(nlm_args_ok(channels, search, patch));
+  const size_t n = (size_t)w * h * channels;
+  if (n == 0) return DSGPU_OK;
+  if (!in || !out) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  DS_CHECK(stage_in(ctx, flags, S_IN, in, n * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, n * sizeof(float), &dout));
+  DS_CHECK(run_nlm(ctx, (const float*)din, w, h, channels, h_param, search, patch, (float*)dout));
+  return finish(ctx, flags, out, dout, n * sizeof(float));
+}
+
+int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t pitch, const uint8_t cfa[4],
+                      float black, const float white[3], const float mul[3], float h_param, int search, int patch,
+                      float* out_rgb, float* out_clip, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  ds_pat pat;
+  DS_CHECK(check_pat(cfa, &pat));
+  DS_CHECK(nlm_args_ok(3, search, patch));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!raw || !out_rgb || !white || !mul || pitch < (size_t)w) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void *drgb, *dclip = nullptr, *mid;
+  DS_CHECK(stage_in(ctx, flags, S_IN, raw, ((size_t)(h - 1) * pitch + w) * sizeof(uint16_t), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &drgb));
+  if (out_clip) DS_CHECK(stage_out_ptr(ctx, flags, S_OUT2, out_clip, n * sizeof(float), &dclip));
+  DS_CHECK(scratch(ctx, S_RGB, n * 3 * sizeof(float), &mid));
+  if (w < 16 || h < 16) {
+    void* cfa_f;
+    DS_CHECK(scratch(ctx, S_CFA, n * sizeof(float), &cfa_f));
+    DS_TRY(ds_launch_normalize_u16(ctx->stream, (const uint16_t*)din, w, h, pitch, pat, black, white, (float*)cfa_f));
+    ctx->launches += 1;
+    DS_CHECK(rcd_dev(ctx, (const float*)cfa_f, w, h, pat, mul, (float*)mid, (float*)dclip));
+  } else {
+    StageMark mark(ctx, DSGPU_STAGE_DEMOSAIC);
+    ds_src_u16 src{(const uint16_t*)din, pitch, black, {white[0], white[1], white[2]}};
+    DS_TRY(ds_launch_rcd_u16(ctx->stream, src, w, h, pat, mul, (float*)mid, (float*)dclip));
+    ctx->launches += 1;
+  }
+  DS_CHECK(run_nlm(ctx, (const float*)mid, w, h, 3, h_param, search, patch, (float*)drgb));
+  return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));
+}
+
+// ------------------------------------------------------------------ scenes
+
+int dsgpu_scene_render_host(const dsgpu_scene_desc* d, int x0, int y0, int cw, int ch, uint16_t* out) {
+  if (!d || !out || cw < 0 || ch < 0 || d->w <= 0 || d->h <= 0) return DSGPU_ERR_ARG;
+  if (x0 < 0 || y0 < 0 || x0 + cw > d->w || y0 + ch > d->h) return DSGPU_ERR_ARG;
+  ds_pat pat;
+  DS_CHECK(check_pat(d->cfa, &pat));
+  ds_scene s = ds_scene_make(d);
+  ds_scene_host(s, x0, y0, cw, ch, out);
+  return DSGPU_OK;
+}
+
+int dsgpu_scene_truth_host(const dsgpu_scene_desc* d, int x0, int y0, int cw, int ch, float* out) {
+  if (!d || !out || cw < 0 || ch < 0 || d->w <= 0 || d->h <= 0) return DSGPU_ERR_ARG;
+  if (x0 < 0 || y0 < 0 || x0 + cw > d->w || y0 + ch > d->h) return DSGPU_ERR_ARG;
+  ds_scene s = ds_scene_make(d);
+  ds_scene_truth(s, x0, y0, cw, ch, out);
+  return DSGPU_OK;
+}
+
+int dsgpu_scene_render(dsgpu_ctx* ctx, const dsgpu_scene_desc* d, uint16_t* out, unsigned flags) {
+  if (!ctx || !d || !out || d->w <= 0 || d->h <= 0) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(d->w, d->h));
+  ds_pat pat;
+  DS_CHECK(check_pat(d->cfa, &pat));
+  DeviceGuard g(ctx->device);
+  const size_t bytes = (size_t)d->w * d->h * sizeof(uint16_t);
+  void* dout;
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, bytes, &dout));
+  ds_scene s = ds_scene_make(d);
+  DS_TRY(ds_launch_scene(ctx->stream, s, (uint16_t*)dout));
+  ctx->launches += 1;
+  return finish(ctx, flags, out, dout, bytes);
+}
+
+}  // extern "C"

@@ -1,0 +1,45 @@
+// Internal declarations shared by the dsgpu translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/dsgpu.h"
+
+// 2x2 Bayer pattern, colour code at (x, y) = c[(y & 1) * 2 + (x & 1)]
+// (decode.rs:26-28 for a 2x2 pattern; the bit test also gives the right
+// parity for the negative coordinates of out-of-image halo sites).
+struct ds_pat {
+  uint32_t packed;  // byte k = colour of pattern index k
+  __host__ __device__ __forceinline__ int at(int x, int y) const {
+    return (packed >> ((((y & 1) << 1) | (x & 1)) * 8)) & 0xFFu;
+  }
+};
+
+// Where a demosaic kernel reads its CFA samples from.
+struct ds_src_f32 {  // normalised float CFA (CfaImage::data)
+  const float* data;
+  int pitch;  // elements
+};
+struct ds_src_u16 {  // integer raw + the normalisation of decode.rs:303
+  const uint16_t* data;
+  size_t pitch;  // elements
+  float black;
+  float white[3];
+};
+
+// kernel launchers (return cudaGetLastError() of the launch)
+cudaError_t ds_launch_normalize_u16(cudaStream_t st, const uint16_t* raw, int w, int h, size_t pitch, ds_pat pat,
+                                    float black, const float white[3], float* out);
+cudaError_t ds_launch_clip_plane(cudaStream_t st, const float* cfa, int w, int h, float* out);
+cudaError_t ds_launch_mhc(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, const float mul[3],
+                          float* out_rgb);
+cudaError_t ds_launch_rcd_f32(cudaStream_t st, ds_src_f32 src, int w, int h, ds_pat pat, const float mul[3],
+                              float* out_rgb, float* out_clip);
+cudaError_t ds_launch_rcd_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, const float mul[3],
+                              float* out_rgb, float* out_clip);
+cudaError_t ds_launch_superpixel(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, const float mul[3],
+                                 float* out_rgb, float* out_clip);
+cudaError_t ds_launch_box_blur(cudaStream_t st, const float* in, int w, int h, int r, float* tmp, float* out);
+cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int channels, float h_param, int search,
+                          int patch, float* out);

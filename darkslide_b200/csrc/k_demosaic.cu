@@ -1,0 +1,417 @@
+// Demosaic kernels: CFA normalisation, clip plane, MHC, superpixel and the
+// fused RCD tile kernel.
+//
+// This file is compiled with -fmad=false: the reference (Rust) rounds every
+// product before adding it, so the GPU must not contract a*b+c into FMAs for
+// these kernels to reproduce it bit for bit. Divisions are IEEE (__fdiv_rn).
+#include "internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ------------------------------------------------------------ normalisation
+// decode.rs:292-306: v = (raw - black) / max(white[c] - black, 1)
+__device__ __forceinline__ float norm_u16(uint16_t raw, float black, float white_c) {
+  return __fdiv_rn((float)raw - black, fmaxf(white_c - black, 1.0f));
+}
+
+__global__ void normalize_u16_kernel(const uint16_t* __restrict__ raw, int w, int h, size_t pitch, ds_pat pat,
+                                     float black, float w0, float w1, float w2, float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w) return;
+  const int c = pat.at(x, y);
+  const float wc = c == 0 ? w0 : (c == 1 ? w1 : w2);
+  out[(size_t)y * w + x] = norm_u16(raw[(size_t)y * pitch + x], black, wc);
+}
+
+// ---------------------------------------------------------------- clip plane
+// demosaic.rs:31-42 (CLIP = 0.995, demosaic.rs:17)
+__global__ void clip_plane_kernel(const float* __restrict__ cfa, int w, int h, float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w) return;
+  float m = 0.0f;
+  for (int dy = -1; dy <= 1; dy++)
+    for (int dx = -1; dx <= 1; dx++) {
+      const float v = cfa[(size_t)clampi(y + dy, 0, h - 1) * w + clampi(x + dx, 0, w - 1)];
+      m = fmaxf(m, v >= 0.995f ? 1.0f : 0.0f);
+    }
+  out[(size_t)y * w + x] = m;
+}
+
+// ------------------------------------------------------------------- MHC
+// demosaic.rs:90-124. `at(dx,dy)` returns data*mul at the clamped site,
+// without max(0). The formulas keep the reference's evaluation order.
+template <class At>
+__device__ __forceinline__ void mhc_formulas(At p, int c, int row_c, float& o0, float& o1, float& o2) {
+  const float v = p(0, 0);
+  const float g_at_rb = __fdiv_rn(4.0f * v + 2.0f * (p(0, -1) + p(-1, 0) + p(1, 0) + p(0, 1)) -
+                                      (p(0, -2) + p(-2, 0) + p(2, 0) + p(0, 2)),
+                                  8.0f);
+  const float rb_g_row = __fdiv_rn(5.0f * v + 4.0f * (p(-1, 0) + p(1, 0)) -
+                                       (p(-2, 0) + p(2, 0) + p(-1, -1) + p(1, -1) + p(-1, 1) + p(1, 1)) +
+                                       0.5f * (p(0, -2) + p(0, 2)),
+                                   8.0f);
+  const float rb_g_col = __fdiv_rn(5.0f * v + 4.0f * (p(0, -1) + p(0, 1)) -
+                                       (p(0, -2) + p(0, 2) + p(-1, -1) + p(1, -1) + p(-1, 1) + p(1, 1)) +
+                                       0.5f * (p(-2, 0) + p(2, 0)),
+                                   8.0f);
+  const float rb_diag = __fdiv_rn(6.0f * v + 2.0f * (p(-1, -1) + p(1, -1) + p(-1, 1) + p(1, 1)) -
+                                      1.5f * (p(0, -2) + p(-2, 0) + p(2, 0) + p(0, 2)),
+                                  8.0f);
+  if (c == 1) {
+    if (row_c == 0) { o0 = rb_g_row; o1 = v; o2 = rb_g_col; }
+    else            { o0 = rb_g_col; o1 = v; o2 = rb_g_row; }
+  } else if (c == 0) { o0 = v; o1 = g_at_rb; o2 = rb_diag; }
+  else               { o0 = rb_diag; o1 = g_at_rb; o2 = v; }
+  o0 = fmaxf(o0, 0.0f);
+  o1 = fmaxf(o1, 0.0f);
+  o2 = fmaxf(o2, 0.0f);
+}
+
+__global__ void mhc_kernel(const float* __restrict__ cfa, int w, int h, ds_pat pat, float m0, float m1, float m2,
+                           float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w) return;
+  auto p = [&](int dx, int dy) {
+    const int sx = clampi(x + dx, 0, w - 1), sy = clampi(y + dy, 0, h - 1);
+    const int c = pat.at(sx, sy);
+    return cfa[(size_t)sy * w + sx] * (c == 0 ? m0 : (c == 1 ? m1 : m2));
+  };
+  float o0, o1, o2;
+  mhc_formulas(p, pat.at(x, y), pat.at(x + 1, y), o0, o1, o2);
+  float* o = out + ((size_t)y * w + x) * 3;
+  o[0] = o0;
+  o[1] = o1;
+  o[2] = o2;
+}
+
+// --------------------------------------------------------------- superpixel
+// demosaic.rs:45-87 for a Bayer (2x2) pattern: output (w/2, h/2).
+__global__ void superpixel_kernel(const float* __restrict__ cfa, int w, int h, ds_pat pat, float m0, float m1,
+                                  float m2, float* __restrict__ out, float* __restrict__ clip) {
+  const int ow = w / 2;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= ow) return;
+  const float CLIP = 0.995f;
+  float acc[3] = {0.f, 0.f, 0.f}, mx[3] = {0.f, 0.f, 0.f};
+  unsigned n[3] = {0, 0, 0}, clipped = 0;
+  for (int dy = 0; dy < 2; dy++)
+    for (int dx = 0; dx < 2; dx++) {
+      const int sx = x * 2 + dx, sy = y * 2 + dy;
+      const int c = pat.at(sx, sy);
+      const float v = cfa[(size_t)sy * w + sx];
+      if (v >= CLIP) clipped++;
+      mx[c] = fmaxf(mx[c], v);
+      acc[c] += v;
+      n[c]++;
+    }
+  const float mul[3] = {m0, m1, m2};
+  float* o = out + ((size_t)y * ow + x) * 3;
+  for (int c = 0; c < 3; c++) {
+    const float v = mx[c] >= CLIP ? mx[c] : (n[c] > 0 ? __fdiv_rn(acc[c], (float)n[c]) : 0.0f);
+    o[c] = v * mul[c];
+  }
+  if (clip) clip[(size_t)y * ow + x] = fminf(__fdiv_rn((float)clipped, 4.0f) * 2.0f, 1.0f);
+}
+
+// ------------------------------------------------------------------ RCD tile
+// One CTA produces a RT x RT tile of RGB (and clip) output. Every RCD pass of
+// demosaic.rs:147-344 runs on the tile plus the halo it needs, in shared
+// memory, in the reference's order and with its global border rules (each
+// stage value at a site follows the site's GLOBAL coordinates: bv/bh/bp/bq on
+// [3, W-3), vh/pq on [4, W-4) else 0.5, lpf on [2, W-2) at R/B sites, RCD
+// writes on [4, W-4), MHC elsewhere).
+//
+// Receptive radius: 4.4 reads 4.3 output at +-3; 4.3 reads g at +-2 and pq at
+// +-1; g reads c at +-4, lpf at +-2, vh at +-1; vh reads bv/bh at +-1, which
+// read c at +-3. So the tile loads a 10-sample halo (local stage regions:
+// m [0,52), b* and lpf [3,49), vh/pq [4,48), g [5,47), r43/b43 [7,45),
+// output [10,42)).
+constexpr int RT = 32;
+constexpr int RH = 10;
+constexpr int RS = RT + 2 * RH;  // 52
+constexpr int RA = RS * RS;      // one stage array
+constexpr int RCD_THREADS = 256;
+constexpr size_t RCD_SMEM = (size_t)8 * RA * sizeof(float) + RA;
+
+struct SrcF32 {
+  ds_src_f32 s;
+  __device__ __forceinline__ float load(int gx, int gy, int) const { return s.data[(size_t)gy * s.pitch + gx]; }
+};
+struct SrcU16 {
+  ds_src_u16 s;
+  __device__ __forceinline__ float load(int gx, int gy, int c) const {
+    const float wc = c == 0 ? s.white[0] : (c == 1 ? s.white[1] : s.white[2]);
+    return norm_u16(s.data[(size_t)gy * s.pitch + gx], s.black, wc);
+  }
+};
+
+__device__ __forceinline__ float sq(float v) { return v * v; }
+
+template <class Src>
+__global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
+                                                               float m1, float m2, float* __restrict__ out_rgb,
+                                                               float* __restrict__ out_clip) {
+  extern __shared__ float4 smem4[];
+  float* M = reinterpret_cast<float*>(smem4);  // data*mul (clamped-site load), not max(0)
+  float* BV = M + RA;   // bv, later g
+  float* BH = BV + RA;  // bh, later r after 4.3
+  float* BP = BH + RA;  // bp, later b after 4.3
+  float* BQ = BP + RA;
+  float* LP = BQ + RA;
+  float* VH = LP + RA;
+  float* PQ = VH + RA;
+  uint8_t* CL = reinterpret_cast<uint8_t*>(PQ + RA);  // [v >= CLIP]
+  float* G = BV;
+  float* R43 = BH;
+  float* B43 = BP;
+
+  const int tid = threadIdx.x;
+  const int gx0 = blockIdx.x * RT - RH, gy0 = blockIdx.y * RT - RH;  // global site of local (0,0)
+  const float eps = 1e-5f;
+
+  // stage 0: load with clamped coordinates
+  for (int i = tid; i < RA; i += RCD_THREADS) {
+    const int ly = i / RS, lx = i - ly * RS;
+    const int gx = clampi(gx0 + lx, 0, W - 1), gy = clampi(gy0 + ly, 0, H - 1);
+    const int col = pat.at(gx, gy);
+    const float v = src.load(gx, gy, col);
+    M[i] = v * (col == 0 ? m0 : (col == 1 ? m1 : m2));
+    CL[i] = v >= 0.995f ? 1 : 0;
+  }
+  __syncthreads();
+
+  auto C = [&](int k) { return fmaxf(M[k], 0.0f); };  // demosaic.rs:154
+  const int w1 = RS, w2 = 2 * RS, w3 = 3 * RS, w4 = 4 * RS;
+
+  // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, RS-3)
+  for (int i = tid; i < (RS - 6) * (RS - 6); i += RCD_THREADS) {
+    const int ly = 3 + i / (RS - 6), lx = 3 + i % (RS - 6);
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    const int k = ly * RS + lx;
+    float bv = 0.f, bh = 0.f, bp = 0.f, bq = 0.f, lp = 0.f;
+    if (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3) {
+      const float c0 = C(k);
+      bv = sq((C(k - w3) - C(k - w1) - C(k + w1) + C(k + w3)) - 3.0f * (C(k - w2) + C(k + w2)) + 6.0f * c0);
+      bh = sq((C(k - 3) - C(k - 1) - C(k + 1) + C(k + 3)) - 3.0f * (C(k - 2) + C(k + 2)) + 6.0f * c0);
+      bp = sq((C(k - w3 - 3) - C(k - w1 - 1) - C(k + w1 + 1) + C(k + w3 + 3)) - 3.0f * (C(k - w2 - 2) + C(k + w2 + 2)) +
+              6.0f * c0);
+      bq = sq((C(k - w3 + 3) - C(k - w1 + 1) - C(k + w1 - 1) + C(k + w3 - 3)) - 3.0f * (C(k - w2 + 2) + C(k + w2 - 2)) +
+              6.0f * c0);
+    }
+    if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2 && pat.at(gx, gy) != 1) {
+      lp = C(k) + 0.5f * (C(k - w1) + C(k + w1) + C(k - 1) + C(k + 1)) +
+           0.25f * (C(k - w1 - 1) + C(k - w1 + 1) + C(k + w1 - 1) + C(k + w1 + 1));
+    }
+    BV[k] = bv;
+    BH[k] = bh;
+    BP[k] = bp;
+    BQ[k] = bq;
+    LP[k] = lp;
+  }
+  __syncthreads();
+
+  // stage 2: vh (:173-184) and pq (:261-272) on [4, RS-4)
+  for (int i = tid; i < (RS - 8) * (RS - 8); i += RCD_THREADS) {
+    const int ly = 4 + i / (RS - 8), lx = 4 + i % (RS - 8);
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    const int k = ly * RS + lx;
+    float vh = 0.5f, pq = 0.5f;
+    if (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4) {
+      const float vs = fmaxf(BV[k - w1] + BV[k] + BV[k + w1], eps);
+      const float hs = fmaxf(BH[k - 1] + BH[k] + BH[k + 1], eps);
+      vh = __fdiv_rn(vs, vs + hs);
+      const float ps = fmaxf(BP[k - w1 - 1] + BP[k] + BP[k + w1 + 1], eps);
+      const float qs = fmaxf(BQ[k - w1 + 1] + BQ[k] + BQ[k + w1 - 1], eps);
+      pq = __fdiv_rn(ps, ps + qs);
+    }
+    VH[k] = vh;
+    PQ[k] = pq;
+  }
+  __syncthreads();
+
+  auto disc = [&](const float* d, int k) {  // :216-220
+    const float central = d[k];
+    const float neigh = 0.25f * (d[k - w1 - 1] + d[k - w1 + 1] + d[k + w1 - 1] + d[k + w1 + 1]);
+    return fabsf(0.5f - central) < fabsf(0.5f - neigh) ? neigh : central;
+  };
+  auto mhc_at = [&](int k, int gx, int gy, float& o0, float& o1, float& o2) {  // ring sites only
+    auto p = [&](int dx, int dy) { return M[k + dy * RS + dx]; };
+    mhc_formulas(p, pat.at(gx, gy), pat.at(gx + 1, gy), o0, o1, o2);
+  };
+
+  // stage 3: green (:203-214 init, :222-245 step 3) on [5, RS-5)
+  for (int i = tid; i < (RS - 10) * (RS - 10); i += RCD_THREADS) {
+    const int ly = 5 + i / (RS - 10), lx = 5 + i % (RS - 10);
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    const int k = ly * RS + lx;
+    const int col = pat.at(gx, gy);
+    float g;
+    if (col == 1) {
+      g = C(k);
+    } else if (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4) {
+      const float vd = disc(VH, k);
+      const float n_grad = eps + fabsf(C(k - w1) - C(k + w1)) + fabsf(C(k) - C(k - w2)) + fabsf(C(k - w1) - C(k - w3)) +
+                           fabsf(C(k - w2) - C(k - w4));
+      const float s_grad = eps + fabsf(C(k - w1) - C(k + w1)) + fabsf(C(k) - C(k + w2)) + fabsf(C(k + w1) - C(k + w3)) +
+                           fabsf(C(k + w2) - C(k + w4));
+      const float w_grad = eps + fabsf(C(k - 1) - C(k + 1)) + fabsf(C(k) - C(k - 2)) + fabsf(C(k - 1) - C(k - 3)) +
+                           fabsf(C(k - 2) - C(k - 4));
+      const float e_grad = eps + fabsf(C(k - 1) - C(k + 1)) + fabsf(C(k) - C(k + 2)) + fabsf(C(k + 1) - C(k + 3)) +
+                           fabsf(C(k + 2) - C(k + 4));
+      const float l0 = LP[k];
+      const float n_est = __fdiv_rn(C(k - w1) * 2.0f * l0, eps + l0 + LP[k - w2]);
+      const float s_est = __fdiv_rn(C(k + w1) * 2.0f * l0, eps + l0 + LP[k + w2]);
+      const float w_est = __fdiv_rn(C(k - 1) * 2.0f * l0, eps + l0 + LP[k - 2]);
+      const float e_est = __fdiv_rn(C(k + 1) * 2.0f * l0, eps + l0 + LP[k + 2]);
+      const float v_est = __fdiv_rn(s_grad * n_est + n_grad * s_est, n_grad + s_grad);
+      const float h_est = __fdiv_rn(w_grad * e_est + e_grad * w_est, e_grad + w_grad);
+      g = fmaxf(vd * h_est + (1.0f - vd) * v_est, 0.0f);
+    } else {
+      float o0, o1, o2;
+      mhc_at(k, gx, gy, o0, o1, o2);
+      g = o1;
+    }
+    G[k] = g;
+  }
+  __syncthreads();
+
+  // stage 4: R at B and B at R (:276-308) on [7, RS-7). The pre-pass clone
+  // read at the diagonal +-1/+-3 sites of an R (B) site holds native B (R)
+  // samples, i.e. c.
+  for (int i = tid; i < (RS - 14) * (RS - 14); i += RCD_THREADS) {
+    const int ly = 7 + i / (RS - 14), lx = 7 + i % (RS - 14);
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    const int k = ly * RS + lx;
+    const int col = pat.at(gx, gy);
+    const bool inner = gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4;
+    float r, b;
+    if (inner) {
+      if (col == 1) continue;  // never read: 4.4 reads R/B sites only
+      const float pd = disc(PQ, k);
+      const float g0 = G[k];
+      const float nw_g = eps + fabsf(C(k - w1 - 1) - C(k + w1 + 1)) + fabsf(C(k - w1 - 1) - C(k - w3 - 3)) + fabsf(g0 - G[k - w2 - 2]);
+      const float ne_g = eps + fabsf(C(k - w1 + 1) - C(k + w1 - 1)) + fabsf(C(k - w1 + 1) - C(k - w3 + 3)) + fabsf(g0 - G[k - w2 + 2]);
+      const float sw_g = eps + fabsf(C(k + w1 - 1) - C(k - w1 + 1)) + fabsf(C(k + w1 - 1) - C(k + w3 - 3)) + fabsf(g0 - G[k + w2 - 2]);
+      const float se_g = eps + fabsf(C(k + w1 + 1) - C(k - w1 - 1)) + fabsf(C(k + w1 + 1) - C(k + w3 + 3)) + fabsf(g0 - G[k + w2 + 2]);
+      const float nw_e = C(k - w1 - 1) - G[k - w1 - 1];
+      const float ne_e = C(k - w1 + 1) - G[k - w1 + 1];
+      const float sw_e = C(k + w1 - 1) - G[k + w1 - 1];
+      const float se_e = C(k + w1 + 1) - G[k + w1 + 1];
+      const float p_est = __fdiv_rn(nw_g * se_e + se_g * nw_e, nw_g + se_g);
+      const float q_est = __fdiv_rn(ne_g * sw_e + sw_g * ne_e, ne_g + sw_g);
+      const float v = fmaxf(g0 + (1.0f - pd) * p_est + pd * q_est, 0.0f);
+      if (col == 2) { r = v; b = C(k); }
+      else          { r = C(k); b = v; }
+    } else {
+      float o0, o1, o2;
+      mhc_at(k, gx, gy, o0, o1, o2);
+      r = col == 0 ? C(k) : o0;
+      b = col == 2 ? C(k) : o2;
+    }
+    R43[k] = r;
+    B43[k] = b;
+  }
+  __syncthreads();
+
+  // stage 5: R and B at G (:310-341) and the tile's output
+  for (int i = tid; i < RT * RT; i += RCD_THREADS) {
+    const int ty = i / RT, tx = i - ty * RT;
+    const int ly = RH + ty, lx = RH + tx;
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    if (gx >= W || gy >= H) continue;
+    const int k = ly * RS + lx;
+    const bool inner = gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4;
+    float r = R43[k], g = G[k], b = B43[k];
+    if (inner && pat.at(gx, gy) == 1) {
+      const float vd = disc(VH, k);
+      auto pass44 = [&](const float* cc) {
+        const float n_g = eps + fabsf(g - G[k - w2]) + fabsf(cc[k - w1] - cc[k + w1]) + fabsf(cc[k - w1] - cc[k - w3]);
+        const float s_g = eps + fabsf(g - G[k + w2]) + fabsf(cc[k + w1] - cc[k - w1]) + fabsf(cc[k + w1] - cc[k + w3]);
+        const float w_g = eps + fabsf(g - G[k - 2]) + fabsf(cc[k - 1] - cc[k + 1]) + fabsf(cc[k - 1] - cc[k - 3]);
+        const float e_g = eps + fabsf(g - G[k + 2]) + fabsf(cc[k + 1] - cc[k - 1]) + fabsf(cc[k + 1] - cc[k + 3]);
+        const float n_e = cc[k - w1] - G[k - w1];
+        const float s_e = cc[k + w1] - G[k + w1];
+        const float w_e = cc[k - 1] - G[k - 1];
+        const float e_e = cc[k + 1] - G[k + 1];
+        const float v_est = __fdiv_rn(n_g * s_e + s_g * n_e, n_g + s_g);
+        const float h_est = __fdiv_rn(e_g * w_e + w_g * e_e, e_g + w_g);
+        return fmaxf(g + (1.0f - vd) * v_est + vd * h_est, 0.0f);
+      };
+      r = pass44(R43);
+      b = pass44(B43);
+    }
+    float* o = out_rgb + ((size_t)gy * W + gx) * 3;
+    o[0] = r;
+    o[1] = g;
+    o[2] = b;
+    if (out_clip) {
+      unsigned m = 0;
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) m |= CL[k + dy * RS + dx];
+      out_clip[(size_t)gy * W + gx] = m ? 1.0f : 0.0f;
+    }
+  }
+}
+
+template <class Src>
+cudaError_t launch_rcd(cudaStream_t st, Src src, int w, int h, ds_pat pat, const float mul[3], float* out_rgb,
+                       float* out_clip) {
+  static bool attr_set = false;  // per process; the attribute is per function
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(rcd_tile_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)RCD_SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  dim3 grid((w + RT - 1) / RT, (h + RT - 1) / RT);
+  rcd_tile_kernel<Src><<<grid, RCD_THREADS, RCD_SMEM, st>>>(src, w, h, pat, mul[0], mul[1], mul[2], out_rgb,
+                                                            out_clip);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t ds_launch_normalize_u16(cudaStream_t st, const uint16_t* raw, int w, int h, size_t pitch, ds_pat pat,
+                                    float black, const float white[3], float* out) {
+  dim3 grid((w + 255) / 256, h);
+  normalize_u16_kernel<<<grid, 256, 0, st>>>(raw, w, h, pitch, pat, black, white[0], white[1], white[2], out);
+  return cudaGetLastError();
+}
+
+cudaError_t ds_launch_clip_plane(cudaStream_t st, const float* cfa, int w, int h, float* out) {
+  dim3 grid((w + 255) / 256, h);
+  clip_plane_kernel<<<grid, 256, 0, st>>>(cfa, w, h, out);
+  return cudaGetLastError();
+}
+
+cudaError_t ds_launch_mhc(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, const float mul[3],
+                          float* out_rgb) {
+  dim3 grid((w + 255) / 256, h);
+  mhc_kernel<<<grid, 256, 0, st>>>(cfa, w, h, pat, mul[0], mul[1], mul[2], out_rgb);
+  return cudaGetLastError();
+}
+
+cudaError_t ds_launch_superpixel(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, const float mul[3],
+                                 float* out_rgb, float* out_clip) {
+  const int ow = w / 2, oh = h / 2;
+  if (ow == 0 || oh == 0) return cudaSuccess;
+  dim3 grid((ow + 255) / 256, oh);
+  superpixel_kernel<<<grid, 256, 0, st>>>(cfa, w, h, pat, mul[0], mul[1], mul[2], out_rgb, out_clip);
+  return cudaGetLastError();
+}
+
+cudaError_t ds_launch_rcd_f32(cudaStream_t st, ds_src_f32 src, int w, int h, ds_pat pat, const float mul[3],
+                              float* out_rgb, float* out_clip) {
+  return launch_rcd(st, SrcF32{src}, w, h, pat, mul, out_rgb, out_clip);
+}
+
+cudaError_t ds_launch_rcd_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, const float mul[3],
+                              float* out_rgb, float* out_clip) {
+  return launch_rcd(st, SrcU16{src}, w, h, pat, mul, out_rgb, out_clip);
+}

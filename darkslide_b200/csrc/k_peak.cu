@@ -1,0 +1,86 @@
+// Throughput microbenchmarks for the roofline of the NLM kernel, which is
+// bound by the SFU (ex2) and FP32 pipes rather than by HBM or tensor cores:
+//   ffma_kernel: 8 independent FFMA chains per thread -> FP32 FLOP/s
+//   ex2_kernel : 8 independent ex2.approx chains per thread -> ex2/s
+// Each runs on every SM (grid = 8 x SM count) for a fixed iteration count.
+#include "internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm volatile("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__global__ void __launch_bounds__(256) ffma_kernel(int iters, float seed, float* sink) {
+  float a[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) a[i] = seed + threadIdx.x * 1e-7f + i;
+  const float m = 0.999999f, c = 1e-7f;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = fmaf(a[i], m, c);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s += a[i];
+  if (s == 12345.678f) sink[0] = s;  // keeps the chains live
+}
+
+__global__ void __launch_bounds__(256) ex2_kernel(int iters, float seed, float* sink) {
+  float a[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) a[i] = seed + threadIdx.x * 1e-7f + i * 0.01f;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = ex2_approx(-a[i]);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s += a[i];
+  if (s == 12345.678f) sink[0] = s;
+}
+
+}  // namespace
+
+// Times both kernels with CUDA events on `st`; returns FLOP/s and ex2/s.
+cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s) {
+  int sms = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  float* sink = nullptr;
+  if ((e = cudaMallocAsync(&sink, 16, st)) != cudaSuccess) return e;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int blocks = sms * 8, threads = 256;
+  const int it_f = 4096, it_e = 512;
+  float ms = 0.f;
+  for (int rep = 0; rep < 2; rep++) {  // first rep warms up
+    cudaEventRecord(a, st);
+    ffma_kernel<<<blocks, threads, 0, st>>>(it_f, 1.0f, sink);
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+  }
+  *ffma_flops = 2.0 * 8 * 16 * (double)it_f * blocks * threads / (ms * 1e-3);
+  for (int rep = 0; rep < 2; rep++) {
+    cudaEventRecord(a, st);
+    ex2_kernel<<<blocks, threads, 0, st>>>(it_e, 0.5f, sink);
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+  }
+  *ex2_per_s = 8.0 * 16 * (double)it_e * blocks * threads / (ms * 1e-3);
+  e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFreeAsync(sink, st);
+  cudaStreamSynchronize(st);
+  return e;
+}

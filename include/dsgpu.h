@@ -1,0 +1,144 @@
+/* dsgpu.h — C ABI of the B200 (sm_100a) RCD demosaic + NLM denoise library.
+ *
+ * This is the drop-in boundary for darkslide-core's raw-develop detail path.
+ * Each entry point replaces one function of the reference (Rust, crates/core);
+ * the reference citation is given beside each declaration. Argument meaning
+ * follows the reference: a Bayer pattern is four colour codes (0=R, 1=G, 2=B)
+ * indexed by (y%2)*2 + x%2 (decode.rs:26-28), images are row-major, RGB
+ * images are interleaved float[3] per pixel (image.rs:7-13), planes are float
+ * (image.rs:15-21), CFA data is normalised so 1.0 is white (decode.rs:49-56).
+ *
+ * Conventions
+ *  - Every call returns DSGPU_OK (0) or a negative DSGPU_ERR_* code; the
+ *    library never aborts. dsgpu_strerror() names a code.
+ *  - Buffers are caller-allocated. Without DSGPU_HOST every pointer is device
+ *    memory of the context's device and the work is enqueued on the context
+ *    stream (dsgpu_set_stream); the call synchronises that stream before
+ *    returning unless DSGPU_ASYNC is given. With DSGPU_HOST every pointer is
+ *    host memory (pinned memory is fastest): the call copies inputs to device
+ *    scratch, runs, copies results back and synchronises.
+ *  - A context is used by one thread at a time (one context per caller
+ *    thread), like the reference's Engine calls on the render worker.
+ *  - Degenerate inputs are absorbed the way the reference absorbs them: RCD
+ *    on w or h < 16 is MHC (demosaic.rs:149-151); NLM floors h^2 and the
+ *    weight sum at 1e-12 (enhance.rs:40,71); a negative search radius gives
+ *    an empty offset set and a zero image (enhance.rs:41,71).
+ */
+#ifndef DSGPU_H
+#define DSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSGPU_ABI_VERSION 1
+
+/* status codes */
+#define DSGPU_OK 0
+#define DSGPU_ERR_ARG (-1)      /* null pointer, negative size or radius out of range */
+#define DSGPU_ERR_CFA (-2)      /* colour code outside {0,1,2} */
+#define DSGPU_ERR_SIZE (-3)     /* image larger than the library limits */
+#define DSGPU_ERR_NOMEM (-4)    /* device or pinned allocation failed */
+#define DSGPU_ERR_CUDA (-5)     /* a CUDA runtime call failed */
+#define DSGPU_ERR_NODEV (-6)    /* no usable sm_100 device */
+#define DSGPU_ERR_TIMEOUT (-7)  /* a bounded device-side wait gave up */
+#define DSGPU_ERR_UNSUPPORTED (-8)
+
+/* flags */
+#define DSGPU_HOST 1u  /* buffers are host memory */
+#define DSGPU_ASYNC 2u /* device buffers: do not synchronise before returning */
+
+/* demosaic quality (demosaic.rs:9-15) */
+#define DSGPU_QUALITY_DRAFT 0
+#define DSGPU_QUALITY_FULL 1
+
+/* limits */
+#define DSGPU_MAX_DIM 65535      /* w, h */
+#define DSGPU_NLM_MAX_SEARCH 16  /* search radius S */
+#define DSGPU_NLM_MAX_PATCH 7    /* patch radius P */
+
+typedef struct dsgpu_ctx dsgpu_ctx;
+
+const char* dsgpu_strerror(int status);
+int dsgpu_abi_version(void);
+
+/* Context: owns a CUDA stream (or borrows the caller's), device scratch and
+ * pinned staging buffers. `device` is a CUDA ordinal. */
+int dsgpu_create(int device, dsgpu_ctx** out);
+int dsgpu_destroy(dsgpu_ctx* ctx);
+/* Use the caller's cudaStream_t (NULL: back to the context's own stream). */
+int dsgpu_set_stream(dsgpu_ctx* ctx, void* cuda_stream);
+void* dsgpu_get_stream(dsgpu_ctx* ctx);
+int dsgpu_synchronize(dsgpu_ctx* ctx);
+/* Release cached scratch (it is regrown on demand). */
+int dsgpu_trim(dsgpu_ctx* ctx);
+/* Text of the last CUDA failure seen by this context ("" if none). */
+const char* dsgpu_last_error(dsgpu_ctx* ctx);
+
+/* Instrumentation; the analogue of the reference's Lap stage timer
+ * (pipeline/mod.rs:106-137), which logs per-stage wall time.
+ * dsgpu_profile(ctx, 1) starts recording CUDA events around each stage of
+ * every later call on the context stream (and discards earlier records);
+ * dsgpu_stage_ms() sums the recorded device time of one stage.
+ * dsgpu_launch_count() is the number of kernels the context has launched.
+ * dsgpu_measure_peaks() times FP32 FMA and ex2 throughput microbenchmarks
+ * (the roofline denominators of the NLM kernel). */
+#define DSGPU_STAGE_DEMOSAIC 0
+#define DSGPU_STAGE_NLM 1
+#define DSGPU_STAGE_COPY 2
+int dsgpu_profile(dsgpu_ctx* ctx, int enable);
+int dsgpu_stage_ms(dsgpu_ctx* ctx, int stage, double* total_ms, int* count);
+unsigned long long dsgpu_launch_count(dsgpu_ctx* ctx);
+int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops_per_s, double* ex2_per_s);
+
+/* CFA normalisation of an integer raw: out = (raw - black) / max(white[c] - black, 1),
+ * c the colour of the site; values are not clamped.
+ * Replaces the integer branch of load_raw, decode.rs:292-306 (formula :303). */
+int dsgpu_normalize_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t pitch_elems,
+                        const uint8_t cfa[4], float black, const float white[3], float* out_cfa,
+                        unsigned flags);
+
+/* 3x3 clamped-edge max of [v >= 0.995]. Replaces clip_plane, demosaic.rs:31-42. */
+int dsgpu_clip_plane(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, float* out_clip, unsigned flags);
+
+/* Malvar-He-Cutler Bayer demosaic. Replaces mhc_bayer, demosaic.rs:90-124. */
+int dsgpu_mhc(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, const uint8_t cfa[4], const float mul[3],
+              float* out_rgb, unsigned flags);
+
+/* RCD Bayer demosaic (MHC when w or h < 16). Replaces rcd_bayer, demosaic.rs:147-344. */
+int dsgpu_rcd(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, const uint8_t cfa[4], const float mul[3],
+              float* out_rgb, unsigned flags);
+
+/* demosaic(cfa, mul, quality) for a Bayer pattern, demosaic.rs:20-27.
+ * FULL: out_rgb is w*h*3 (RCD), out_clip w*h (clip_plane).
+ * DRAFT: superpixel (demosaic.rs:45-87): out_rgb is (w/2)*(h/2)*3 and
+ * out_clip (w/2)*(h/2). out_clip may be NULL. */
+int dsgpu_demosaic(dsgpu_ctx* ctx, const float* cfa_data, int w, int h, const uint8_t cfa[4],
+                   const float mul[3], int quality, float* out_rgb, float* out_clip, unsigned flags);
+
+/* Separable clamped-edge box blur of radius r. Replaces box_blur, image.rs:269-313. */
+int dsgpu_box_blur(dsgpu_ctx* ctx, const float* in, int w, int h, int r, float* out, unsigned flags);
+
+/* Non-local means with patch radius `patch` and search radius `search`
+ * on each of `channels` interleaved channels (1: a Plane; 3: an Image3
+ * denoised per channel as channel()/nlm()/merge3() would).
+ * Replaces nlm, enhance.rs:36-72. */
+int dsgpu_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h_param, int search,
+              int patch, float* out, unsigned flags);
+
+/* The detail path in one call: u16 raw -> normalise -> RCD -> per-channel NLM.
+ * Equivalent to load_raw's normalisation (decode.rs:292-306), demosaic(Full)
+ * (demosaic.rs:20-27) and nlm() on each channel (enhance.rs:36-72).
+ * out_clip (w*h) may be NULL. The demosaiced intermediate lives in context
+ * scratch. */
+int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t pitch_elems,
+                      const uint8_t cfa[4], float black, const float white[3], const float mul[3],
+                      float h_param, int search, int patch, float* out_rgb, float* out_clip, unsigned flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSGPU_H */

@@ -1,0 +1,500 @@
+// dsref — CPU oracle for the RCD demosaic + NLM denoise path.
+//
+// TEST INFRASTRUCTURE ONLY. This library is the checker: the GPU library
+// never links, loads or calls it. Only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference arm of bench.py may use it.
+//
+// It restates, in C++, the CPU code of darkslide-core (Rust) for this path,
+// operation for operation and in the same evaluation order, so that an f32
+// build reproduces the reference bit for bit wherever the reference itself is
+// deterministic:
+//   decode.rs:264-306   CFA normalisation (u16 -> (raw-black)/max(white-black,1))
+//   demosaic.rs:17      CLIP = 0.995
+//   demosaic.rs:20-27   demosaic(Full, Bayer) = rcd_bayer + clip_plane
+//   demosaic.rs:31-42   clip_plane
+//   demosaic.rs:45-87   superpixel (Draft quality, Bayer 2x2)
+//   demosaic.rs:90-124  mhc_bayer
+//   demosaic.rs:147-344 rcd_bayer
+//   image.rs:269-313    box_blur (separable running sums, clamped edges)
+//   enhance.rs:10-32    estimate_noise
+//   enhance.rs:36-72    nlm (offset chunks reduced in chunk order)
+// Every kernel is a template on the arithmetic type; the double instantiation
+// is the FP64 oracle.
+//
+// Parity pin: the reference is Rust and no Rust toolchain exists here, so the
+// reference itself cannot be run. Its own tests (demosaic.rs:514-537,
+// enhance.rs:137-151, image.rs:455-462) are property tests and hold no golden
+// vectors; tests/test_oracle.py restates them against this oracle, and a
+// second, independent numpy restatement (tests/np_restate.py) cross-checks it.
+// Exact-value parity with the Rust binary is therefore UNPINNED.
+//
+// Build with -ffp-contract=off: Rust never fuses a*b+c, so neither may we.
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+template <typename T> inline T tmax(T a, T b) { return std::fmax(a, b); }  // Rust f32::max (NaN-ignoring)
+template <typename T> inline T tabs(T a) { return std::fabs(a); }
+inline float texp(float v) { return expf(v); }
+inline double texp(double v) { return std::exp(v); }
+
+struct Pat {
+  uint8_t c[4];
+  // decode.rs:26-28 color_at(x,y) = colors[(y % 2) * 2 + x % 2] for a 2x2 pattern
+  inline int at(size_t x, size_t y) const { return c[(y & 1) * 2 + (x & 1)]; }
+};
+
+inline long clampi(long v, long lo, long hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ---------------------------------------------------------------- clip_plane
+// demosaic.rs:31-42: 3x3 clamped-edge max of [v >= CLIP]
+template <typename T>
+void clip_plane(const float* cfa, size_t w, size_t h, T* out) {
+  const float CLIP = 0.995f;  // demosaic.rs:17
+  std::vector<T> raw(w * h);
+  for (size_t i = 0; i < w * h; i++) raw[i] = cfa[i] >= CLIP ? T(1) : T(0);
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < (long)h; y++)
+    for (long x = 0; x < (long)w; x++) {
+      T m = 0;
+      for (long dy = -1; dy <= 1; dy++)
+        for (long dx = -1; dx <= 1; dx++) {
+          long sx = clampi(x + dx, 0, (long)w - 1), sy = clampi(y + dy, 0, (long)h - 1);
+          m = tmax(m, raw[sy * w + sx]);
+        }
+      out[y * w + x] = m;
+    }
+}
+
+// ---------------------------------------------------------------- superpixel
+// demosaic.rs:45-87 for a Bayer pattern (t = 2): output (w/2, h/2).
+void superpixel(const float* cfa, size_t w, size_t h, Pat pat, const float mul[3], float* out, float* clip) {
+  const float CLIP = 0.995f;
+  const size_t ow = w / 2, oh = h / 2;
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < (long)oh; y++)
+    for (size_t x = 0; x < ow; x++) {
+      float acc[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+      unsigned n[3] = {0, 0, 0}, clipped = 0;
+      for (size_t dy = 0; dy < 2; dy++)
+        for (size_t dx = 0; dx < 2; dx++) {
+          const size_t sx = x * 2 + dx, sy = y * 2 + dy;
+          const int c = pat.at(sx, sy);
+          const float v = cfa[sy * w + sx];
+          if (v >= CLIP) clipped++;
+          mx[c] = std::fmax(mx[c], v);
+          acc[c] += v;
+          n[c]++;
+        }
+      for (int c = 0; c < 3; c++) {
+        const float v = mx[c] >= CLIP ? mx[c] : (n[c] > 0 ? acc[c] / (float)n[c] : 0.0f);
+        out[(y * ow + x) * 3 + c] = v * mul[c];
+      }
+      clip[y * ow + x] = std::fmin((float)clipped / 4.0f * 2.0f, 1.0f);
+    }
+}
+
+// ----------------------------------------------------------------- mhc_bayer
+// demosaic.rs:90-124. Reads data*mul with clamp-to-edge, NOT clamped at 0.
+template <typename T>
+void mhc_bayer(const float* cfa, size_t w, size_t h, Pat pat, const T mul[3], T* out /*w*h*3*/) {
+  auto at = [&](long x, long y) -> T {
+    x = clampi(x, 0, (long)w - 1);
+    y = clampi(y, 0, (long)h - 1);
+    return T(cfa[y * w + x]) * mul[pat.at(x, y)];
+  };
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < (long)h; y++)
+    for (long x = 0; x < (long)w; x++) {
+      const int c = pat.at(x, y);
+      const T v = at(x, y);
+      auto p = [&](long dx, long dy) { return at(x + dx, y + dy); };
+      const T g_at_rb = (T(4) * v + T(2) * (p(0, -1) + p(-1, 0) + p(1, 0) + p(0, 1)) -
+                         (p(0, -2) + p(-2, 0) + p(2, 0) + p(0, 2))) / T(8);
+      const T rb_g_row = (T(5) * v + T(4) * (p(-1, 0) + p(1, 0)) -
+                          (p(-2, 0) + p(2, 0) + p(-1, -1) + p(1, -1) + p(-1, 1) + p(1, 1)) +
+                          T(0.5) * (p(0, -2) + p(0, 2))) / T(8);
+      const T rb_g_col = (T(5) * v + T(4) * (p(0, -1) + p(0, 1)) -
+                          (p(0, -2) + p(0, 2) + p(-1, -1) + p(1, -1) + p(-1, 1) + p(1, 1)) +
+                          T(0.5) * (p(-2, 0) + p(2, 0))) / T(8);
+      const T rb_diag = (T(6) * v + T(2) * (p(-1, -1) + p(1, -1) + p(-1, 1) + p(1, 1)) -
+                         T(1.5) * (p(0, -2) + p(-2, 0) + p(2, 0) + p(0, 2))) / T(8);
+      T o0, o1, o2;
+      if (c == 1) {
+        const int row_c = pat.at(x + 1, y);  // demosaic.rs:116
+        if (row_c == 0) { o0 = rb_g_row; o1 = v; o2 = rb_g_col; }
+        else            { o0 = rb_g_col; o1 = v; o2 = rb_g_row; }
+      } else if (c == 0) { o0 = v; o1 = g_at_rb; o2 = rb_diag; }
+      else               { o0 = rb_diag; o1 = g_at_rb; o2 = v; }
+      T* o = out + (y * w + x) * 3;
+      o[0] = tmax(o0, T(0));
+      o[1] = tmax(o1, T(0));
+      o[2] = tmax(o2, T(0));
+    }
+}
+
+// ----------------------------------------------------------------- rcd_bayer
+// demosaic.rs:147-344, pass for pass.
+template <typename T>
+void rcd_bayer(const float* cfa, size_t w, size_t h, Pat pat, const T mul[3], T* out /*w*h*3*/) {
+  if (w < 16 || h < 16) {  // demosaic.rs:149-151
+    mhc_bayer<T>(cfa, w, h, pat, mul, out);
+    return;
+  }
+  const size_t n = w * h;
+  auto fc = [&](size_t x, size_t y) { return pat.at(x, y); };
+  std::vector<T> c(n);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; i++) c[i] = tmax(T(cfa[i]) * mul[fc(i % w, i / w)], T(0));  // :154
+  const T eps = T(1e-5f);  // :155 (an f32 literal in the reference)
+  auto sq = [](T v) { return v * v; };
+  const long w1 = w, w2 = 2 * w, w3 = 3 * w, w4 = 4 * w;
+  const size_t border = 4;
+
+  // step 1 (:160-184)
+  std::vector<T> bv(n, T(0)), bh(n, T(0));
+#pragma omp parallel for schedule(static)
+  for (long y = 3; y < (long)h - 3; y++)
+    for (size_t x = 3; x < w - 3; x++) {
+      const long i = y * w + x;
+      bv[i] = sq((c[i - w3] - c[i - w1] - c[i + w1] + c[i + w3]) - T(3) * (c[i - w2] + c[i + w2]) + T(6) * c[i]);
+      bh[i] = sq((c[i - 3] - c[i - 1] - c[i + 1] + c[i + 3]) - T(3) * (c[i - 2] + c[i + 2]) + T(6) * c[i]);
+    }
+  std::vector<T> vh(n, T(0.5));
+#pragma omp parallel for schedule(static)
+  for (long y = border; y < (long)(h - border); y++)
+    for (size_t x = border; x < w - border; x++) {
+      const long i = y * w + x;
+      const T vs = tmax(bv[i - w1] + bv[i] + bv[i + w1], eps);
+      const T hs = tmax(bh[i - 1] + bh[i] + bh[i + 1], eps);
+      vh[i] = vs / (vs + hs);
+    }
+  std::vector<T>().swap(bv);
+  std::vector<T>().swap(bh);
+
+  // step 2 (:188-201)
+  std::vector<T> lpf(n, T(0));
+#pragma omp parallel for schedule(static)
+  for (long y = 2; y < (long)h - 2; y++)
+    for (size_t x = 2; x < w - 2; x++) {
+      if (fc(x, y) == 1) continue;
+      const long i = y * w + x;
+      lpf[i] = c[i] + T(0.5) * (c[i - w1] + c[i + w1] + c[i - 1] + c[i + 1]) +
+               T(0.25) * (c[i - w1 - 1] + c[i - w1 + 1] + c[i + w1 - 1] + c[i + w1 + 1]);
+    }
+
+  // r/g/b init (:203-214)
+  std::vector<T> base(n * 3);
+  mhc_bayer<T>(cfa, w, h, pat, mul, base.data());
+  std::vector<T> r(n), g(n), b(n);
+  for (size_t i = 0; i < n; i++) {
+    const int col = fc(i % w, i / w);
+    r[i] = col == 0 ? c[i] : base[i * 3 + 0];
+    g[i] = col == 1 ? c[i] : base[i * 3 + 1];
+    b[i] = col == 2 ? c[i] : base[i * 3 + 2];
+  }
+  std::vector<T>().swap(base);
+
+  auto disc = [&](const std::vector<T>& d, long i) -> T {  // :216-220
+    const T central = d[i];
+    const T neigh = T(0.25) * (d[i - w1 - 1] + d[i - w1 + 1] + d[i + w1 - 1] + d[i + w1 + 1]);
+    return tabs(T(0.5) - central) < tabs(T(0.5) - neigh) ? neigh : central;
+  };
+
+  // step 3: green at R/B (:222-245)
+#pragma omp parallel for schedule(static)
+  for (long y = border; y < (long)(h - border); y++)
+    for (size_t x = border; x < w - border; x++) {
+      if (fc(x, y) == 1) continue;
+      const long i = y * w + x;
+      const T vd = disc(vh, i);
+      const T n_grad = eps + tabs(c[i - w1] - c[i + w1]) + tabs(c[i] - c[i - w2]) + tabs(c[i - w1] - c[i - w3]) + tabs(c[i - w2] - c[i - w4]);
+      const T s_grad = eps + tabs(c[i - w1] - c[i + w1]) + tabs(c[i] - c[i + w2]) + tabs(c[i + w1] - c[i + w3]) + tabs(c[i + w2] - c[i + w4]);
+      const T w_grad = eps + tabs(c[i - 1] - c[i + 1]) + tabs(c[i] - c[i - 2]) + tabs(c[i - 1] - c[i - 3]) + tabs(c[i - 2] - c[i - 4]);
+      const T e_grad = eps + tabs(c[i - 1] - c[i + 1]) + tabs(c[i] - c[i + 2]) + tabs(c[i + 1] - c[i + 3]) + tabs(c[i + 2] - c[i + 4]);
+      const T n_est = c[i - w1] * T(2) * lpf[i] / (eps + lpf[i] + lpf[i - w2]);
+      const T s_est = c[i + w1] * T(2) * lpf[i] / (eps + lpf[i] + lpf[i + w2]);
+      const T w_est = c[i - 1] * T(2) * lpf[i] / (eps + lpf[i] + lpf[i - 2]);
+      const T e_est = c[i + 1] * T(2) * lpf[i] / (eps + lpf[i] + lpf[i + 2]);
+      const T v_est = (s_grad * n_est + n_grad * s_est) / (n_grad + s_grad);
+      const T h_est = (w_grad * e_est + e_grad * w_est) / (e_grad + w_grad);
+      g[i] = tmax(vd * h_est + (T(1) - vd) * v_est, T(0));
+    }
+  std::vector<T>().swap(lpf);
+
+  // step 4.1/4.2 (:248-272)
+  std::vector<T> bp(n, T(0)), bq(n, T(0));
+#pragma omp parallel for schedule(static)
+  for (long y = 3; y < (long)h - 3; y++)
+    for (size_t x = 3; x < w - 3; x++) {
+      const long i = y * w + x;
+      bp[i] = sq((c[i - w3 - 3] - c[i - w1 - 1] - c[i + w1 + 1] + c[i + w3 + 3]) - T(3) * (c[i - w2 - 2] + c[i + w2 + 2]) + T(6) * c[i]);
+      bq[i] = sq((c[i - w3 + 3] - c[i - w1 + 1] - c[i + w1 - 1] + c[i + w3 - 3]) - T(3) * (c[i - w2 + 2] + c[i + w2 - 2]) + T(6) * c[i]);
+    }
+  std::vector<T> pq(n, T(0.5));
+#pragma omp parallel for schedule(static)
+  for (long y = border; y < (long)(h - border); y++)
+    for (size_t x = border; x < w - border; x++) {
+      const long i = y * w + x;
+      const T ps = tmax(bp[i - w1 - 1] + bp[i] + bp[i + w1 + 1], eps);
+      const T qs = tmax(bq[i - w1 + 1] + bq[i] + bq[i + w1 - 1], eps);
+      pq[i] = ps / (ps + qs);
+    }
+  std::vector<T>().swap(bp);
+  std::vector<T>().swap(bq);
+
+  // step 4.3: R at B and B at R (:276-308); chan is the pre-pass clone
+  auto pass43 = [&](std::vector<T>& target, int at_color) {
+    const std::vector<T> cc = target;
+#pragma omp parallel for schedule(static)
+    for (long y = border; y < (long)(h - border); y++)
+      for (size_t x = border; x < w - border; x++) {
+        if (fc(x, y) != at_color) continue;
+        const long i = y * w + x;
+        const T pd = disc(pq, i);
+        const T nw_g = eps + tabs(cc[i - w1 - 1] - cc[i + w1 + 1]) + tabs(cc[i - w1 - 1] - cc[i - w3 - 3]) + tabs(g[i] - g[i - w2 - 2]);
+        const T ne_g = eps + tabs(cc[i - w1 + 1] - cc[i + w1 - 1]) + tabs(cc[i - w1 + 1] - cc[i - w3 + 3]) + tabs(g[i] - g[i - w2 + 2]);
+        const T sw_g = eps + tabs(cc[i + w1 - 1] - cc[i - w1 + 1]) + tabs(cc[i + w1 - 1] - cc[i + w3 - 3]) + tabs(g[i] - g[i + w2 - 2]);
+        const T se_g = eps + tabs(cc[i + w1 + 1] - cc[i - w1 - 1]) + tabs(cc[i + w1 + 1] - cc[i + w3 + 3]) + tabs(g[i] - g[i + w2 + 2]);
+        const T nw_e = cc[i - w1 - 1] - g[i - w1 - 1];
+        const T ne_e = cc[i - w1 + 1] - g[i - w1 + 1];
+        const T sw_e = cc[i + w1 - 1] - g[i + w1 - 1];
+        const T se_e = cc[i + w1 + 1] - g[i + w1 + 1];
+        const T p_est = (nw_g * se_e + se_g * nw_e) / (nw_g + se_g);
+        const T q_est = (ne_g * sw_e + sw_g * ne_e) / (ne_g + sw_g);
+        target[i] = tmax(g[i] + (T(1) - pd) * p_est + pd * q_est, T(0));
+      }
+  };
+  pass43(r, 2);
+  pass43(b, 0);
+
+  // step 4.4: R and B at G (:310-341); chan is the post-4.3 clone
+  auto pass44 = [&](std::vector<T>& target) {
+    const std::vector<T> cc = target;
+#pragma omp parallel for schedule(static)
+    for (long y = border; y < (long)(h - border); y++)
+      for (size_t x = border; x < w - border; x++) {
+        if (fc(x, y) != 1) continue;
+        const long i = y * w + x;
+        const T vd = disc(vh, i);
+        const T n_g = eps + tabs(g[i] - g[i - w2]) + tabs(cc[i - w1] - cc[i + w1]) + tabs(cc[i - w1] - cc[i - w3]);
+        const T s_g = eps + tabs(g[i] - g[i + w2]) + tabs(cc[i + w1] - cc[i - w1]) + tabs(cc[i + w1] - cc[i + w3]);
+        const T w_g = eps + tabs(g[i] - g[i - 2]) + tabs(cc[i - 1] - cc[i + 1]) + tabs(cc[i - 1] - cc[i - 3]);
+        const T e_g = eps + tabs(g[i] - g[i + 2]) + tabs(cc[i + 1] - cc[i - 1]) + tabs(cc[i + 1] - cc[i + 3]);
+        const T n_e = cc[i - w1] - g[i - w1];
+        const T s_e = cc[i + w1] - g[i + w1];
+        const T w_e = cc[i - 1] - g[i - 1];
+        const T e_e = cc[i + 1] - g[i + 1];
+        const T v_est = (n_g * s_e + s_g * n_e) / (n_g + s_g);
+        const T h_est = (e_g * w_e + w_g * e_e) / (e_g + w_g);
+        target[i] = tmax(g[i] + (T(1) - vd) * v_est + vd * h_est, T(0));
+      }
+  };
+  pass44(r);
+  pass44(b);
+
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; i++) {
+    out[i * 3 + 0] = r[i];
+    out[i * 3 + 1] = g[i];
+    out[i * 3 + 2] = b[i];
+  }
+}
+
+// ------------------------------------------------------------------ box_blur
+// image.rs:269-313: horizontal running sum per row, then vertical running sum
+// per 64-column strip; each pass multiplies by 1/(2r+1).
+template <typename T>
+void box_blur(const T* p, size_t w, size_t h, size_t r, T* out) {
+  if (r == 0 || w == 0 || h == 0) {
+    std::memcpy(out, p, w * h * sizeof(T));
+    return;
+  }
+  const T norm = T(1) / T(2 * r + 1);
+  std::vector<T> tmp(w * h);
+  const long R = (long)r;
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < (long)h; y++) {
+    const T* row = p + y * w;
+    auto at = [&](long i) { return row[clampi(i, 0, (long)w - 1)]; };
+    T acc = 0;
+    for (long i = -R; i <= R; i++) acc += at(i);
+    T* o = tmp.data() + y * w;
+    for (long x = 0; x < (long)w; x++) {
+      o[x] = acc * norm;
+      acc += at(x + R + 1) - at(x - R);
+    }
+  }
+  const size_t STRIP = 64;
+  const long nstrips = (long)((w + STRIP - 1) / STRIP);
+#pragma omp parallel for schedule(static)
+  for (long s = 0; s < nstrips; s++) {
+    const size_t x0 = s * STRIP, x1 = std::min(x0 + STRIP, w), sw = x1 - x0;
+    std::vector<T> acc(sw, T(0));
+    auto at = [&](long y, size_t x) { return tmp[clampi(y, 0, (long)h - 1) * w + x]; };
+    for (long i = -R; i <= R; i++)
+      for (size_t k = 0; k < sw; k++) acc[k] += at(i, x0 + k);
+    for (long y = 0; y < (long)h; y++)
+      for (size_t k = 0; k < sw; k++) {
+        out[y * w + x0 + k] = acc[k] * norm;
+        acc[k] += at(y + R + 1, x0 + k) - at(y - R, x0 + k);
+      }
+  }
+}
+
+// ----------------------------------------------------------------------- nlm
+// enhance.rs:36-72. Offsets in (dy outer, dx inner) order are split into
+// chunks of ceil(N / nthreads); each chunk accumulates its own a/s planes and
+// the chunks are summed in order, exactly as the rayon code does for a pool
+// of `nthreads` threads.
+template <typename T>
+void nlm(const T* p, size_t w, size_t hh, T h_param, long search, size_t patch, int nthreads, T* out) {
+  const size_t n = w * hh;
+  const T h2 = tmax(h_param * h_param, T(1e-12f));
+  std::vector<std::pair<long, long>> offs;
+  for (long dy = -search; dy <= search; dy++)
+    for (long dx = -search; dx <= search; dx++) offs.push_back({dx, dy});
+  const size_t nt = nthreads > 0 ? (size_t)nthreads : 1;
+  const size_t csz = std::max<size_t>((offs.size() + nt - 1) / nt, 1);
+  const size_t nchunks = (offs.size() + csz - 1) / csz;
+  std::vector<std::vector<T>> pa(nchunks), ps(nchunks);
+  auto get_clamped = [&](long x, long y) {
+    return p[clampi(y, 0, (long)hh - 1) * w + clampi(x, 0, (long)w - 1)];
+  };
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long ci = 0; ci < (long)nchunks; ci++) {
+    std::vector<T> a(n, T(0)), s(n, T(0)), diff(n), dist(n);
+    const size_t o0 = ci * csz, o1 = std::min(o0 + csz, offs.size());
+    for (size_t oi = o0; oi < o1; oi++) {
+      const long dx = offs[oi].first, dy = offs[oi].second;
+      for (long y = 0; y < (long)hh; y++)
+        for (long x = 0; x < (long)w; x++) {
+          const T q = get_clamped(x + dx, y + dy);
+          const T d = p[y * w + x] - q;
+          diff[y * w + x] = d * d;
+        }
+      // box_blur is itself OpenMP-parallel; nested regions run serially here
+      box_blur<T>(diff.data(), w, hh, patch, dist.data());
+      for (long y = 0; y < (long)hh; y++)
+        for (long x = 0; x < (long)w; x++) {
+          const size_t i = y * w + x;
+          const T wt = texp(-(dist[i] / h2));
+          a[i] += wt * get_clamped(x + dx, y + dy);
+          s[i] += wt;
+        }
+    }
+    pa[ci].swap(a);
+    ps[ci].swap(s);
+  }
+  std::vector<T> acc(n, T(0)), wsum(n, T(0));
+  for (size_t ci = 0; ci < nchunks; ci++)
+    for (size_t i = 0; i < n; i++) {
+      acc[i] += pa[ci][i];
+      wsum[i] += ps[ci][i];
+    }
+  for (size_t i = 0; i < n; i++) out[i] = acc[i] / tmax(wsum[i], T(1e-12f));
+}
+
+// ------------------------------------------------------------ estimate_noise
+// enhance.rs:10-32
+float estimate_noise(const float* p, size_t w, size_t h) {
+  const size_t step = std::max<size_t>((w * h) / 200000, 1);
+  std::vector<float> v;
+  for (size_t i = 0; i < w * h; i += step) {
+    const size_t x = i % w, y = i / w;
+    if (x < 1 || y < 1 || x + 1 >= w || y + 1 >= h) continue;
+    const float c = p[i];
+    const float lap = 4.0f * c - p[i - 1] - p[i + 1] - p[i - w] - p[i + w];
+    v.push_back(std::fabs(lap));
+  }
+  if (v.empty()) return 0.0f;
+  const size_t mid = v.size() / 2;
+  std::nth_element(v.begin(), v.begin() + mid, v.end());
+  return v[mid] / 0.6745f / std::sqrt(20.0f);
+}
+
+}  // namespace
+
+extern "C" {
+
+int dsref_omp_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void dsref_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+// decode.rs:292-306 (integer raws): v = (raw - black) / max(white[c] - black, 1)
+void dsref_normalize_u16(const uint16_t* raw, int w, int h, size_t pitch, const uint8_t cfa[4], float black,
+                         const float white[3], float* out) {
+  Pat pat;
+  std::memcpy(pat.c, cfa, 4);
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < h; y++)
+    for (long x = 0; x < w; x++) {
+      const int c = pat.at(x, y);
+      const float raw_v = (float)raw[y * pitch + x];
+      out[y * w + x] = (raw_v - black) / std::fmax(white[c] - black, 1.0f);
+    }
+}
+
+void dsref_clip_plane_f32(const float* cfa, int w, int h, float* out) { clip_plane<float>(cfa, w, h, out); }
+
+void dsref_mhc_f32(const float* cfa, int w, int h, const uint8_t pat[4], const float mul[3], float* out) {
+  Pat p;
+  std::memcpy(p.c, pat, 4);
+  mhc_bayer<float>(cfa, w, h, p, mul, out);
+}
+
+void dsref_superpixel_f32(const float* cfa, int w, int h, const uint8_t pat[4], const float mul[3], float* out,
+                          float* clip) {
+  Pat p;
+  std::memcpy(p.c, pat, 4);
+  superpixel(cfa, w, h, p, mul, out, clip);
+}
+
+void dsref_rcd_f32(const float* cfa, int w, int h, const uint8_t pat[4], const float mul[3], float* out) {
+  Pat p;
+  std::memcpy(p.c, pat, 4);
+  rcd_bayer<float>(cfa, w, h, p, mul, out);
+}
+
+void dsref_rcd_f64(const float* cfa, int w, int h, const uint8_t pat[4], const float mul[3], double* out) {
+  Pat p;
+  std::memcpy(p.c, pat, 4);
+  const double m[3] = {mul[0], mul[1], mul[2]};
+  rcd_bayer<double>(cfa, w, h, p, m, out);
+}
+
+void dsref_box_blur_f32(const float* in, int w, int h, int r, float* out) { box_blur<float>(in, w, h, r, out); }
+void dsref_box_blur_f64(const double* in, int w, int h, int r, double* out) { box_blur<double>(in, w, h, r, out); }
+
+void dsref_nlm_f32(const float* in, int w, int h, float h_param, int search, int patch, int nthreads, float* out) {
+  nlm<float>(in, w, h, h_param, search, patch, nthreads, out);
+}
+
+void dsref_nlm_f64(const double* in, int w, int h, double h_param, int search, int patch, int nthreads, double* out) {
+  nlm<double>(in, w, h, h_param, search, patch, nthreads, out);
+}
+
+float dsref_estimate_noise_f32(const float* p, int w, int h) { return estimate_noise(p, w, h); }
+
+}  // extern "C"

@@ -1,0 +1,123 @@
+"""The CPU oracle: the reference's own property tests, a cross-check
+against an independent numpy restatement, and the committed golden fixtures."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import np_restate as R
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+PATTERNS = [[0, 1, 1, 2], [2, 1, 1, 0], [1, 0, 2, 1], [1, 2, 0, 1]]
+
+
+def lcg_noise(n):
+    """enhance.rs:139-143: seed = seed*1664525 + 1013904223; (seed>>8)/2^24 - 0.5"""
+    seed = 1
+    out = np.empty(n, np.float32)
+    for i in range(n):
+        seed = (seed * 1664525 + 1013904223) & 0xFFFFFFFF
+        out[i] = np.float32(seed >> 8) / np.float32(1 << 24) - np.float32(0.5)
+    return out
+
+
+def test_flat_field_is_preserved(oracle):
+    """demosaic.rs:514-521: 32x32 RGGB flat [0.2,0.4,0.3], mul 1, Full quality."""
+    pat = [0, 1, 1, 2]
+    v = np.array([0.2, 0.4, 0.3], np.float32)
+    yy, xx = np.mgrid[0:32, 0:32]
+    col = np.asarray(pat).reshape(2, 2)[yy % 2, xx % 2]
+    cfa = v[col].astype(np.float32)
+    rgb = oracle.rcd(cfa, pat, [1, 1, 1])
+    p = rgb[16, 16]
+    assert np.all(np.abs(p - v) < 1e-4), p
+
+
+def test_nlm_reduces_noise(oracle):
+    """enhance.rs:137-151 with the reference's own LCG noise."""
+    p = np.where(np.arange(64)[None, :] < 32, 0.3, 0.7).astype(np.float32) * np.ones((64, 1), np.float32)
+    noisy = (p.ravel() + lcg_noise(64 * 64) * np.float32(0.1)).reshape(64, 64).astype(np.float32)
+    s = oracle.estimate_noise(noisy)
+    assert 0.01 < s < 0.06, s
+    d = oracle.nlm(noisy, s * 1.5, 3, 1)
+    err = lambda q: float(((q - p) ** 2).sum())
+    assert err(d) < err(noisy) * 0.5
+
+
+def test_box_blur_preserves_constant(oracle):
+    """image.rs:455-459 (box part)."""
+    p = np.full((23, 37), 0.5, np.float32)
+    b = oracle.box_blur(p, 4)
+    assert np.all(np.abs(b - 0.5) < 1e-5)
+
+
+@pytest.mark.parametrize("pat", PATTERNS)
+@pytest.mark.parametrize("hw", [(16, 16), (17, 33), (40, 37), (12, 20), (64, 48)])
+def test_oracle_matches_numpy_restatement_rcd(oracle, pat, hw):
+    rng = np.random.default_rng(hash((tuple(pat), hw)) & 0xFFFF)
+    cfa = rng.uniform(-0.05, 1.05, hw).astype(np.float32)
+    mul = [2.0, 1.0, 1.4285714]
+    a = oracle.rcd(cfa, pat, mul)
+    with np.errstate(all="ignore"):
+        b = R.rcd(cfa, pat, mul)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(oracle.clip_plane(cfa), R.clip_plane(cfa))
+    np.testing.assert_array_equal(oracle.mhc(cfa, pat, mul), R.mhc(cfa, pat, mul))
+
+
+@pytest.mark.parametrize("r", [0, 1, 3, 5])
+def test_oracle_matches_numpy_restatement_box(oracle, r):
+    p = np.random.default_rng(r).uniform(0, 1, (29, 41)).astype(np.float32)
+    np.testing.assert_array_equal(oracle.box_blur(p, r), R.box_blur(p, r))
+
+
+@pytest.mark.parametrize("nthreads", [1, 3, 8])
+@pytest.mark.parametrize("sp", [(3, 1), (2, 0), (0, 2), (4, 3), (-1, 1)])
+def test_oracle_matches_numpy_restatement_nlm(oracle, nthreads, sp):
+    s, p = sp
+    img = np.random.default_rng(7).uniform(0, 1, (23, 31)).astype(np.float32)
+    a = oracle.nlm(img, 0.1, s, p, nthreads=nthreads)
+    b = R.nlm(img, 0.1, s, p, nthreads=nthreads)
+    # identical up to the last ulp of exp (glibc expf vs exp rounded from f64)
+    np.testing.assert_allclose(a, b, rtol=4e-7, atol=1e-7)
+
+
+def test_nlm_edge_cases(oracle):
+    img = np.random.default_rng(3).uniform(0, 1, (9, 11)).astype(np.float32)
+    assert np.all(oracle.nlm(img, 0.1, -1, 1) == 0)  # empty offset set -> 0/1e-12
+    np.testing.assert_array_equal(oracle.nlm(img, 0.1, 0, 3), img)  # centre weight only
+
+
+def test_fp64_oracle_close_to_fp32(oracle):
+    rng = np.random.default_rng(11)
+    cfa = rng.uniform(0, 1, (40, 48)).astype(np.float32)
+    a32 = oracle.rcd(cfa, [0, 1, 1, 2], [2, 1, 1.4])
+    a64 = oracle.rcd(cfa, [0, 1, 1, 2], [2, 1, 1.4], fp64=True)
+    assert np.abs(a32 - a64).max() < 1e-4
+    p = a32[..., 1].copy()
+    n32 = oracle.nlm(p, 0.05, 3, 1)
+    n64 = oracle.nlm(p.astype(np.float64), 0.05, 3, 1, fp64=True)
+    assert np.abs(n32 - n64).max() < 1e-5
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))), ids=os.path.basename)
+def test_golden_fixtures(oracle, path):
+    z = np.load(path)
+    name = os.path.basename(path)
+    if name.startswith("nlm_"):
+        out = oracle.nlm(z["inp"], float(z["h"]), int(z["search"]), int(z["patch"]), nthreads=1)
+        np.testing.assert_array_equal(out, z["out"])
+    elif name.startswith("box_"):
+        np.testing.assert_array_equal(oracle.box_blur(z["inp"], int(z["r"])), z["out"])
+    else:
+        cfa = oracle.normalize_u16(z["raw"], z["pattern"], float(z["black"]), z["white"])
+        np.testing.assert_array_equal(cfa, z["cfa"])
+        np.testing.assert_array_equal(oracle.rcd(cfa, z["pattern"], z["mul"]), z["rgb"])
+        np.testing.assert_array_equal(oracle.clip_plane(cfa), z["clip"])
+        # the integer pre-stage against its closed form in float64 then rounded
+        col = np.asarray(z["pattern"]).reshape(2, 2)
+        yy, xx = np.mgrid[0:cfa.shape[0], 0:cfa.shape[1]]
+        wc = z["white"][col[yy % 2, xx % 2]]
+        ref = ((z["raw"].astype(np.float32) - z["black"]) / np.maximum(wc - z["black"], np.float32(1))).astype(np.float32)
+        np.testing.assert_array_equal(cfa, ref)
