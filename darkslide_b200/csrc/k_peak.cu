@@ -59,7 +59,7 @@ cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, do
   cudaEventCreate(&a);
   cudaEventCreate(&b);
   const int blocks = sms * 8, threads = 256;
-  const int it_f = 4096, it_e = 512;
+  const int it_f = 256, it_e = 1024;
   float ms = 0.f;
   for (int rep = 0; rep < 2; rep++) {  // first rep warms up
     cudaEventRecord(a, st);
