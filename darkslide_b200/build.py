@@ -31,6 +31,7 @@ UNITS = [
     ("k_nlm.cu", []),
     ("k_peak.cu", []),
     ("api.cu", []),
+    ("noalloc.cu", []),
 ]
 
 

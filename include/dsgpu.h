@@ -138,6 +138,33 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
                       const uint8_t cfa[4], float black, const float white[3], const float mul[3],
                       float h_param, int search, int patch, float* out_rgb, float* out_clip, unsigned flags);
 
+/* The same detail path for callers that cannot allocate device memory.
+ * No counterpart in the reference. It is for callers that manage every byte
+ * of device memory themselves (a pool or a framework's caching allocator
+ * that must not be bypassed) or that run where cudaMalloc is not allowed or
+ * would stall the device. dsgpu_develop_u16 allocates its demosaiced
+ * intermediate in context scratch; this call instead uses one fixed array
+ * of DSGPU_NOALLOC_SCRATCH_BYTES inside the library's device image, which
+ * every GPU that loads the library holds until the process exits. It calls
+ * no cudaMalloc, cudaFree or other allocating routine.
+ *  - All pointers are device memory of the current device; DSGPU_HOST is
+ *    rejected (DSGPU_ERR_ARG). Work goes on `cuda_stream` (NULL: the legacy
+ *    default stream); the call synchronises it unless DSGPU_ASYNC is given.
+ *  - Frames above DSGPU_NOALLOC_MAX_PIXELS (w*h) are rejected with
+ *    DSGPU_ERR_SIZE.
+ *  - The first call on a device looks up the array's device address (once per
+ *    device, with that device current); make that first call before any
+ *    stream capture.
+ *  - Every call shares the array and it keeps the last call's contents (each
+ *    call overwrites what it reads). Calls that overlap on the GPU race on it:
+ *    serialise them. */
+#define DSGPU_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define DSGPU_NOALLOC_MAX_PIXELS (1 << 20) /* 16 B per pixel: RGB intermediate + normalised CFA */
+int dsgpu_develop_u16_noalloc(void* cuda_stream, const uint16_t* raw, int w, int h, size_t pitch_elems,
+                              const uint8_t cfa[4], float black, const float white[3], const float mul[3],
+                              float h_param, int search, int patch, float* out_rgb, float* out_clip,
+                              unsigned flags);
+
 #ifdef __cplusplus
 }
 #endif
