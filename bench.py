@@ -286,7 +286,7 @@ def run_ours(args):
     e2e = ws * W * H * k_e2e / t_e2e / 1e6
 
     if rank == 0:
-        fl, ex2 = ctx.measure_peaks()
+        fl, ex2, fl2 = ctx.measure_peaks()
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -319,7 +319,7 @@ def run_ours(args):
                 "traffic": (traffic or {}).get("nlm_bytes_per_launch"),
                 "algorithmic": f"{updates:.4g} exp per launch (W*H*3*(2S+1)^2, one exp per pixel, channel and offset)",
                 "peak_source": "ex2.approx throughput microbenchmark on this GPU (dsgpu_measure_peaks)",
-                "launch_ms": nlm_launch_ms, "fp32_peak_tflops": fl / 1e12,
+                "launch_ms": nlm_launch_ms, "fp32_peak_tflops": fl / 1e12, "fp32x2_peak_tflops": fl2 / 1e12,
             },
             "roofline_hbm": {
                 "kernel": "rcd_tile_kernel<SrcU16>", "bound": "hbm", "achieved": rcd_bytes / (dem_launch_ms * 1e-3) / 1e9,

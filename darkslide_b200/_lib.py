@@ -99,7 +99,7 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_profile.argtypes = [vp, i]
             L.dsgpu_stage_ms.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i)]
             L.dsgpu_launch_count.argtypes = [vp]
-            L.dsgpu_measure_peaks.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+            L.dsgpu_measure_peaks.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 3
             L.dsgpu_scene_render_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
             L.dsgpu_scene_truth_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
             L.dsgpu_scene_render.argtypes = [vp, ctypes.POINTER(SceneDesc), vp, u]
@@ -148,10 +148,12 @@ class Context:
     def launch_count(self) -> int:
         return int(lib().dsgpu_launch_count(self.handle))
 
-    def measure_peaks(self) -> tuple[float, float]:
-        f, e = ctypes.c_double(), ctypes.c_double()
-        self.check(lib().dsgpu_measure_peaks(self.handle, ctypes.byref(f), ctypes.byref(e)), "dsgpu_measure_peaks")
-        return f.value, e.value
+    def measure_peaks(self) -> tuple[float, float, float]:
+        """(FP32 FMA FLOP/s, ex2/s, packed f32x2 FMA FLOP/s) on this device."""
+        f, e, f2 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self.check(lib().dsgpu_measure_peaks(self.handle, ctypes.byref(f), ctypes.byref(e), ctypes.byref(f2)),
+                   "dsgpu_measure_peaks")
+        return f.value, e.value, f2.value
 
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and _lib is not None:

@@ -13,7 +13,8 @@ ds_scene ds_scene_make(const dsgpu_scene_desc* d);
 cudaError_t ds_launch_scene(cudaStream_t st, const ds_scene& s, uint16_t* out);
 void ds_scene_host(const ds_scene& s, int x0, int y0, int cw, int ch, uint16_t* out);
 void ds_scene_truth(const ds_scene& s, int x0, int y0, int cw, int ch, float* out);
-cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s);
+cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s,
+                             double* ffma2_flops);
 
 namespace {
 
@@ -327,11 +328,13 @@ int dsgpu_stage_ms(dsgpu_ctx* ctx, int stage, double* total_ms, int* count) {
   return DSGPU_OK;
 }
 
-int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops, double* ex2_per_s) {
+int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops, double* ex2_per_s, double* ffma2_flops) {
   if (!ctx || !ffma_flops || !ex2_per_s) return DSGPU_ERR_ARG;
   DeviceGuard g(ctx->device);
-  DS_TRY(ds_measure_peaks(ctx->stream, ctx->device, ffma_flops, ex2_per_s));
-  ctx->launches += 4;
+  double f2 = 0.0;
+  DS_TRY(ds_measure_peaks(ctx->stream, ctx->device, ffma_flops, ex2_per_s, &f2));
+  if (ffma2_flops) *ffma2_flops = f2;
+  ctx->launches += 6;
   return DSGPU_OK;
 }
 

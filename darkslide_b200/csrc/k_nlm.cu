@@ -7,158 +7,226 @@
 // (:58) and accumulates weight*sample and weight (:59-60); the result is
 // a/max(s,1e-12) (:71).
 //
-// Here one CTA owns a TX x TY tile of one channel and keeps its a/s
-// accumulators in registers across all offsets. Per offset:
-//   phase A: each thread takes a 16-wide row segment of the tile (plus P rows
-//            above/below), forms the differences against the shifted
-//            samples from the shared-memory copy of the tile + (S+P) halo,
-//            and writes the horizontal (2P+1)-sums as a running sum into a
-//            shared H buffer (double-buffered, so one barrier per offset);
-//   phase B: each thread reads a 4x4 block of H columns (float4), forms the
-//            vertical (2P+1)-sums as a running sum, and accumulates
-//            w = 2^(sum * kexp) (kexp = -log2(e) / (2P+1)^2 / h^2) times the
-//            shifted sample.
-// Clamped edges: the shared copy is loaded at clamped coordinates, so the
-// shifted sample p_clamped(x+o) is a plain shared read; the box filter of the
-// reference clamps the DIFFERENCE plane, so rows are clamped per segment and,
-// in tiles whose patch window leaves the image, columns per element.
+// B200 design. The kernel is bound by shared-memory bandwidth (one 128-byte
+// wavefront per clock per SM) long before the ex2 unit (16/clock/SM), so the
+// layout minimises shared bytes per (pixel, channel, offset) update:
+//  - one CTA owns a 64-wide tile of one channel, TY = 64 - 2P rows tall, so
+//    that the horizontal box sums it needs cover exactly 64 rows;
+//  - the tile plus its S+P+1 halo is staged once in shared memory, PRE-SCALED
+//    by sigma = sqrt(log2(e) / (h^2 (2P+1)^2)): the squared differences of
+//    scaled samples sum directly to the ex2 exponent, so a weight costs one
+//    ex2 and no multiply;
+//  - offsets are processed in 2x2 blocks {dx0, dx0+1} x {dy0, dy0+1}:
+//    phase A: thread t owns H row t%64 (a 16-wide segment, its 22 centre
+//      samples kept in registers for the whole kernel) and forms the
+//      horizontal running sums for the block's offsets from one 23-sample
+//      load of each shifted row (so one load serves both dx);
+//    phase B: thread t owns one column and a quarter of the tile's rows,
+//      sums 2P+1 H rows as a running vertical sum, and accumulates; the
+//      shifted sample of row r at dy0+1 is the one of row r+1 at dy0, so one
+//      column load serves both dy;
+//  - all shared pitches are odd, so a warp's 32 rows (phase A) or 32 columns
+//    (phase B) hit 32 distinct banks.
+// Clamped edges: the staged copy is loaded at clamped coordinates, so the
+// shifted sample p_clamped(x+o) is a plain shared read; the reference's box
+// filter clamps the DIFFERENCE plane, so H rows are clamped per row and, in
+// tiles whose patch window leaves the image, columns per element.
+#include <type_traits>
+
 #include "internal.cuh"
 
 namespace {
 
 constexpr int NLM_THREADS = 256;
-constexpr int TX = 64, TY = 64;
-constexpr int SEG = 16;
-constexpr int SEGS_PER_ROW = TX / SEG;
+constexpr int TX = 64;   // tile width
+constexpr int HRW = 64;  // H rows per offset (TY + 2P)
+constexpr int SEG = 16;  // phase-A segment width
+constexpr int HP = TX + 1;  // odd H pitch
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-__device__ __forceinline__ float ex2_approx(float x) {
+__device__ __forceinline__ float ex2(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
 
-__host__ __device__ constexpr int nlm_h_rows(int P) { return TY + 2 * P; }
+constexpr int HBR = HRW + 4;  // H rows allocated: phase B of the last quarter reads past row 63
 
-__host__ size_t nlm_smem_bytes(int S, int P) {
-  const int R = S + P;
-  const size_t pr = (size_t)(TX + 2 * R) * (TY + 2 * R);
-  const size_t pr_al = (pr + 3) & ~(size_t)3;
-  return (pr_al + 2 * (size_t)nlm_h_rows(P) * TX) * sizeof(float);
+// Plane pitch: odd and fixed per P (sized for the largest search radius) so
+// that every shared address offset is a compile-time constant.
+__host__ __device__ constexpr int nlm_pitch(int P) { return (TX + 2 * (DSGPU_NLM_MAX_SEARCH + P + 1)) | 1; }
+
+struct NlmGeom {
+  int R, PW, PH, PHA;  // halo, region width, region height, allocated rows
+};
+
+__host__ __device__ inline NlmGeom nlm_geom(int S, int P) {
+  NlmGeom g;
+  const int TY = HRW - 2 * P;
+  g.R = S + P + 1;
+  g.PW = TX + 2 * g.R;
+  g.PH = TY + 2 * g.R;
+  g.PHA = g.PH + 4;  // phase B of the last quarter reads up to 3 rows past the region
+  return g;
+}
+
+size_t nlm_smem_bytes(int S, int P) {
+  const NlmGeom g = nlm_geom(S, P);
+  size_t plane = (size_t)nlm_pitch(P) * g.PHA;
+  size_t hb = (size_t)4 * HBR * HP;
+  return (plane + hb) * sizeof(float);
 }
 
 template <int P>
-__global__ void __launch_bounds__(NLM_THREADS) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
-                                                               int S, float kexp, float* __restrict__ out) {
-  constexpr int HR = nlm_h_rows(P);
-  constexpr int NSEG = HR * SEGS_PER_ROW;
-  constexpr int DW = SEG + 2 * P;
-  const int R = S + P;
-  const int PW = TX + 2 * R, PH = TY + 2 * R;
+__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
+                                                                  int S, float sigma, float* __restrict__ out) {
+  constexpr int TY = HRW - 2 * P;
+  constexpr int DW = SEG + 2 * P;  // differences per phase-A segment
+  constexpr int RB = (TY + 3) / 4; // phase-B rows per thread (a quarter of the tile)
+  constexpr int PP = nlm_pitch(P);
+  const NlmGeom g = nlm_geom(S, P);
   extern __shared__ float4 smem4[];
-  float* PR = reinterpret_cast<float*>(smem4);
-  float* HB = PR + ((PW * PH + 3) & ~3);
+  float* PL = reinterpret_cast<float*>(smem4);  // scaled plane, pitch PP
+  float* HB = PL + PP * g.PHA;                  // 4 offsets x HBR rows x HP
 
   const int ch = blockIdx.z;
   const int X0 = blockIdx.x * TX, Y0 = blockIdx.y * TY;
   const int tid = threadIdx.x;
+  const int ox0 = X0 - g.R, oy0 = Y0 - g.R;  // global site of plane (0,0)
 
-  for (int i = tid; i < PW * PH; i += NLM_THREADS) {
-    const int ly = i / PW, lx = i - ly * PW;
-    const int gx = clampi(X0 - R + lx, 0, W - 1), gy = clampi(Y0 - R + ly, 0, H - 1);
-    PR[i] = in[((size_t)gy * W + gx) * C + ch];
+  for (int i = tid; i < g.PW * g.PH; i += NLM_THREADS) {
+    const int ly = i / g.PW, lx = i - ly * g.PW;
+    const int gx = clampi(ox0 + lx, 0, W - 1), gy = clampi(oy0 + ly, 0, H - 1);
+    PL[ly * PP + lx] = in[((size_t)gy * W + gx) * C + ch] * sigma;
   }
-  __syncthreads();
+  for (int i = tid; i < (g.PHA - g.PH) * PP; i += NLM_THREADS) PL[g.PH * PP + i] = 0.f;
 
+  // ---- phase-A role: H row `arow` (tile row arow - P), segment at ax0
+  const int arow = tid & (HRW - 1);
+  const int ax0 = (tid >> 6) * SEG;
+  const int aprow = clampi(Y0 + arow - P, 0, H - 1) - oy0;  // plane row of the clamped H row
   const bool xin = (X0 - P >= 0) && (X0 + TX + P <= W);
-  const int bx = (tid & 15) * 4, by = (tid >> 4) * 4;
-  float a[16], s[16];
+  const int acol0 = ax0 - P + g.R;  // plane column of difference 0 (interior tiles)
+  // ---- phase-B role: column bcol, rows [brow0, brow0 + RB) (clipped to TY)
+  const int bcol = tid & (TX - 1);
+  const int brow0 = (tid >> 6) * RB;
+
+  __syncthreads();
+  float pv[DW];  // centre samples of this thread's phase-A segment
 #pragma unroll
-  for (int i = 0; i < 16; i++) {
-    a[i] = 0.f;
-    s[i] = 0.f;
+  for (int k = 0; k < DW; k++) {
+    const int col = xin ? acol0 + k : clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
+    pv[k] = PL[aprow * PP + col];
+  }
+  float a[RB], s[RB];
+#pragma unroll
+  for (int r = 0; r < RB; r++) {
+    a[r] = 0.f;
+    s[r] = 0.f;
   }
 
-  int par = 0;
-  for (int dy = -S; dy <= S; dy++) {
-    for (int dx = -S; dx <= S; dx++) {
-      float* Hb = HB + par * (HR * TX);
-      // phase A: horizontal sums of the squared differences
-      for (int seg = tid; seg < NSEG; seg += NLM_THREADS) {
-        const int row = seg / SEGS_PER_ROW;
-        const int x0 = (seg - row * SEGS_PER_ROW) * SEG;
-        const int gy = clampi(Y0 + row - P, 0, H - 1);
-        const float* rp = PR + (gy - (Y0 - R)) * PW;
-        const float* rq = rp + dy * PW + dx;
-        float d[DW];
-        if (xin) {
-          const int lx0 = x0 - P + R;
+  // One 2x2 block of offsets {dx0, dx0+1} x {dy0, dy0+NJ-1}.
+  auto block = [&](int dx0, int dy0, auto nj_tag) {
+    constexpr int NJ = decltype(nj_tag)::value;
+    // phase A: horizontal sums, stored NEGATED (-sum d^2) so that phase B's
+    // vertical sum is the ex2 argument itself
 #pragma unroll
-          for (int k = 0; k < DW; k++) d[k] = rp[lx0 + k] - rq[lx0 + k];
-        } else {
+    for (int j = 0; j < NJ; j++) {
+      const float* qrow = PL + (aprow + dy0 + j) * PP + dx0;
+      float d0[DW], d1[DW];
+      if (xin) {
+        float q[DW + 1];
 #pragma unroll
-          for (int k = 0; k < DW; k++) {
-            const int lx = clampi(X0 + x0 - P + k, 0, W - 1) - (X0 - R);
-            d[k] = rp[lx] - rq[lx];
+        for (int k = 0; k <= DW; k++) q[k] = qrow[acol0 + k];
+#pragma unroll
+        for (int k = 0; k < DW; k++) {
+          d0[k] = pv[k] - q[k];
+          d1[k] = pv[k] - q[k + 1];
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < DW; k++) {
+          const int col = clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
+          d0[k] = pv[k] - qrow[col];
+          d1[k] = pv[k] - qrow[col + 1];
+        }
+      }
+      float h0 = 0.f, h1 = 0.f;
+#pragma unroll
+      for (int k = 0; k <= 2 * P; k++) {
+        h0 = fmaf(-d0[k], d0[k], h0);
+        h1 = fmaf(-d1[k], d1[k], h1);
+      }
+      float* H0 = HB + (j * 2 + 0) * (HBR * HP) + arow * HP + ax0;
+      float* H1 = HB + (j * 2 + 1) * (HBR * HP) + arow * HP + ax0;
+      H0[0] = h0;
+      H1[0] = h1;
+#pragma unroll
+      for (int k = 1; k < SEG; k++) {
+        h0 = fmaf(-d0[k + 2 * P], d0[k + 2 * P], h0);
+        h0 = fmaf(d0[k - 1], d0[k - 1], h0);
+        h1 = fmaf(-d1[k + 2 * P], d1[k + 2 * P], h1);
+        h1 = fmaf(d1[k - 1], d1[k - 1], h1);
+        H0[k] = h0;
+        H1[k] = h1;
+      }
+    }
+    __syncthreads();
+    // phase B: vertical sums, weights, accumulation for (dx0 + i, dy0 + j)
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      if (dx0 + i <= S) {  // false only for the dx tail of an odd search width
+        const float* qc = PL + (brow0 + g.R + dy0) * PP + bcol + g.R + dx0 + i;
+        float qv[RB + NJ - 1];
+#pragma unroll
+        for (int r = 0; r < RB + NJ - 1; r++) qv[r] = qc[r * PP];
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+          const float* hc = HB + (j * 2 + i) * (HBR * HP) + brow0 * HP + bcol;
+          float hv[RB + 2 * P];
+#pragma unroll
+          for (int r = 0; r < RB + 2 * P; r++) hv[r] = hc[r * HP];
+          float v = 0.f;
+#pragma unroll
+          for (int r = 0; r <= 2 * P; r++) v += hv[r];
+#pragma unroll
+          for (int r = 0; r < RB; r++) {
+            if (r > 0) v = v + hv[r + 2 * P] - hv[r - 1];
+            const float wgt = ex2(v);
+            a[r] = fmaf(wgt, qv[r + j], a[r]);
+            s[r] += wgt;
           }
         }
-        float acc = 0.f;
-#pragma unroll
-        for (int k = 0; k <= 2 * P; k++) acc = fmaf(d[k], d[k], acc);
-        float* hrow = Hb + row * TX + x0;
-        hrow[0] = acc;
-#pragma unroll
-        for (int j = 1; j < SEG; j++) {
-          acc = fmaf(d[j + 2 * P], d[j + 2 * P], acc);
-          acc = fmaf(-d[j - 1], d[j - 1], acc);
-          hrow[j] = acc;
-        }
       }
-      __syncthreads();
-      // phase B: vertical sums, weights, accumulation
-      float4 hv[4 + 2 * P];
-#pragma unroll
-      for (int r = 0; r < 4 + 2 * P; r++) hv[r] = *reinterpret_cast<const float4*>(Hb + (by + r) * TX + bx);
-      const float* qrow = PR + (by + R + dy) * PW + bx + R + dx;
-#pragma unroll
-      for (int col = 0; col < 4; col++) {
-        auto hc = [&](int r) -> float {
-          return col == 0 ? hv[r].x : col == 1 ? hv[r].y : col == 2 ? hv[r].z : hv[r].w;
-        };
-        float v = 0.f;
-#pragma unroll
-        for (int r = 0; r <= 2 * P; r++) v += hc(r);
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-          if (t > 0) v = v + hc(t + 2 * P) - hc(t - 1);
-          const float wgt = ex2_approx(v * kexp);
-          const float q = qrow[t * PW + col];
-          a[t * 4 + col] = fmaf(wgt, q, a[t * 4 + col]);
-          s[t * 4 + col] += wgt;
-        }
-      }
-      par ^= 1;
     }
-  }
+    __syncthreads();
+  };
 
+  int dy0 = -S;
+  for (; dy0 + 1 <= S; dy0 += 2)
+    for (int dx0 = -S; dx0 <= S; dx0 += 2) block(dx0, dy0, std::integral_constant<int, 2>{});
+  if (dy0 <= S)  // the dy tail of an odd search width
+    for (int dx0 = -S; dx0 <= S; dx0 += 2) block(dx0, dy0, std::integral_constant<int, 1>{});
+
+  const float inv_sigma = 1.0f / sigma;
 #pragma unroll
-  for (int t = 0; t < 4; t++)
-#pragma unroll
-    for (int col = 0; col < 4; col++) {
-      const int gx = X0 + bx + col, gy = Y0 + by + t;
-      if (gx < W && gy < H)
-        out[((size_t)gy * W + gx) * C + ch] = __fdiv_rn(a[t * 4 + col], fmaxf(s[t * 4 + col], 1e-12f));
-    }
+  for (int r = 0; r < RB; r++) {
+    const int y = brow0 + r;
+    const int gx = X0 + bcol, gy = Y0 + y;
+    if (y < TY && gx < W && gy < H)
+      out[((size_t)gy * W + gx) * C + ch] = __fdiv_rn(a[r] * inv_sigma, fmaxf(s[r], 1e-12f));
+  }
 }
 
 template <int P>
-cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float kexp, float* out) {
+cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float sigma, float* out) {
+  constexpr int TY = HRW - 2 * P;
   const size_t smem = nlm_smem_bytes(S, P);
   cudaError_t e = cudaFuncSetAttribute(nlm_tile_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY, C);
-  nlm_tile_kernel<P><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, kexp, out);
+  nlm_tile_kernel<P><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, out);
   return cudaGetLastError();
 }
 
@@ -166,21 +234,25 @@ cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, 
 
 cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int channels, float h_param, int search,
                           int patch, float* out) {
+  if (search == 0) {  // only the centre offset: weight 1, out = p exactly (enhance.rs:41-71)
+    return cudaMemcpyAsync(out, in, (size_t)w * h * channels * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  }
   // enhance.rs:40: h2 = max(h*h, 1e-12) in f32; box_blur's norm is 1/(2r+1)
-  // in f32 and is applied once per pass (image.rs:274, 285, 307).
+  // in f32, applied once per pass (image.rs:274, 285, 307). The weight is
+  // exp(-sum d^2 * norm^2 / h2) = 2^-(sum (sigma d)^2).
   const float h2 = fmaxf(h_param * h_param, 1e-12f);
   const float norm = patch == 0 ? 1.0f : 1.0f / (float)(2 * patch + 1);
-  const double kexp = -((double)norm * (double)norm) / (double)h2 * 1.4426950408889634;
-  const float k = (float)kexp;
+  const double sig2 = (double)norm * (double)norm / (double)h2 * 1.4426950408889634;
+  const float sigma = (float)sqrt(sig2);
   switch (patch) {
-    case 0: return launch_nlm_p<0>(st, in, w, h, channels, search, k, out);
-    case 1: return launch_nlm_p<1>(st, in, w, h, channels, search, k, out);
-    case 2: return launch_nlm_p<2>(st, in, w, h, channels, search, k, out);
-    case 3: return launch_nlm_p<3>(st, in, w, h, channels, search, k, out);
-    case 4: return launch_nlm_p<4>(st, in, w, h, channels, search, k, out);
-    case 5: return launch_nlm_p<5>(st, in, w, h, channels, search, k, out);
-    case 6: return launch_nlm_p<6>(st, in, w, h, channels, search, k, out);
-    case 7: return launch_nlm_p<7>(st, in, w, h, channels, search, k, out);
+    case 0: return launch_nlm_p<0>(st, in, w, h, channels, search, sigma, out);
+    case 1: return launch_nlm_p<1>(st, in, w, h, channels, search, sigma, out);
+    case 2: return launch_nlm_p<2>(st, in, w, h, channels, search, sigma, out);
+    case 3: return launch_nlm_p<3>(st, in, w, h, channels, search, sigma, out);
+    case 4: return launch_nlm_p<4>(st, in, w, h, channels, search, sigma, out);
+    case 5: return launch_nlm_p<5>(st, in, w, h, channels, search, sigma, out);
+    case 6: return launch_nlm_p<6>(st, in, w, h, channels, search, sigma, out);
+    case 7: return launch_nlm_p<7>(st, in, w, h, channels, search, sigma, out);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -2,6 +2,7 @@
 // bound by the SFU (ex2) and FP32 pipes rather than by HBM or tensor cores:
 //   ffma_kernel: 8 independent FFMA chains per thread -> FP32 FLOP/s
 //   ex2_kernel : 8 independent ex2.approx chains per thread -> ex2/s
+//   ffma2_kernel: 8 independent fma.rn.f32x2 chains per thread -> packed FP32 FLOP/s
 // Each runs on every SM (grid = 8 x SM count) for a fixed iteration count.
 #include "internal.cuh"
 
@@ -46,10 +47,39 @@ __global__ void __launch_bounds__(256) ex2_kernel(int iters, float seed, float* 
   if (s == 12345.678f) sink[0] = s;
 }
 
+// packed FP32: 8 independent fma.rn.f32x2 chains (two lanes each) per thread
+__global__ void __launch_bounds__(256) ffma2_kernel(int iters, float seed, float* sink) {
+  unsigned long long a[8];
+  const float m = 0.999999f, c = 1e-7f;
+  unsigned long long mm, cc;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(mm) : "f"(m), "f"(m));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(cc) : "f"(c), "f"(c));
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const float lo = seed + threadIdx.x * 1e-7f + i, hi = lo + 0.5f;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(a[i]) : "f"(lo), "f"(hi));
+  }
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+#pragma unroll
+      for (int i = 0; i < 8; i++) asm volatile("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(a[i]) : "l"(mm), "l"(cc));
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a[i]));
+    s += lo + hi;
+  }
+  if (s == 12345.678f) sink[0] = s;
+}
+
 }  // namespace
 
 // Times both kernels with CUDA events on `st`; returns FLOP/s and ex2/s.
-cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s) {
+cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s,
+                             double* ffma2_flops) {
   int sms = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
@@ -77,6 +107,14 @@ cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, do
     cudaEventElapsedTime(&ms, a, b);
   }
   *ex2_per_s = 8.0 * 16 * (double)it_e * blocks * threads / (ms * 1e-3);
+  for (int rep = 0; rep < 2; rep++) {
+    cudaEventRecord(a, st);
+    ffma2_kernel<<<blocks, threads, 0, st>>>(it_f, 1.0f, sink);
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+  }
+  *ffma2_flops = 2.0 * 2 * 8 * 16 * (double)it_f * blocks * threads / (ms * 1e-3);
   e = cudaGetLastError();
   cudaEventDestroy(a);
   cudaEventDestroy(b);

@@ -84,15 +84,16 @@ const char* dsgpu_last_error(dsgpu_ctx* ctx);
  * every later call on the context stream (and discards earlier records);
  * dsgpu_stage_ms() sums the recorded device time of one stage.
  * dsgpu_launch_count() is the number of kernels the context has launched.
- * dsgpu_measure_peaks() times FP32 FMA and ex2 throughput microbenchmarks
- * (the roofline denominators of the NLM kernel). */
+ * dsgpu_measure_peaks() times FP32 FMA, ex2 and packed (f32x2) FMA
+ * throughput microbenchmarks, the roofline denominators of the NLM kernel
+ * (ffma2_flops_per_s may be NULL). */
 #define DSGPU_STAGE_DEMOSAIC 0
 #define DSGPU_STAGE_NLM 1
 #define DSGPU_STAGE_COPY 2
 int dsgpu_profile(dsgpu_ctx* ctx, int enable);
 int dsgpu_stage_ms(dsgpu_ctx* ctx, int stage, double* total_ms, int* count);
 unsigned long long dsgpu_launch_count(dsgpu_ctx* ctx);
-int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops_per_s, double* ex2_per_s);
+int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops_per_s, double* ex2_per_s, double* ffma2_flops_per_s);
 
 /* CFA normalisation of an integer raw: out = (raw - black) / max(white[c] - black, 1),
  * c the colour of the site; values are not clamped.
