@@ -266,3 +266,21 @@ def test_errors_are_status_codes(ctx):
     assert e.value.status == -3
     # the context stays usable after argument errors
     assert np.all(ds.box_blur(pl, 1, ctx=ctx).data == 0)
+
+
+def test_row_band_split_on_gpu(ctx):
+    """The row-band split of darkslide_b200.shard on the GPU kernels: bands
+    developed one after another reassemble the whole-frame result."""
+    from darkslide_b200 import shard
+
+    sc = ds.Scene(seed=21, w=640, h=480, pattern=ds.GRBG, black=512, white=16383, gain=0.5, read_sigma=6)
+    raw = sc.render_host()
+    white = np.full(3, 16383, np.float32)
+    S, P, h = 10, 3, 1.5 * sc.sigma_norm()
+    full = ds.develop_u16(raw, ds.GRBG, 512, white, WB, h, S, P, ctx=ctx).data
+    for world in (2, 3):
+        parts = [shard.develop_band(raw, ds.GRBG, shard.band(480, r, world, shard.halo_rows(S, P)), 512, white, WB,
+                                    h, S, P, ctx=ctx) for r in range(world)]
+        got = np.concatenate(parts, axis=0)
+        assert got.shape == full.shape
+        assert np.abs(got - full).max() <= 1e-6
