@@ -13,6 +13,10 @@ the reference's stage API (crates/core, Rust) over the C ABI of libdsgpu.so:
   nlm(p, h, search, patch)  enhance.rs:36
   normalize_u16             decode.rs:292-306 (integer raws)
   develop_u16               the three steps above in one device pass
+  estimate_noise            enhance.rs:10-32
+  guided_filter             image.rs:385-405
+  denoise(img, amount)      enhance.rs:75-92 (Oklab, NLM on L, guided chroma)
+  Oklab                     color.rs:380-419 (matrices)
 
 Buffers may be numpy arrays (host memory: the call stages them through the
 device) or CUDA torch tensors (device memory: the call is ordered on torch's
@@ -32,7 +36,7 @@ from ._lib import Context, DsgpuError, SceneDesc, default_context, lib
 
 __all__ = [
     "CfaPattern", "CfaImage", "Plane", "Image3", "Quality", "demosaic", "rcd_bayer", "mhc_bayer", "clip_plane",
-    "box_blur", "nlm", "normalize_u16", "develop_u16", "Context", "DsgpuError", "default_context", "Scene",
+    "box_blur", "nlm", "normalize_u16", "develop_u16", "estimate_noise", "guided_filter", "denoise", "Oklab", "Context", "DsgpuError", "default_context", "Scene",
     "RGGB", "BGGR", "GRBG", "GBRG",
 ]
 
@@ -258,6 +262,47 @@ def develop_u16(raw, pattern: CfaPattern, black: float, white, mul, h_param: flo
                 "dsgpu_develop_u16")
     img = Image3(w, h, rgb)
     return (img, Plane(w, h, clip)) if with_clip else img
+
+
+def estimate_noise(p: Plane, ctx: Context | None = None) -> float:
+    """enhance.rs:10-32: robust noise sigma (MAD of a Laplacian high pass)."""
+    c = _Call(p.data, ctx)
+    src, pi = c.inp(p.data, np.float32)
+    sig = ctypes.c_float()
+    c.ctx.check(lib().dsgpu_estimate_noise(c.ctx.handle, pi, p.w, p.h, ctypes.byref(sig), c.flags & _lib.DSGPU_HOST),
+                "dsgpu_estimate_noise")
+    return float(sig.value)
+
+
+def guided_filter(i: Plane, p: Plane, r: int, eps: float, ctx: Context | None = None) -> Plane:
+    """image.rs:385-405."""
+    c = _Call(i.data, ctx)
+    _, pI = c.inp(i.data, np.float32)
+    _, pP = c.inp(p.data, np.float32)
+    out, po = c.out((i.h, i.w))
+    c.ctx.check(lib().dsgpu_guided_filter(c.ctx.handle, pI, pP, i.w, i.h, int(r), float(eps), po, c.flags),
+                "dsgpu_guided_filter")
+    return Plane(i.w, i.h, out)
+
+
+def denoise(img: Image3, amount: float, ctx: Context | None = None) -> Image3:
+    """enhance.rs:75-92: Oklab L through NLM (3, 1), chroma through guided filters."""
+    c = _Call(img.data, ctx)
+    _, pi = c.inp(img.data, np.float32)
+    out, po = c.out((img.h, img.w, 3))
+    c.ctx.check(lib().dsgpu_denoise(c.ctx.handle, pi, img.w, img.h, float(amount), po, c.flags), "dsgpu_denoise")
+    return Image3(img.w, img.h, out)
+
+
+class Oklab:
+    """Oklab::new() of color.rs:394-399 (matrices computed by the library)."""
+
+    def __init__(self):
+        m = np.empty(27, np.float32)
+        st = lib().dsgpu_oklab_matrices(_vp(m))
+        if st != 0:
+            raise DsgpuError(st, "dsgpu_oklab_matrices")
+        self.to_lms, self.from_lms, self.m2_inv = m.reshape(3, 3, 3)
 
 
 # ------------------------------------------------------------ synthetic input

@@ -34,7 +34,8 @@ EXPORTS = [
     "dsgpu_strerror", "dsgpu_abi_version", "dsgpu_create", "dsgpu_destroy", "dsgpu_set_stream",
     "dsgpu_get_stream", "dsgpu_synchronize", "dsgpu_trim", "dsgpu_last_error", "dsgpu_normalize_u16",
     "dsgpu_clip_plane", "dsgpu_mhc", "dsgpu_rcd", "dsgpu_demosaic", "dsgpu_box_blur", "dsgpu_nlm",
-    "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
+    "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_estimate_noise", "dsgpu_guided_filter",
+    "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
     "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render",
 ]
 
@@ -96,6 +97,10 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_nlm.argtypes = [vp, vp, i, i, i, f, i, i, vp, u]
             L.dsgpu_develop_u16.argtypes = [vp, vp, i, i, sz, vp, f, vp, vp, f, i, i, vp, vp, u]
             L.dsgpu_develop_u16_noalloc.argtypes = [vp, vp, i, i, sz, vp, f, vp, vp, f, i, i, vp, vp, u]
+            L.dsgpu_estimate_noise.argtypes = [vp, vp, i, i, ctypes.POINTER(f), u]
+            L.dsgpu_guided_filter.argtypes = [vp, vp, vp, i, i, i, f, vp, u]
+            L.dsgpu_oklab_matrices.argtypes = [vp]
+            L.dsgpu_denoise.argtypes = [vp, vp, i, i, f, vp, u]
             L.dsgpu_profile.argtypes = [vp, i]
             L.dsgpu_stage_ms.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i)]
             L.dsgpu_launch_count.argtypes = [vp]

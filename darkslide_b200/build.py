@@ -28,6 +28,7 @@ UNITS = [
     ("k_demosaic.cu", ["-fmad=false"]),
     ("k_box.cu", ["-fmad=false"]),
     ("k_scene.cu", ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]),
+    ("k_denoise.cu", ["-fmad=false"]),
     ("k_nlm.cu", []),
     ("k_peak.cu", []),
     ("api.cu", []),

@@ -18,7 +18,7 @@ cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, do
 
 namespace {
 
-enum Slot { S_IN = 0, S_OUT, S_OUT2, S_CFA, S_RGB, S_TMP, S_COUNT };
+enum Slot { S_IN = 0, S_IN2, S_OUT, S_OUT2, S_CFA, S_RGB, S_TMP, S_WORK, S_COUNT };
 
 }  // namespace
 
@@ -524,6 +524,82 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
   }
   DS_CHECK(run_nlm(ctx, (const float*)mid, w, h, 3, h_param, search, patch, (float*)drgb));
   return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));
+}
+
+// ----------------------------------------------------------------- denoise
+
+int dsgpu_oklab_matrices(float* out27) {
+  if (!out27) return DSGPU_ERR_ARG;
+  ds_oklab_matrices(out27);
+  return DSGPU_OK;
+}
+
+int dsgpu_estimate_noise(dsgpu_ctx* ctx, const float* plane, int w, int h, float* sigma, unsigned flags) {
+  if (!ctx || !sigma) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  const size_t n = (size_t)w * h;
+  if (n == 0) {  // enhance.rs:25-27
+    *sigma = 0.0f;
+    return DSGPU_OK;
+  }
+  if (!plane) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* work;
+  DS_CHECK(stage_in(ctx, flags, S_IN, plane, n * sizeof(float), &din));
+  DS_CHECK(scratch(ctx, S_WORK, ds_noise_scratch_bytes(w, h) + 8 * sizeof(float), &work));
+  float* out3 = static_cast<float*>(work) + ds_noise_scratch_bytes(w, h) / sizeof(float);
+  DS_TRY(ds_launch_estimate_noise(ctx->stream, (const float*)din, w, h, 0.0f, work, out3));
+  ctx->launches += 2;
+  float host4[4];
+  DS_TRY(cudaMemcpyAsync(host4, out3, 4 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  *sigma = host4[3];  // without denoise's 1e-4 floor (enhance.rs:82)
+  return DSGPU_OK;
+}
+
+int dsgpu_guided_filter(dsgpu_ctx* ctx, const float* I, const float* p, int w, int h, int r, float eps, float* out,
+                        unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  if (r < 0) return DSGPU_ERR_ARG;
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!I || !p || !out) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void *dI, *dp;
+  void *dout, *work;
+  DS_CHECK(stage_in(ctx, flags, S_IN, I, n * sizeof(float), &dI));
+  DS_CHECK(stage_in(ctx, flags, S_IN2, p, n * sizeof(float), &dp));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, n * sizeof(float), &dout));
+  DS_CHECK(scratch(ctx, S_WORK, 9 * n * sizeof(float), &work));
+  float* ws = static_cast<float*>(work);
+  DS_TRY(ds_launch_guide_means(ctx->stream, (const float*)dI, w, h, r, ws, ws + n, ws + 8 * n, ws + 2 * n));
+  DS_TRY(ds_launch_guided_filter(ctx->stream, (const float*)dI, (const float*)dp, w, h, r, nullptr, eps,
+                                 (float*)dout, ws + 2 * n, ws, ws + n));
+  ctx->launches += 5 + 11;
+  return finish(ctx, flags, out, dout, n * sizeof(float));
+}
+
+int dsgpu_denoise(dsgpu_ctx* ctx, const float* in_rgb, int w, int h, float amount, float* out_rgb, unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!in_rgb || !out_rgb) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void *dout, *work;
+  DS_CHECK(stage_in(ctx, flags, S_IN, in_rgb, n * 3 * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &dout));
+  DS_CHECK(scratch(ctx, S_WORK, ds_denoise_scratch_bytes(w, h), &work));
+  unsigned nl = 0;
+  {
+    StageMark mark(ctx, DSGPU_STAGE_NLM);
+    DS_TRY(ds_launch_denoise(ctx->stream, (const float*)din, w, h, amount, work, (float*)dout, nullptr, &nl));
+  }
+  ctx->launches += nl;
+  return finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float));
 }
 
 // ------------------------------------------------------------------ scenes

@@ -43,3 +43,18 @@ cudaError_t ds_launch_superpixel(cudaStream_t st, const float* cfa, int w, int h
 cudaError_t ds_launch_box_blur(cudaStream_t st, const float* in, int w, int h, int r, float* tmp, float* out);
 cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int channels, float h_param, int search,
                           int patch, float* out);
+cudaError_t ds_launch_nlm_dev_h(cudaStream_t st, const float* in, int w, int h, int channels, const float* h_dev,
+                                int search, int patch, float* out);
+// denoise composite (enhance.rs:75-92) and its parts
+size_t ds_denoise_scratch_bytes(int w, int h);
+size_t ds_noise_scratch_bytes(int w, int h);
+cudaError_t ds_launch_estimate_noise(cudaStream_t st, const float* p, int w, int h, float k, void* scratch,
+                                     float* out3);
+cudaError_t ds_launch_guided_filter(cudaStream_t st, const float* I, const float* p, int w, int h, int r,
+                                    const float* eps_dev, float eps_host, float* out, float* scratch,
+                                    const float* mean_i, const float* mean_ii);
+cudaError_t ds_launch_guide_means(cudaStream_t st, const float* I, int w, int h, int r, float* mean_i, float* mean_ii,
+                                  float* tmp, float* tmp2);
+cudaError_t ds_launch_denoise(cudaStream_t st, const float* rgb, int w, int h, float amount, void* scratch,
+                              float* out, float* sigma_dev_out, unsigned* launches);
+void ds_oklab_matrices(float out[27]);

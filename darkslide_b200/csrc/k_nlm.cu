@@ -80,7 +80,12 @@ size_t nlm_smem_bytes(int S, int P) {
 
 template <int P>
 __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
-                                                                  int S, float sigma, float* __restrict__ out) {
+                                                                  int S, float sigma, const float* __restrict__ h_dev,
+                                                                  float norm2_log2e, float* __restrict__ out) {
+  if (h_dev) {  // strength computed on the device (enhance.rs:40 floor included)
+    const float hh = *h_dev;
+    sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
+  }
   constexpr int TY = HRW - 2 * P;
   constexpr int DW = SEG + 2 * P;  // differences per phase-A segment
   constexpr int RB = (TY + 3) / 4; // phase-B rows per thread (a quarter of the tile)
@@ -220,14 +225,36 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* _
 }
 
 template <int P>
-cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float sigma, float* out) {
+cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float sigma,
+                         const float* h_dev, float norm2_log2e, float* out) {
   constexpr int TY = HRW - 2 * P;
   const size_t smem = nlm_smem_bytes(S, P);
   cudaError_t e = cudaFuncSetAttribute(nlm_tile_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY, C);
-  nlm_tile_kernel<P><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, out);
+  nlm_tile_kernel<P><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, out);
   return cudaGetLastError();
+}
+
+}  // namespace
+
+namespace {
+
+cudaError_t dispatch_nlm(cudaStream_t st, const float* in, int w, int h, int C, int S, int P, float sigma,
+                         const float* h_dev, float* out) {
+  const float norm = P == 0 ? 1.0f : 1.0f / (float)(2 * P + 1);
+  const float n2l = norm * norm * 1.4426950408889634f;
+  switch (P) {
+    case 0: return launch_nlm_p<0>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 1: return launch_nlm_p<1>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 2: return launch_nlm_p<2>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 3: return launch_nlm_p<3>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 4: return launch_nlm_p<4>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 5: return launch_nlm_p<5>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 6: return launch_nlm_p<6>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 7: return launch_nlm_p<7>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
@@ -243,16 +270,13 @@ cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int ch
   const float h2 = fmaxf(h_param * h_param, 1e-12f);
   const float norm = patch == 0 ? 1.0f : 1.0f / (float)(2 * patch + 1);
   const double sig2 = (double)norm * (double)norm / (double)h2 * 1.4426950408889634;
-  const float sigma = (float)sqrt(sig2);
-  switch (patch) {
-    case 0: return launch_nlm_p<0>(st, in, w, h, channels, search, sigma, out);
-    case 1: return launch_nlm_p<1>(st, in, w, h, channels, search, sigma, out);
-    case 2: return launch_nlm_p<2>(st, in, w, h, channels, search, sigma, out);
-    case 3: return launch_nlm_p<3>(st, in, w, h, channels, search, sigma, out);
-    case 4: return launch_nlm_p<4>(st, in, w, h, channels, search, sigma, out);
-    case 5: return launch_nlm_p<5>(st, in, w, h, channels, search, sigma, out);
-    case 6: return launch_nlm_p<6>(st, in, w, h, channels, search, sigma, out);
-    case 7: return launch_nlm_p<7>(st, in, w, h, channels, search, sigma, out);
-    default: return cudaErrorInvalidValue;
-  }
+  return dispatch_nlm(st, in, w, h, channels, search, patch, (float)sqrt(sig2), nullptr, out);
+}
+
+// The same with the strength h read from device memory (search > 0).
+cudaError_t ds_launch_nlm_dev_h(cudaStream_t st, const float* in, int w, int h, int channels, const float* h_dev,
+                                int search, int patch, float* out) {
+  if (search == 0)
+    return cudaMemcpyAsync(out, in, (size_t)w * h * channels * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  return dispatch_nlm(st, in, w, h, channels, search, patch, 1.0f, h_dev, out);
 }

@@ -3,6 +3,7 @@
     python -m darkslide_b200.profile_case nlm   # 4096x3072x3 NLM, 7x7 / 21x21
     python -m darkslide_b200.profile_case rcd   # 6000x4000 u16 -> RCD (+clip)
     python -m darkslide_b200.profile_case develop [--w W --h H]
+    python -m darkslide_b200.profile_case denoise  # enhance::denoise, amount 50
 
 Each case does one warm-up call and `--reps` timed calls on cuda:0 and
 prints the mean device time per call (CUDA events).
@@ -21,7 +22,7 @@ from darkslide_b200 import _lib
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["nlm", "rcd", "develop"])
+    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise"])
     ap.add_argument("--w", type=int, default=0)
     ap.add_argument("--h", type=int, default=0)
     ap.add_argument("--reps", type=int, default=2)
@@ -58,13 +59,15 @@ def main():
         elif a.case == "rcd":
             r = L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(mul.ctypes.data),
                                  _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(clip.data_ptr()), _lib.DSGPU_ASYNC)
+        elif a.case == "denoise":
+            r = L.dsgpu_denoise(ctx.handle, vp(rgb.data_ptr()), w, h, 50.0, vp(out.data_ptr()), _lib.DSGPU_ASYNC)
         else:
             r = L.dsgpu_develop_u16(ctx.handle, vp(raw.data_ptr()), w, h, w, vp(pat.ctypes.data), 512.0,
                                     vp(white.ctypes.data), vp(mul.ctypes.data), float(hp), a.search, a.patch,
                                     vp(out.data_ptr()), vp(0), _lib.DSGPU_ASYNC)
         ctx.check(r, a.case)
 
-    if a.case == "nlm":  # NLM input: the demosaiced frame
+    if a.case in ("nlm", "denoise"):  # input: the demosaiced frame
         ctx.check(L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(mul.ctypes.data),
                                    _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(0), 0), "demosaic")
     call()

@@ -130,6 +130,25 @@ int dsgpu_box_blur(dsgpu_ctx* ctx, const float* in, int w, int h, int r, float* 
 int dsgpu_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h_param, int search,
               int patch, float* out, unsigned flags);
 
+/* Robust noise sigma of a plane: median |Laplacian| of up to ~200k sampled
+ * sites / 0.6745 / sqrt(20), 0 for planes without interior sites.
+ * Replaces estimate_noise, enhance.rs:10-32. `sigma` is host memory. */
+int dsgpu_estimate_noise(dsgpu_ctx* ctx, const float* plane, int w, int h, float* sigma, unsigned flags);
+
+/* He et al. guided filter of p guided by I, box radius r, regulariser eps.
+ * Replaces guided_filter, image.rs:385-405. */
+int dsgpu_guided_filter(dsgpu_ctx* ctx, const float* I, const float* p, int w, int h, int r, float eps, float* out,
+                        unsigned flags);
+
+/* Oklab matrices of Oklab::new() (color.rs:394-399): to_lms, from_lms and
+ * inverse M2, row-major, 27 floats. Host only. */
+int dsgpu_oklab_matrices(float* out27);
+
+/* Strong denoise of an interleaved linear RGB image, amount 0..100: Oklab L
+ * through NLM (search 3, patch 1, h = sigma (0.6 + 1.6 amount/100)), chroma
+ * through guided filters. Replaces denoise, enhance.rs:75-92. */
+int dsgpu_denoise(dsgpu_ctx* ctx, const float* in_rgb, int w, int h, float amount, float* out_rgb, unsigned flags);
+
 /* The detail path in one call: u16 raw -> normalise -> RCD -> per-channel NLM.
  * Equivalent to load_raw's normalisation (decode.rs:292-306), demosaic(Full)
  * (demosaic.rs:20-27) and nlm() on each channel (enhance.rs:36-72).

@@ -18,6 +18,9 @@
 //   image.rs:269-313    box_blur (separable running sums, clamped edges)
 //   enhance.rs:10-32    estimate_noise
 //   enhance.rs:36-72    nlm (offset chunks reduced in chunk order)
+//   enhance.rs:75-92    denoise (Oklab L NLM + guided chroma)
+//   image.rs:385-405    guided_filter
+//   color.rs:6-98, 380-419  matrix helpers, Bradford, ProPhoto, Oklab
 // Every kernel is a template on the arithmetic type; the double instantiation
 // is the FP64 oracle.
 //
@@ -422,6 +425,171 @@ float estimate_noise(const float* p, size_t w, size_t h) {
   return v[mid] / 0.6745f / std::sqrt(20.0f);
 }
 
+
+// -------------------------------------------------------------- colour / Oklab
+// color.rs:6-100 (matrix helpers, chromaticities, Bradford) and :380-419
+// (Oklab from linear ProPhoto). Matrix products accumulate in f64 and round
+// to f32 (color.rs:15-23); inversion runs in f64 (color.rs:25-42).
+typedef float M3[3][3];
+
+void mul_mv3(const M3 m, const float v[3], float o[3]) {  // color.rs:11-13
+  o[0] = m[0][0] * v[0] + m[0][1] * v[1] + m[0][2] * v[2];
+  o[1] = m[1][0] * v[0] + m[1][1] * v[1] + m[1][2] * v[2];
+  o[2] = m[2][0] * v[0] + m[2][1] * v[1] + m[2][2] * v[2];
+}
+
+void mul_mm3(const M3 a, const M3 b, M3 o) {  // color.rs:15-23
+  M3 t;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; k++) acc += (double)a[i][k] * (double)b[k][j];
+      t[i][j] = (float)acc;
+    }
+  std::memcpy(o, t, sizeof(M3));
+}
+
+void invert3(const M3 mf, M3 o) {  // color.rs:25-42
+  double m[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) m[i][j] = mf[i][j];
+  const double det = m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                     m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+  if (std::fabs(det) < 1e-12) {
+    const M3 id = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    std::memcpy(o, id, sizeof(M3));
+    return;
+  }
+  const double inv = 1.0 / det;
+  const double r[3][3] = {
+      {(m[1][1] * m[2][2] - m[2][1] * m[1][2]) * inv, (m[0][2] * m[2][1] - m[0][1] * m[2][2]) * inv, (m[0][1] * m[1][2] - m[0][2] * m[1][1]) * inv},
+      {(m[1][2] * m[2][0] - m[1][0] * m[2][2]) * inv, (m[0][0] * m[2][2] - m[0][2] * m[2][0]) * inv, (m[1][0] * m[0][2] - m[0][0] * m[1][2]) * inv},
+      {(m[1][0] * m[2][1] - m[2][0] * m[1][1]) * inv, (m[2][0] * m[0][1] - m[0][0] * m[2][1]) * inv, (m[0][0] * m[1][1] - m[1][0] * m[0][1]) * inv}};
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) o[i][j] = (float)r[i][j];
+}
+
+void xy_to_xyz(const float xy[2], float o[3]) {  // color.rs:65-69
+  const float x = xy[0], y = std::fmax(xy[1], 1e-6f);
+  o[0] = x / y;
+  o[1] = 1.0f;
+  o[2] = (1.0f - x - y) / y;
+}
+
+const float D50_XY[2] = {0.34567f, 0.35850f};  // color.rs:62-63
+const float D65_XY[2] = {0.31271f, 0.32902f};
+
+void bradford(const float src[2], const float dst[2], M3 o) {  // color.rs:80-88
+  const M3 B = {{0.8951f, 0.2664f, -0.1614f}, {-0.7502f, 1.7135f, 0.0367f}, {0.0389f, -0.0685f, 1.0296f}};
+  float xs[3], xd[3], s[3], d[3];
+  xy_to_xyz(src, xs);
+  xy_to_xyz(dst, xd);
+  mul_mv3(B, xs, s);
+  mul_mv3(B, xd, d);
+  const M3 scale = {{d[0] / s[0], 0, 0}, {0, d[1] / s[1], 0}, {0, 0, d[2] / s[2]}};
+  M3 binv, t;
+  invert3(B, binv);
+  mul_mm3(scale, B, t);
+  mul_mm3(binv, t, o);
+}
+
+void prophoto_to_xyz(M3 o) {  // color.rs:90-98 with the ProPhoto primaries of :129 (white D50)
+  const float r[2] = {0.734699f, 0.265301f}, g[2] = {0.159597f, 0.840403f}, b[2] = {0.036598f, 0.000105f};
+  float pr[3], pg[3], pb[3], wv[3], sv[3];
+  xy_to_xyz(r, pr);
+  xy_to_xyz(g, pg);
+  xy_to_xyz(b, pb);
+  const M3 m = {{pr[0], pg[0], pb[0]}, {pr[1], pg[1], pb[1]}, {pr[2], pg[2], pb[2]}};
+  M3 minv;
+  invert3(m, minv);
+  xy_to_xyz(D50_XY, wv);
+  mul_mv3(minv, wv, sv);
+  const M3 dg = {{sv[0], 0, 0}, {0, sv[1], 0}, {0, 0, sv[2]}};
+  mul_mm3(m, dg, o);  // white == D50: no further adaptation
+}
+
+struct Oklab {  // color.rs:380-419
+  M3 to_lms, from_lms, m2, m2_inv;
+  Oklab() {
+    const M3 M1 = {{0.818933f, 0.36186674f, -0.12885971f}, {0.032984544f, 0.9293119f, 0.03614564f}, {0.0482003f, 0.26436627f, 0.6338517f}};
+    const M3 M2 = {{0.21045426f, 0.7936178f, -0.004072047f}, {1.9779985f, -2.4285922f, 0.4505937f}, {0.025904037f, 0.78277177f, -0.80867577f}};
+    M3 brad, pp, t;
+    bradford(D50_XY, D65_XY, brad);
+    prophoto_to_xyz(pp);
+    mul_mm3(brad, pp, t);
+    mul_mm3(M1, t, to_lms);
+    invert3(to_lms, from_lms);
+    std::memcpy(m2, M2, sizeof(M3));
+    invert3(M2, m2_inv);
+  }
+  void from_prophoto(const float p[3], float o[3]) const {
+    float lms[3];
+    mul_mv3(to_lms, p, lms);
+    for (int i = 0; i < 3; i++) lms[i] = std::cbrt(lms[i]);
+    mul_mv3(m2, lms, o);
+  }
+  void to_prophoto(const float lab[3], float o[3]) const {
+    float l[3];
+    mul_mv3(m2_inv, lab, l);
+    const float c[3] = {l[0] * l[0] * l[0], l[1] * l[1] * l[1], l[2] * l[2] * l[2]};
+    mul_mv3(from_lms, c, o);
+  }
+};
+
+// ------------------------------------------------------------- guided filter
+// image.rs:385-405 (He et al.), every box via box_blur (image.rs:269-313).
+void guided_filter(const float* I, const float* p, size_t w, size_t h, size_t r, float eps, float* out) {
+  const size_t n = w * h;
+  std::vector<float> mean_i(n), mean_p(n), ip(n), ii(n), mean_ip(n), mean_ii(n), a(n), b(n), ma(n), mb(n);
+  box_blur<float>(I, w, h, r, mean_i.data());
+  box_blur<float>(p, w, h, r, mean_p.data());
+  for (size_t k = 0; k < n; k++) {
+    ip[k] = I[k] * p[k];
+    ii[k] = I[k] * I[k];
+  }
+  box_blur<float>(ip.data(), w, h, r, mean_ip.data());
+  box_blur<float>(ii.data(), w, h, r, mean_ii.data());
+  for (size_t k = 0; k < n; k++) {
+    const float cov = mean_ip[k] - mean_i[k] * mean_p[k];
+    const float var = mean_ii[k] - mean_i[k] * mean_i[k];
+    a[k] = cov / (var + eps);
+    b[k] = mean_p[k] - a[k] * mean_i[k];
+  }
+  box_blur<float>(a.data(), w, h, r, ma.data());
+  box_blur<float>(b.data(), w, h, r, mb.data());
+  for (size_t k = 0; k < n; k++) out[k] = ma[k] * I[k] + mb[k];
+}
+
+// ------------------------------------------------------------------ denoise
+// enhance.rs:75-92
+void denoise(const float* img, size_t w, size_t h, float amount, int nthreads, float* out, float* sigma_out) {
+  const Oklab ok;
+  const size_t n = w * h;
+  std::vector<float> l(n), a(n), b(n), lf(n), l2(n), a2(n), b2(n);
+  for (size_t i = 0; i < n; i++) {
+    float lab[3];
+    ok.from_prophoto(img + i * 3, lab);
+    l[i] = lab[0];
+    a[i] = lab[1];
+    b[i] = lab[2];
+  }
+  const float sigma = std::fmax(estimate_noise(l.data(), w, h), 1e-4f);
+  if (sigma_out) *sigma_out = sigma;
+  const float k = amount / 100.0f;
+  nlm<float>(l.data(), w, h, sigma * (0.6f + 1.6f * k), 3, 1, nthreads, lf.data());
+  for (size_t i = 0; i < n; i++) l2[i] = l[i] + (lf[i] - l[i]) * (0.5f + 0.5f * k);
+  const size_t r = (size_t)std::fmax(((float)std::max(w, h) / 600.0f) * (1.0f + 2.0f * k), 2.0f);
+  const float eps = (sigma * 2.0f) * (sigma * 2.0f);
+  guided_filter(l2.data(), a.data(), w, h, r, eps, a2.data());
+  guided_filter(l2.data(), b.data(), w, h, r, eps, b2.data());
+  for (size_t i = 0; i < n; i++) {
+    const float lab[3] = {l2[i], a2[i], b2[i]};
+    float o[3];
+    ok.to_prophoto(lab, o);
+    for (int c = 0; c < 3; c++) out[i * 3 + c] = std::fmax(o[c], 0.0f);
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -496,5 +664,31 @@ void dsref_nlm_f64(const double* in, int w, int h, double h_param, int search, i
 }
 
 float dsref_estimate_noise_f32(const float* p, int w, int h) { return estimate_noise(p, w, h); }
+
+// Oklab matrices (to_lms, from_lms, m2_inv), row-major, 27 floats.
+void dsref_oklab_matrices(float* out) {
+  const Oklab ok;
+  std::memcpy(out, ok.to_lms, sizeof(M3));
+  std::memcpy(out + 9, ok.from_lms, sizeof(M3));
+  std::memcpy(out + 18, ok.m2_inv, sizeof(M3));
+}
+
+void dsref_oklab_from_prophoto(const float* rgb, int n, float* lab) {
+  const Oklab ok;
+  for (int i = 0; i < n; i++) ok.from_prophoto(rgb + 3 * i, lab + 3 * i);
+}
+
+void dsref_oklab_to_prophoto(const float* lab, int n, float* rgb) {
+  const Oklab ok;
+  for (int i = 0; i < n; i++) ok.to_prophoto(lab + 3 * i, rgb + 3 * i);
+}
+
+void dsref_guided_filter_f32(const float* I, const float* p, int w, int h, int r, float eps, float* out) {
+  guided_filter(I, p, w, h, r, eps, out);
+}
+
+void dsref_denoise_f32(const float* img, int w, int h, float amount, int nthreads, float* out, float* sigma) {
+  denoise(img, w, h, amount, nthreads, out, sigma);
+}
 
 }  // extern "C"

@@ -54,6 +54,11 @@ def lib():
         L.dsref_nlm_f64.argtypes = [_f64p, i, i, d, i, i, i, _f64p]
         L.dsref_estimate_noise_f32.argtypes = [_f32p, i, i]
         L.dsref_estimate_noise_f32.restype = f
+        L.dsref_oklab_matrices.argtypes = [_f32p]
+        L.dsref_oklab_from_prophoto.argtypes = [_f32p, i, _f32p]
+        L.dsref_oklab_to_prophoto.argtypes = [_f32p, i, _f32p]
+        L.dsref_guided_filter_f32.argtypes = [_f32p, _f32p, i, i, i, f, _f32p]
+        L.dsref_denoise_f32.argtypes = [_f32p, i, i, f, i, _f32p, _f32p]
         _lib = L
     return _lib
 
@@ -167,3 +172,46 @@ def estimate_noise(p: np.ndarray) -> float:
     """enhance.rs:10-32."""
     a = np.ascontiguousarray(p, dtype=np.float32)
     return float(lib().dsref_estimate_noise_f32(a, a.shape[1], a.shape[0]))
+
+
+def oklab_matrices() -> np.ndarray:
+    """(3, 3, 3): to_lms, from_lms, m2_inv of Oklab::new() (color.rs:395-398)."""
+    out = np.empty(27, np.float32)
+    lib().dsref_oklab_matrices(out)
+    return out.reshape(3, 3, 3)
+
+
+def oklab_from_prophoto(rgb: np.ndarray) -> np.ndarray:
+    """color.rs:401-406 on an (..., 3) array."""
+    a = np.ascontiguousarray(rgb, dtype=np.float32)
+    out = np.empty_like(a)
+    lib().dsref_oklab_from_prophoto(a, a.size // 3, out)
+    return out
+
+
+def oklab_to_prophoto(lab: np.ndarray) -> np.ndarray:
+    """color.rs:408-412 on an (..., 3) array."""
+    a = np.ascontiguousarray(lab, dtype=np.float32)
+    out = np.empty_like(a)
+    lib().dsref_oklab_to_prophoto(a, a.size // 3, out)
+    return out
+
+
+def guided_filter(I: np.ndarray, p: np.ndarray, r: int, eps: float) -> np.ndarray:
+    """image.rs:385-405."""
+    a = np.ascontiguousarray(I, dtype=np.float32)
+    b = np.ascontiguousarray(p, dtype=np.float32)
+    out = np.empty_like(a)
+    lib().dsref_guided_filter_f32(a, b, a.shape[1], a.shape[0], int(r), float(eps), out)
+    return out
+
+
+def denoise(img: np.ndarray, amount: float, nthreads: int | None = None):
+    """enhance.rs:75-92 on an (h, w, 3) image; returns (out, sigma)."""
+    a = np.ascontiguousarray(img, dtype=np.float32)
+    h, w, _ = a.shape
+    out = np.empty_like(a)
+    sig = np.zeros(1, np.float32)
+    nt = threads() if nthreads is None else int(nthreads)
+    lib().dsref_denoise_f32(a, w, h, float(amount), nt, out, sig)
+    return out, float(sig[0])

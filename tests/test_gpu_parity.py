@@ -283,4 +283,6 @@ def test_row_band_split_on_gpu(ctx):
                                     h, S, P, ctx=ctx) for r in range(world)]
         got = np.concatenate(parts, axis=0)
         assert got.shape == full.shape
-        assert np.abs(got - full).max() <= 1e-6
+        # bands place the NLM tiles differently, which changes the order of
+        # the FMA sums: equal to ~20 ulps
+        assert np.abs(got - full).max() <= 1e-5

@@ -121,3 +121,28 @@ def test_golden_fixtures(oracle, path):
         wc = z["white"][col[yy % 2, xx % 2]]
         ref = ((z["raw"].astype(np.float32) - z["black"]) / np.maximum(wc - z["black"], np.float32(1))).astype(np.float32)
         np.testing.assert_array_equal(cfa, ref)
+
+
+def test_oklab_roundtrip_and_white(oracle):
+    """color.rs:502-512."""
+    w = oracle.oklab_from_prophoto(np.array([1.0, 1.0, 1.0], np.float32))
+    assert abs(w[0] - 1.0) < 1e-3 and abs(w[1]) < 1e-3 and abs(w[2]) < 1e-3
+    c = np.array([0.3, 0.1, 0.6], np.float32)
+    back = oracle.oklab_to_prophoto(oracle.oklab_from_prophoto(c))
+    assert np.all(np.abs(back - c) < 1e-4)
+
+
+def test_guided_preserves_edge(oracle):
+    """image.rs:464-471."""
+    p = np.where(np.arange(40)[None, :] < 20, 0.1, 0.9).astype(np.float32) * np.ones((30, 1), np.float32)
+    g = oracle.guided_filter(p, p, 4, 1e-4)
+    assert abs(g[5, 5] - 0.1) < 0.02 and abs(g[5, 35] - 0.9) < 0.02
+
+
+def test_denoise_reduces_noise(oracle):
+    rng = np.random.default_rng(2)
+    clean = np.stack([np.where(np.arange(80)[None, :] < 40, 0.2, 0.6) * np.ones((60, 1))] * 3, -1).astype(np.float32)
+    noisy = (clean + rng.normal(0, 0.03, clean.shape)).astype(np.float32)
+    out, sigma = oracle.denoise(noisy, 60)
+    assert sigma > 0
+    assert ((out - clean) ** 2).sum() < ((noisy - clean) ** 2).sum() * 0.5
