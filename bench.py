@@ -35,7 +35,7 @@ BLACK, WHITE = 512, 16383
 GAIN, READ_SIGMA = 0.5, 6.0
 SEARCH, PATCH = 10, 3
 WB = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
-CPU_SAMPLE = (512, 384)  # oracle crop (w, h) of the same frame for the CPU baseline
+CPU_SAMPLE = (1536, 1024)  # oracle crop (w, h) of the same frame for the CPU baseline
 
 
 def workload_config(n_gpus: int) -> dict:
@@ -70,7 +70,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -110,7 +110,7 @@ class Clocks:
                 "power_w_max": max(power) if power else None}
 
 
-def cpu_baseline(threads: int | None = None, repeats: int = 1) -> dict:
+def cpu_baseline(threads: int | None = None, repeats: int = 3) -> dict:
     """The oracle (a C++ restatement of the reference's CPU path, OpenMP over
     all host threads) on a crop of the same frame; returns Mpix/s."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -139,6 +139,22 @@ def cpu_baseline(threads: int | None = None, repeats: int = 1) -> dict:
     return {"value": cw * ch / t / 1e6, "unit": "Mpix/s", "cores": nt, "kind": "port",
             "sample": f"{cw}x{ch} crop of the 6000x4000 frame (normalise+RCD+clip+NLM x3), median of {repeats}, "
                       f"{t:.2f} s each", "seconds": t}
+
+
+def read_traffic() -> dict:
+    """DRAM bytes per launch at this workload, from the committed ncu summary
+    (profiles/dram_traffic.txt: `key = bytes` lines)."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    if os.path.exists(path):
+        for ln in open(path):
+            if "=" in ln and not ln.lstrip().startswith("#"):
+                k, v = ln.split("=", 1)
+                try:
+                    out[k.strip()] = float(v.split()[0])
+                except (ValueError, IndexError):
+                    pass
+    return out
 
 
 def dist_env():
@@ -300,13 +316,7 @@ def run_ours(args):
         achieved_ex2 = updates / (nlm_launch_ms * 1e-3) / 1e9
         dem_launch_ms = dem_ms / max(dem_n, 1)
         rcd_bytes = W * H * (2 + 12)  # u16 in, RGB f32 out
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath):
-            try:
-                traffic = json.load(open(tpath))
-            except ValueError:
-                traffic = None
+        traffic = read_traffic()
         line = {
             "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -348,7 +358,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
