@@ -245,16 +245,32 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
     mhc_formulas(p, pat.at(gx, gy), pat.at(gx + 1, gy), o0, o1, o2);
   };
 
-  // stage 3: green (:203-214 init, :222-245 step 3) on [5, RS-5)
-  for (int i = tid; i < (RS - 10) * (RS - 10); i += RCD_THREADS) {
-    const int ly = 5 + i / (RS - 10), lx = 5 + i % (RS - 10);
+  // Sites of one colour class come every other column, so the heavy stages
+  // below enumerate only the sites that need work (no divergence between
+  // neighbouring lanes): col_start() is the first local column >= lx0 in row
+  // ly whose global colour is (or, with want_g=false, is not) green.
+  auto col_start = [&](int ly, int lx0, bool want_g) {
+    const int gy = gy0 + ly, gx = gx0 + lx0;
+    const bool g_here = pat.at(gx, gy) == 1;
+    return lx0 + ((g_here == want_g) ? 0 : 1);
+  };
+  auto inner = [&](int gx, int gy) { return gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4; };
+
+  // stage 3: green (:203-214 init, :222-245 step 3) on [5, RS-5): 42 x 21
+  // sites of each class
+  constexpr int S3 = RS - 10, S3H = S3 / 2;
+  for (int i = tid; i < S3 * S3H; i += RCD_THREADS) {  // green sites: native sample
+    const int ly = 5 + i / S3H, lx = col_start(ly, 5, true) + 2 * (i % S3H);
+    if (lx >= RS - 5) continue;
+    G[ly * RS + lx] = C(ly * RS + lx);
+  }
+  for (int i = tid; i < S3 * S3H; i += RCD_THREADS) {  // R/B sites
+    const int ly = 5 + i / S3H, lx = col_start(ly, 5, false) + 2 * (i % S3H);
+    if (lx >= RS - 5) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RS + lx;
-    const int col = pat.at(gx, gy);
     float g;
-    if (col == 1) {
-      g = C(k);
-    } else if (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4) {
+    if (inner(gx, gy)) {
       const float vd = disc(VH, k);
       const float n_grad = eps + fabsf(C(k - w1) - C(k + w1)) + fabsf(C(k) - C(k - w2)) + fabsf(C(k - w1) - C(k - w3)) +
                            fabsf(C(k - w2) - C(k - w4));
@@ -283,16 +299,17 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
 
   // stage 4: R at B and B at R (:276-308) on [7, RS-7). The pre-pass clone
   // read at the diagonal +-1/+-3 sites of an R (B) site holds native B (R)
-  // samples, i.e. c.
-  for (int i = tid; i < (RS - 14) * (RS - 14); i += RCD_THREADS) {
-    const int ly = 7 + i / (RS - 14), lx = 7 + i % (RS - 14);
+  // samples, i.e. c. Interior green sites are never read (4.4 reads R/B
+  // sites only); ring green sites keep their MHC values.
+  constexpr int S4 = RS - 14, S4H = S4 / 2;
+  for (int i = tid; i < S4 * S4H; i += RCD_THREADS) {  // R/B sites
+    const int ly = 7 + i / S4H, lx = col_start(ly, 7, false) + 2 * (i % S4H);
+    if (lx >= RS - 7) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RS + lx;
     const int col = pat.at(gx, gy);
-    const bool inner = gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4;
     float r, b;
-    if (inner) {
-      if (col == 1) continue;  // never read: 4.4 reads R/B sites only
+    if (inner(gx, gy)) {
       const float pd = disc(PQ, k);
       const float g0 = G[k];
       const float nw_g = eps + fabsf(C(k - w1 - 1) - C(k + w1 + 1)) + fabsf(C(k - w1 - 1) - C(k - w3 - 3)) + fabsf(g0 - G[k - w2 - 2]);
@@ -317,18 +334,36 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
     R43[k] = r;
     B43[k] = b;
   }
+  for (int i = tid; i < S4 * S4H; i += RCD_THREADS) {  // green sites of the ring
+    const int ly = 7 + i / S4H, lx = col_start(ly, 7, true) + 2 * (i % S4H);
+    if (lx >= RS - 7) continue;
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    if (inner(gx, gy)) continue;
+    const int k = ly * RS + lx;
+    float o0, o1, o2;
+    mhc_at(k, gx, gy, o0, o1, o2);
+    R43[k] = o0;
+    B43[k] = o2;
+  }
   __syncthreads();
 
-  // stage 5: R and B at G (:310-341) and the tile's output
-  for (int i = tid; i < RT * RT; i += RCD_THREADS) {
-    const int ty = i / RT, tx = i - ty * RT;
-    const int ly = RH + ty, lx = RH + tx;
+  // stage 5: the tile's output; R and B at green sites (:310-341)
+  constexpr int TH = RT / 2;
+  auto clip_at = [&](int k) {
+    unsigned m = 0;
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) m |= CL[k + dy * RS + dx];
+    return m ? 1.0f : 0.0f;
+  };
+  for (int i = tid; i < RT * TH; i += RCD_THREADS) {  // green sites
+    const int ly = RH + i / TH, lx = col_start(ly, RH, true) + 2 * (i % TH);
+    if (lx >= RH + RT) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
     if (gx >= W || gy >= H) continue;
     const int k = ly * RS + lx;
-    const bool inner = gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4;
-    float r = R43[k], g = G[k], b = B43[k];
-    if (inner && pat.at(gx, gy) == 1) {
+    float r = R43[k], b = B43[k];
+    const float g = G[k];
+    if (inner(gx, gy)) {
       const float vd = disc(VH, k);
       auto pass44 = [&](const float* cc) {
         const float n_g = eps + fabsf(g - G[k - w2]) + fabsf(cc[k - w1] - cc[k + w1]) + fabsf(cc[k - w1] - cc[k - w3]);
@@ -350,12 +385,19 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
     o[0] = r;
     o[1] = g;
     o[2] = b;
-    if (out_clip) {
-      unsigned m = 0;
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) m |= CL[k + dy * RS + dx];
-      out_clip[(size_t)gy * W + gx] = m ? 1.0f : 0.0f;
-    }
+    if (out_clip) out_clip[(size_t)gy * W + gx] = clip_at(k);
+  }
+  for (int i = tid; i < RT * TH; i += RCD_THREADS) {  // R/B sites: values settled by stage 4
+    const int ly = RH + i / TH, lx = col_start(ly, RH, false) + 2 * (i % TH);
+    if (lx >= RH + RT) continue;
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    if (gx >= W || gy >= H) continue;
+    const int k = ly * RS + lx;
+    float* o = out_rgb + ((size_t)gy * W + gx) * 3;
+    o[0] = R43[k];
+    o[1] = G[k];
+    o[2] = B43[k];
+    if (out_clip) out_clip[(size_t)gy * W + gx] = clip_at(k);
   }
 }
 
