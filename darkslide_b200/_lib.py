@@ -28,6 +28,7 @@ DSGPU_QUALITY_FULL = 1
 DSGPU_STAGE_DEMOSAIC = 0
 DSGPU_STAGE_NLM = 1
 DSGPU_STAGE_COPY = 2
+DSGPU_STAGE_CNN = 3
 
 # every symbol include/dsgpu.h and include/dsgpu_scene.h declare
 EXPORTS = [
@@ -35,7 +36,10 @@ EXPORTS = [
     "dsgpu_get_stream", "dsgpu_synchronize", "dsgpu_trim", "dsgpu_last_error", "dsgpu_normalize_u16",
     "dsgpu_clip_plane", "dsgpu_mhc", "dsgpu_rcd", "dsgpu_demosaic", "dsgpu_box_blur", "dsgpu_nlm",
     "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_estimate_noise", "dsgpu_guided_filter",
-    "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
+    "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_cnn_param_count", "dsgpu_cnn_create", "dsgpu_cnn_destroy",
+    "dsgpu_cnn_state", "dsgpu_cnn_gradients", "dsgpu_cnn_train_step", "dsgpu_cnn_infer", "dsgpu_cnn_denoise",
+    "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
+    "dsgpu_measure_mma_sync",
     "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render",
 ]
 
@@ -101,6 +105,17 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_guided_filter.argtypes = [vp, vp, vp, i, i, i, f, vp, u]
             L.dsgpu_oklab_matrices.argtypes = [vp]
             L.dsgpu_denoise.argtypes = [vp, vp, i, i, f, vp, u]
+            L.dsgpu_cnn_param_count.argtypes = []
+            L.dsgpu_cnn_create.argtypes = [vp, i, i, ctypes.POINTER(vp)]
+            L.dsgpu_cnn_destroy.argtypes = [vp, vp]
+            L.dsgpu_cnn_state.argtypes = [vp, vp, i, vp, i, ctypes.POINTER(ctypes.c_longlong), u]
+            L.dsgpu_cnn_gradients.argtypes = [vp, vp, vp, vp, f, vp, i, vp, ctypes.POINTER(f), u]
+            L.dsgpu_cnn_train_step.argtypes = [vp, vp, vp, vp, f, vp, i, f, ctypes.POINTER(f)]
+            L.dsgpu_cnn_infer.argtypes = [vp, vp, vp, i, i, f, vp, u]
+            L.dsgpu_cnn_denoise.argtypes = [vp, vp, vp, i, i, f, i, i, f, vp, ctypes.POINTER(i), u]
+            L.dsgpu_develop_u16_cnn.argtypes = [vp, vp, vp, i, i, sz, vp, f, vp, vp, f, i, i, f, vp, vp, u]
+            L.dsgpu_measure_mma_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+            L.dsgpu_cnn_set_engine.argtypes = [vp, vp, i]
             L.dsgpu_profile.argtypes = [vp, i]
             L.dsgpu_stage_ms.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i)]
             L.dsgpu_launch_count.argtypes = [vp]
@@ -159,6 +174,11 @@ class Context:
         self.check(lib().dsgpu_measure_peaks(self.handle, ctypes.byref(f), ctypes.byref(e), ctypes.byref(f2)),
                    "dsgpu_measure_peaks")
         return f.value, e.value, f2.value
+
+    def measure_mma_sync(self) -> float:
+        f = ctypes.c_double()
+        self.check(lib().dsgpu_measure_mma_sync(self.handle, ctypes.byref(f)), "dsgpu_measure_mma_sync")
+        return f.value
 
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and _lib is not None:

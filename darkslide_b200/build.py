@@ -31,6 +31,8 @@ UNITS = [
     ("k_denoise.cu", ["-fmad=false"]),
     ("k_nlm.cu", []),
     ("k_peak.cu", []),
+    ("k_cnn.cu", []),
+    ("k_cnn_tc.cu", []),
     ("api.cu", []),
     ("noalloc.cu", []),
 ]

@@ -16,6 +16,25 @@ void ds_scene_truth(const ds_scene& s, int x0, int y0, int cw, int ch, float* ou
 cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s,
                              double* ffma2_flops);
 
+cudaError_t ds_measure_mma_sync(cudaStream_t st, int device, double* flops);
+struct DsCnn;
+size_t ds_cnn_param_count();
+cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out);
+void ds_cnn_destroy(DsCnn* net);
+float* ds_cnn_param_ptr(DsCnn* net);
+float* ds_cnn_grad_ptr(DsCnn* net);
+float* ds_cnn_moment_ptr(DsCnn* net, int which);
+long long* ds_cnn_step_ptr(DsCnn* net);
+cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, const float* strength_map,
+                             float strength, const float* tgt, int B, float* loss_sum_host);
+cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr);
+cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out);
+void ds_cnn_set_engine(DsCnn* net, int use_tc);
+int ds_cnn_take_status(DsCnn* net, cudaStream_t st);
+cudaError_t ds_cnn_denoise(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float h_param, int search,
+                           int patch, float tau, float strength_scale, float* out, unsigned char* flags_scratch,
+                           unsigned* count_dev);
+
 namespace {
 
 enum Slot { S_IN = 0, S_IN2, S_OUT, S_OUT2, S_CFA, S_RGB, S_TMP, S_WORK, S_COUNT };
@@ -338,6 +357,14 @@ int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops, double* ex2_per_s, d
   return DSGPU_OK;
 }
 
+int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s) {
+  if (!ctx || !bf16_flops_per_s) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  DS_TRY(ds_measure_mma_sync(ctx->stream, ctx->device, bf16_flops_per_s));
+  ctx->launches += 2;
+  return DSGPU_OK;
+}
+
 int dsgpu_normalize_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t pitch, const uint8_t cfa[4],
                         float black, const float white[3], float* out, unsigned flags) {
   if (!ctx) return DSGPU_ERR_ARG;
@@ -600,6 +627,203 @@ int dsgpu_denoise(dsgpu_ctx* ctx, const float* in_rgb, int w, int h, float amoun
   }
   ctx->launches += nl;
   return finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float));
+}
+
+// --------------------------------------------------------------------- CNN
+
+struct dsgpu_cnn {
+  DsCnn* net = nullptr;
+  int max_batch = 0, crop = 0;
+};
+
+int dsgpu_cnn_param_count(void) { return (int)ds_cnn_param_count(); }
+
+int dsgpu_cnn_create(dsgpu_ctx* ctx, int max_batch, int crop, dsgpu_cnn** out) {
+  if (!ctx || !out || max_batch < 0 || crop < 0 || crop > 4096 || (max_batch > 0 && crop < 1)) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  dsgpu_cnn* c = new (std::nothrow) dsgpu_cnn();
+  if (!c) return DSGPU_ERR_NOMEM;
+  cudaError_t e = ds_cnn_create(max_batch, crop, &c->net);
+  if (e != cudaSuccess) {
+    delete c;
+    return map_cuda(ctx, e, "ds_cnn_create");
+  }
+  c->max_batch = max_batch;
+  c->crop = crop;
+  *out = c;
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_destroy(dsgpu_ctx* ctx, dsgpu_cnn* c) {
+  if (!ctx || !c) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ds_cnn_destroy(c->net);
+  delete c;
+  return DSGPU_OK;
+}
+
+// which: 0 parameters, 1 Adam first moment, 2 Adam second moment
+int dsgpu_cnn_state(dsgpu_ctx* ctx, dsgpu_cnn* c, int which, float* buf, int set, long long* step, unsigned flags) {
+  if (!ctx || !c || which < 0 || which > 2) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  float* dev = which == 0 ? ds_cnn_param_ptr(c->net) : ds_cnn_moment_ptr(c->net, which - 1);
+  const size_t bytes = ds_cnn_param_count() * sizeof(float);
+  if (buf) {
+    const cudaMemcpyKind k = (flags & DSGPU_HOST) ? (set ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost)
+                                                  : cudaMemcpyDeviceToDevice;
+    DS_TRY(cudaMemcpyAsync(set ? (void*)dev : (void*)buf, set ? (const void*)buf : (const void*)dev, bytes, k,
+                           ctx->stream));
+  }
+  if (step) {
+    if (set) *ds_cnn_step_ptr(c->net) = *step;
+    else *step = *ds_cnn_step_ptr(c->net);
+  }
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  return DSGPU_OK;
+}
+
+static int cnn_batch_args(dsgpu_cnn* c, const float* rgb, const float* tgt, int batch) {
+  if (!rgb || !tgt || batch < 1 || batch > c->max_batch) return DSGPU_ERR_ARG;
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_gradients(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* rgb, const float* strength_map, float strength,
+                        const float* target, int batch, float* grads, float* loss_sum, unsigned flags) {
+  if (!ctx || !c) return DSGPU_ERR_ARG;
+  DS_CHECK(cnn_batch_args(c, rgb, target, batch));
+  if (flags & DSGPU_HOST) return DSGPU_ERR_ARG;  // device batches only
+  DeviceGuard g(ctx->device);
+  float loss = 0.f;
+  DS_TRY(ds_cnn_gradients(c->net, ctx->stream, rgb, strength_map, strength, target, batch, &loss));
+  if (loss_sum) *loss_sum = loss;
+  if (grads)
+    DS_TRY(cudaMemcpyAsync(grads, ds_cnn_grad_ptr(c->net), ds_cnn_param_count() * sizeof(float),
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_train_step(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* rgb, const float* strength_map, float strength,
+                         const float* target, int batch, float lr, float* loss_sum) {
+  if (!ctx || !c) return DSGPU_ERR_ARG;
+  DS_CHECK(cnn_batch_args(c, rgb, target, batch));
+  DeviceGuard g(ctx->device);
+  float loss = 0.f;
+  DS_TRY(ds_cnn_gradients(c->net, ctx->stream, rgb, strength_map, strength, target, batch, loss_sum ? &loss : nullptr));
+  DS_TRY(ds_cnn_adam(c->net, ctx->stream, lr));
+  if (loss_sum) *loss_sum = loss;
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, int h, float strength, float* out_rgb,
+                    unsigned flags) {
+  if (!ctx || !c) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!in_rgb || !out_rgb) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  DS_CHECK(stage_in(ctx, flags, S_IN, in_rgb, n * 3 * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &dout));
+  {
+    StageMark mark(ctx, DSGPU_STAGE_CNN);
+    DS_TRY(ds_cnn_infer(c->net, ctx->stream, (const float*)din, w, h, strength, (float*)dout));
+  }
+  ctx->launches += 2 + 8 + 8;
+  DS_CHECK(finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float)));
+  return (flags & DSGPU_ASYNC) ? DSGPU_OK : ds_cnn_take_status(c->net, ctx->stream);
+}
+
+int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* c, int tensor_core_gen5) {
+  if (!ctx || !c) return DSGPU_ERR_ARG;
+  ds_cnn_set_engine(c->net, tensor_core_gen5);
+  return DSGPU_OK;
+}
+
+// Scratch for the fallback: the tile flags (one byte per NLM tile) + u32 count
+static int fallback_scratch(dsgpu_ctx* ctx, int w, int h, int patch, unsigned char** flags, unsigned** count) {
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  const size_t nflags = ((size_t)tx * ty + 15) & ~(size_t)15;
+  void* p;
+  DS_CHECK(scratch(ctx, S_TMP, nflags + 16, &p));
+  *flags = static_cast<unsigned char*>(p);
+  *count = reinterpret_cast<unsigned*>(*flags + nflags);
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, int h, float h_param, int search,
+                      int patch, float tau, float* out_rgb, int* fallback_tiles, unsigned flags) {
+  if (!ctx || !c) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  DS_CHECK(nlm_args_ok(3, search, patch));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!in_rgb || !out_rgb || search < 1) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  unsigned char* fl;
+  unsigned* cnt;
+  DS_CHECK(stage_in(ctx, flags, S_IN, in_rgb, n * 3 * sizeof(float), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &dout));
+  DS_CHECK(fallback_scratch(ctx, w, h, patch, &fl, &cnt));
+  {
+    StageMark mark(ctx, DSGPU_STAGE_CNN);
+    DS_TRY(ds_cnn_denoise(c->net, ctx->stream, (const float*)din, w, h, h_param, search, patch, tau,
+                          DSGPU_CNN_STRENGTH_SCALE, (float*)dout, fl, cnt));
+  }
+  ctx->launches += 2 + 8 + 8 + (tau > 0.f ? 2 : 0);
+  if (!(flags & DSGPU_ASYNC)) DS_CHECK(ds_cnn_take_status(c->net, ctx->stream));
+  if (fallback_tiles) {
+    unsigned hc = 0;
+    if (tau > 0.f) {
+      DS_TRY(cudaMemcpyAsync(&hc, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+      DS_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    *fallback_tiles = (int)hc;
+  }
+  return finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float));
+}
+
+int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* c, const uint16_t* raw, int w, int h, size_t pitch,
+                          const uint8_t cfa[4], float black, const float white[3], const float mul[3], float h_param,
+                          int search, int patch, float tau, float* out_rgb, float* out_clip, unsigned flags) {
+  if (!ctx || !c) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  ds_pat pat;
+  DS_CHECK(check_pat(cfa, &pat));
+  DS_CHECK(nlm_args_ok(3, search, patch));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!raw || !out_rgb || !white || !mul || pitch < (size_t)w || search < 1) return DSGPU_ERR_ARG;
+  if (w < 16 || h < 16) return DSGPU_ERR_UNSUPPORTED;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void *drgb, *dclip = nullptr, *mid;
+  unsigned char* fl;
+  unsigned* cnt;
+  DS_CHECK(stage_in(ctx, flags, S_IN, raw, ((size_t)(h - 1) * pitch + w) * sizeof(uint16_t), &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &drgb));
+  if (out_clip) DS_CHECK(stage_out_ptr(ctx, flags, S_OUT2, out_clip, n * sizeof(float), &dclip));
+  DS_CHECK(scratch(ctx, S_RGB, n * 3 * sizeof(float), &mid));
+  DS_CHECK(fallback_scratch(ctx, w, h, patch, &fl, &cnt));
+  {
+    StageMark mark(ctx, DSGPU_STAGE_DEMOSAIC);
+    ds_src_u16 src{(const uint16_t*)din, pitch, black, {white[0], white[1], white[2]}};
+    DS_TRY(ds_launch_rcd_u16(ctx->stream, src, w, h, pat, mul, (float*)mid, (float*)dclip));
+    ctx->launches += 1;
+  }
+  {
+    StageMark mark(ctx, DSGPU_STAGE_CNN);
+    DS_TRY(ds_cnn_denoise(c->net, ctx->stream, (const float*)mid, w, h, h_param, search, patch, tau,
+                          DSGPU_CNN_STRENGTH_SCALE, (float*)drgb, fl, cnt));
+    ctx->launches += 2 + 8 + 8 + (tau > 0.f ? 2 : 0);
+  }
+  return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));
 }
 
 // ------------------------------------------------------------------ scenes

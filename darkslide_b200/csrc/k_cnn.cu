@@ -1,0 +1,716 @@
+// The learned stand-in for NLM: a residual CNN of 8 conv3x3 layers
+// (4 -> 48 -> ... -> 48 -> 3, ReLU between), input = demosaiced RGB plus a
+// constant map of the NLM strength, output = input RGB + network output.
+// It is trained on the GPU to reproduce plain NLM (enhance.rs:36-72) and
+// runs with NLM as the per-tile fallback.
+//
+// Tensor-core kernels: BF16 operands, FP32 accumulation (mma.sync m16n8k16 fed
+// by ldmatrix from shared memory). Activations are NHWC bf16 with the channel
+// count padded to a multiple of 16 (input 16, hidden 48; the last layer's
+// gradient 16). Every conv is an implicit GEMM: M = 16 output pixels of one
+// tile row per warp, N = output channels, K = 9 taps x input channels.
+//   forward       conv_fwd_kernel<CIN, COUT, EPI_RELU / EPI_RESID>
+//   data gradient conv_fwd_kernel with the tap-flipped, transposed weights and
+//                 EPI_MASK (the ReLU mask of the layer below)
+//   weight grad   conv_wgrad_kernel<CIN, COUTW>: M = out channels, N = in
+//                 channels, K = pixels; per-CTA partial sums reduced in a
+//                 fixed order (deterministic)
+#include <cuda_bf16.h>
+
+#include <vector>
+
+#include "internal.cuh"
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int CT_W = 16, CT_H = 8;             // output tile: 8 rows of 16 pixels
+constexpr int CT_XW = CT_W + 2, CT_XH = CT_H + 2;  // with the 1-pixel halo
+constexpr int CNN_THREADS = 256;
+
+enum { EPI_RELU = 0, EPI_MASK = 1, EPI_RESID = 2 };
+
+// shared-memory row stride (bytes) for c bf16 channels: an odd number of
+// 16-byte chunks, so the 8 rows of an ldmatrix phase hit 8 distinct chunks
+__host__ __device__ constexpr int row_stride(int c) { return c * 2 + 16; }
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ldsm_x4(unsigned a, unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2(unsigned a, unsigned& r0, unsigned& r1) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x4_t(unsigned a, unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
+}
+__device__ __forceinline__ void mma16816(float* d, unsigned a0, unsigned a1, unsigned a2, unsigned a3, unsigned b0,
+                                         unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+struct TileIdx {
+  int b, x0, y0;
+};
+__device__ __forceinline__ TileIdx tile_of(int t, int tiles_x, int tiles_y) {
+  TileIdx r;
+  const int per = tiles_x * tiles_y;
+  r.b = t / per;
+  const int q = t - r.b * per;
+  const int ty = q / tiles_x;
+  r.x0 = (q - ty * tiles_x) * CT_W;
+  r.y0 = ty * CT_H;
+  return r;
+}
+
+// stage an NHWC tile with a 1-pixel halo (zero outside the image)
+template <int C, int PW, int PH>
+__device__ __forceinline__ void stage_tile(unsigned char* dst, const bf16* __restrict__ src, int b, int H, int W,
+                                           int x0, int y0) {
+  constexpr int CH = C * 2 / 16, RS = row_stride(C);
+  for (int i = threadIdx.x; i < PH * PW * CH; i += CNN_THREADS) {
+    const int pix = i / CH, ch = i - pix * CH;
+    const int py = pix / PW, px = pix - py * PW;
+    const int gy = y0 + py, gx = x0 + px;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (gy >= 0 && gy < H && gx >= 0 && gx < W)
+      v = reinterpret_cast<const uint4*>(src + (((size_t)b * H + gy) * W + gx) * C)[ch];
+    *reinterpret_cast<uint4*>(dst + pix * RS + ch * 16) = v;
+  }
+}
+
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(CNN_THREADS) conv_fwd_kernel(const bf16* __restrict__ x, int B, int H, int W,
+                                                               const bf16* __restrict__ wt,
+                                                               const float* __restrict__ bias, bf16* __restrict__ y,
+                                                               const bf16* __restrict__ mask,
+                                                               const float* __restrict__ resid,
+                                                               float* __restrict__ yf) {
+  static_assert(CIN % 16 == 0 && COUT % 8 == 0, "channel padding");
+  constexpr int RSX = row_stride(CIN), RSW = row_stride(CIN), NT = COUT / 8;
+  extern __shared__ __align__(16) unsigned char sm[];
+  unsigned char* ws = sm;                    // [9][COUT] rows of CIN bf16
+  unsigned char* xs = sm + 9 * COUT * RSW;   // [CT_XH][CT_XW] pixels of CIN bf16
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  {
+    constexpr int CH = CIN * 2 / 16;
+    for (int i = tid; i < 9 * COUT * CH; i += CNN_THREADS) {
+      const int row = i / CH, ch = i - row * CH;
+      *reinterpret_cast<uint4*>(ws + row * RSW + ch * 16) = reinterpret_cast<const uint4*>(wt)[i];
+    }
+  }
+  const int tiles_x = (W + CT_W - 1) / CT_W, tiles_y = (H + CT_H - 1) / CT_H;
+  const int ntiles = B * tiles_x * tiles_y;
+  const int g = lane >> 2, c = lane & 3;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileIdx ti = tile_of(t, tiles_x, tiles_y);
+    __syncthreads();  // weights staged / previous tile consumed
+    stage_tile<CIN, CT_XW, CT_XH>(xs, x, ti.b, H, W, ti.x0 - 1, ti.y0 - 1);
+    __syncthreads();
+    float acc[NT][4];
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+#pragma unroll
+    for (int tap = 0; tap < 9; tap++) {
+      const int ky = tap / 3, kx = tap % 3;
+#pragma unroll
+      for (int kc = 0; kc < CIN / 16; kc++) {
+        unsigned a0, a1, a2, a3;
+        ldsm_x4(smem_u32(xs + ((warp + ky) * CT_XW + (lane & 15) + kx) * RSX + (kc * 16 + (lane >> 4) * 8) * 2), a0,
+                a1, a2, a3);
+#pragma unroll
+        for (int j = 0; j + 1 < NT; j += 2) {
+          const int co = (j + (lane >> 4)) * 8 + (lane & 7);
+          unsigned b0, b1, b2, b3;
+          ldsm_x4(smem_u32(ws + (tap * COUT + co) * RSW + (kc * 16 + ((lane >> 3) & 1) * 8) * 2), b0, b1, b2, b3);
+          mma16816(acc[j], a0, a1, a2, a3, b0, b1);
+          mma16816(acc[j + 1], a0, a1, a2, a3, b2, b3);
+        }
+        if (NT & 1) {
+          const int co = (NT - 1) * 8 + (lane & 7);
+          unsigned b0, b1;
+          ldsm_x2(smem_u32(ws + (tap * COUT + co) * RSW + (kc * 16 + ((lane >> 3) & 1) * 8) * 2), b0, b1);
+          mma16816(acc[NT - 1], a0, a1, a2, a3, b0, b1);
+        }
+      }
+    }
+    // epilogue: rows g and g+8 of the warp's 16 pixels, channels 2c, 2c+1 of each n8 tile
+    const int gy = ti.y0 + warp;
+    if (gy < H) {
+#pragma unroll
+      for (int half = 0; half < 2; half++) {
+        const int gx = ti.x0 + g + half * 8;
+        if (gx >= W) continue;
+        const size_t pix = ((size_t)ti.b * H + gy) * W + gx;
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+          const int co = j * 8 + 2 * c;
+          float v0 = acc[j][half * 2], v1 = acc[j][half * 2 + 1];
+          if (EPI == EPI_RELU) {
+            v0 = fmaxf(v0 + bias[co], 0.f);
+            v1 = fmaxf(v1 + bias[co + 1], 0.f);
+            *reinterpret_cast<__nv_bfloat162*>(y + pix * COUT + co) = __floats2bfloat162_rn(v0, v1);
+          } else if (EPI == EPI_MASK) {
+            const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162*>(mask + pix * COUT + co);
+            v0 = __bfloat162float(m.x) > 0.f ? v0 : 0.f;
+            v1 = __bfloat162float(m.y) > 0.f ? v1 : 0.f;
+            *reinterpret_cast<__nv_bfloat162*>(y + pix * COUT + co) = __floats2bfloat162_rn(v0, v1);
+          } else {  // EPI_RESID: out = input RGB + conv + bias, channels 0..2 in fp32
+            if (co < 3) yf[pix * 3 + co] = resid[pix * 3 + co] + (v0 + bias[co]);
+            if (co + 1 < 3) yf[pix * 3 + co + 1] = resid[pix * 3 + co + 1] + (v1 + bias[co + 1]);
+          }
+        }
+      }
+    }
+  }
+}
+
+// Weight gradient: dW[tap][co][ci] = sum_p dY[p][co] X[p + tap][ci]. A warp
+// owns up to 4 (tap, 16-channel block of co) units; K runs over the 16
+// pixels of each tile row. Partial sums per CTA go to `part`.
+template <int CIN, int COUTW>
+__global__ void __launch_bounds__(CNN_THREADS) conv_wgrad_kernel(const bf16* __restrict__ x,
+                                                                 const bf16* __restrict__ dy, int B, int H, int W,
+                                                                 float* __restrict__ part) {
+  constexpr int RSX = row_stride(CIN), RSD = row_stride(COUTW);
+  constexpr int MT = COUTW / 16, UNITS = 9 * MT, UPW = (UNITS + 7) / 8, NT = CIN / 8;
+  extern __shared__ __align__(16) unsigned char sm[];
+  unsigned char* xs = sm;                          // [CT_XH][CT_XW] x CIN
+  unsigned char* ds = sm + CT_XH * CT_XW * RSX;    // [CT_H][CT_W] x COUTW
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, c = lane & 3;
+  float acc[UPW][NT][4];
+#pragma unroll
+  for (int u = 0; u < UPW; u++)
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[u][j][0] = acc[u][j][1] = acc[u][j][2] = acc[u][j][3] = 0.f;
+  const int tiles_x = (W + CT_W - 1) / CT_W, tiles_y = (H + CT_H - 1) / CT_H;
+  const int ntiles = B * tiles_x * tiles_y;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileIdx ti = tile_of(t, tiles_x, tiles_y);
+    __syncthreads();
+    stage_tile<CIN, CT_XW, CT_XH>(xs, x, ti.b, H, W, ti.x0 - 1, ti.y0 - 1);
+    stage_tile<COUTW, CT_W, CT_H>(ds, dy, ti.b, H, W, ti.x0, ti.y0);  // zero outside the image
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < UPW; u++) {
+      const int unit = warp + u * 8;
+      if (unit >= UNITS) break;
+      const int tap = unit / MT, mt = unit - tap * MT;
+      const int ky = tap / 3, kx = tap % 3;
+#pragma unroll 1
+      for (int r = 0; r < CT_H; r++) {  // K: the 16 pixels of tile row r
+        unsigned a0, a1, a2, a3;
+        // A = dY^T: matrices (pixels 0-7, co 0-7), (pixels 0-7, co 8-15), (pixels 8-15, co 0-7), (8-15, 8-15)
+        {
+          const int pix = (lane & 7) + ((lane >> 4) & 1) * 8;
+          const int cb = ((lane >> 3) & 1) * 8;
+          ldsm_x4_t(smem_u32(ds + (r * CT_W + pix) * RSD + (mt * 16 + cb) * 2), a0, a1, a2, a3);
+        }
+#pragma unroll
+        for (int j = 0; j < NT; j += 2) {
+          // B = X shifted by the tap: matrices (pixels 0-7, ci j), (pixels 8-15, ci j), (0-7, j+1), (8-15, j+1)
+          const int pix = (lane & 7) + ((lane >> 3) & 1) * 8;
+          const int cj = (j + (lane >> 4)) * 8;
+          unsigned b0, b1, b2, b3;
+          ldsm_x4_t(smem_u32(xs + ((r + ky) * CT_XW + pix + kx) * RSX + cj * 2), b0, b1, b2, b3);
+          mma16816(acc[u][j], a0, a1, a2, a3, b0, b1);
+          if (j + 1 < NT) mma16816(acc[u][j + 1], a0, a1, a2, a3, b2, b3);
+        }
+      }
+    }
+  }
+  // write this CTA's partial sums: part[block][tap][co][ci]
+  float* P = part + (size_t)blockIdx.x * 9 * COUTW * CIN;
+#pragma unroll
+  for (int u = 0; u < UPW; u++) {
+    const int unit = warp + u * 8;
+    if (unit >= UNITS) break;
+    const int tap = unit / MT, mt = unit - tap * MT;
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+      const int co = mt * 16 + g, ci = j * 8 + 2 * c;
+      float* p0 = P + ((size_t)tap * COUTW + co) * CIN + ci;
+      p0[0] = acc[u][j][0];
+      p0[1] = acc[u][j][1];
+      p0[8 * CIN] = acc[u][j][2];
+      p0[8 * CIN + 1] = acc[u][j][3];
+    }
+  }
+}
+
+// Per-CTA channel sums of dY (bias gradient partials).
+template <int C>
+__global__ void bias_grad_kernel(const bf16* __restrict__ dy, size_t n, float* __restrict__ part) {
+  __shared__ float s[CNN_THREADS];
+  const int ch = threadIdx.x % C;
+  const int lanes = (CNN_THREADS / C) * C;  // threads that take part
+  float acc = 0.f;
+  if ((int)threadIdx.x < lanes)
+    for (size_t p = blockIdx.x * (size_t)(lanes / C) + threadIdx.x / C; p < n; p += (size_t)gridDim.x * (lanes / C))
+      acc += __bfloat162float(dy[p * C + ch]);
+  s[threadIdx.x] = (int)threadIdx.x < lanes ? acc : 0.f;
+  __syncthreads();
+  if ((int)threadIdx.x < C) {
+    float t = 0.f;
+    for (int i = threadIdx.x; i < lanes; i += C) t += s[i];
+    part[(size_t)blockIdx.x * C + threadIdx.x] = t;
+  }
+}
+
+// grads[layer] (real shape [9][cout][cin] then [cout]) from the partials
+__global__ void reduce_grads_kernel(const float* __restrict__ wpart, int nw, int coutw, int cinp,
+                                    const float* __restrict__ bpart, int nb, int cb, int cout, int cin,
+                                    float* __restrict__ gw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nwreal = 9 * cout * cin;
+  if (i < nwreal) {
+    const int tap = i / (cout * cin), r = i - tap * cout * cin, co = r / cin, ci = r - co * cin;
+    const size_t off = ((size_t)tap * coutw + co) * cinp + ci, stride = (size_t)9 * coutw * cinp;
+    float s = 0.f;
+    for (int k = 0; k < nw; k++) s += wpart[k * stride + off];
+    gw[i] = s;
+  } else if (i < nwreal + cout) {
+    const int co = i - nwreal;
+    float s = 0.f;
+    for (int k = 0; k < nb; k++) s += bpart[(size_t)k * cb + co];
+    gw[i] = s;
+  }
+}
+
+// out = in RGB (fp32) and a constant strength channel -> NHWC16 bf16
+__global__ void pack_input_kernel(const float* __restrict__ rgb, size_t n, const float* __restrict__ strength_map,
+                                  float strength, bf16* __restrict__ x) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  __align__(16) bf16 v[16];
+  v[0] = __float2bfloat16_rn(rgb[p * 3]);
+  v[1] = __float2bfloat16_rn(rgb[p * 3 + 1]);
+  v[2] = __float2bfloat16_rn(rgb[p * 3 + 2]);
+  v[3] = __float2bfloat16_rn(strength_map ? strength_map[p] : strength);
+#pragma unroll
+  for (int k = 4; k < 16; k++) v[k] = __float2bfloat16_rn(0.f);
+  reinterpret_cast<uint4*>(x + p * 16)[0] = reinterpret_cast<uint4*>(v)[0];
+  reinterpret_cast<uint4*>(x + p * 16)[1] = reinterpret_cast<uint4*>(v)[1];
+}
+
+// MSE over n pixels x 3 channels: dY = 2 (out - t) / (3n) into NHWC16 bf16
+// (channels 3..15 zero); per-CTA partial sums of (out - t)^2.
+__global__ void mse_kernel(const float* __restrict__ out, const float* __restrict__ tgt, size_t n,
+                           bf16* __restrict__ dy, float* __restrict__ part) {
+  __shared__ float s[CNN_THREADS];
+  const float scale = 2.0f / (3.0f * (float)n);
+  float acc = 0.f;
+  for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    __align__(16) bf16 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = __float2bfloat16_rn(0.f);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float d = out[p * 3 + k] - tgt[p * 3 + k];
+      acc += d * d;
+      v[k] = __float2bfloat16_rn(d * scale);
+    }
+    reinterpret_cast<uint4*>(dy + p * 16)[0] = reinterpret_cast<uint4*>(v)[0];
+    reinterpret_cast<uint4*>(dy + p * 16)[1] = reinterpret_cast<uint4*>(v)[1];
+  }
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int k = CNN_THREADS / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+
+__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ gr, float* __restrict__ m,
+                            float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = gr[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// master fp32 [9][cout][cin] + [cout] -> forward weights bf16 [9][coutp][cinp],
+// bias fp32 [coutp], and (when wd) data-gradient weights bf16
+// [9][cinp_d][coutp_d] with the taps flipped: wd[8 - tap][ci][co] = w[tap][co][ci].
+__global__ void pack_weights_kernel(const float* __restrict__ w, int cout, int cin, int coutp, int cinp,
+                                    bf16* __restrict__ wf, float* __restrict__ bias, bf16* __restrict__ wd,
+                                    int cinp_d, int coutp_d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = 9 * coutp * cinp;
+  if (i < nf) {
+    const int tap = i / (coutp * cinp), r = i - tap * coutp * cinp, co = r / cinp, ci = r - co * cinp;
+    const float v = (co < cout && ci < cin) ? w[(tap * cout + co) * cin + ci] : 0.f;
+    wf[i] = __float2bfloat16_rn(v);
+  }
+  if (i < coutp) bias[i] = i < cout ? w[9 * cout * cin + i] : 0.f;
+  if (wd) {
+    const int nd = 9 * cinp_d * coutp_d;
+    if (i < nd) {
+      const int tp = i / (cinp_d * coutp_d), r = i - tp * cinp_d * coutp_d, ci = r / coutp_d, co = r - ci * coutp_d;
+      const int tap = 8 - tp;
+      const float v = (co < cout && ci < cin) ? w[(tap * cout + co) * cin + ci] : 0.f;
+      wd[i] = __float2bfloat16_rn(v);
+    }
+  }
+}
+
+// Residual check of the learned output: one CTA per NLM tile (tile_w x
+// tile_h). The tile falls back to NLM when the RMS of what the network
+// removed, out - in, exceeds tau * sigma (sigma = the noise level implied by
+// the NLM strength, h / 1.5), or when the output is not finite.
+__global__ void residual_check_kernel(const float* __restrict__ in, const float* __restrict__ out, int w, int h,
+                                      int tile_w, int tile_h, float limit2, unsigned char* __restrict__ flags,
+                                      unsigned* __restrict__ count) {
+  __shared__ float s[CNN_THREADS];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  const int x0 = blockIdx.x * tile_w, y0 = blockIdx.y * tile_h;
+  float acc = 0.f;
+  int n = 0;
+  for (int i = threadIdx.x; i < tile_w * tile_h; i += CNN_THREADS) {
+    const int y = y0 + i / tile_w, x = x0 + i % tile_w;
+    if (x >= w || y >= h) continue;
+    const size_t p = ((size_t)y * w + x) * 3;
+    for (int k = 0; k < 3; k++) {
+      const float o = out[p + k];
+      if (!isfinite(o)) bad = 1;
+      const float d = o - in[p + k];
+      acc += d * d;
+    }
+    n += 3;
+  }
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int k = CNN_THREADS / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int tw = min(tile_w, w - x0), th = min(tile_h, h - y0);
+    const float mean = s[0] / (float)(3 * tw * th);
+    const unsigned char f = (bad || !(mean <= limit2)) ? 1 : 0;
+    flags[blockIdx.y * gridDim.x + blockIdx.x] = f;
+    if (f) atomicAdd(count, 1u);
+  }
+  (void)n;
+}
+
+// ------------------------------------------------------------------ host side
+
+template <int CIN, int COUT, int EPI>
+cudaError_t launch_fwd(cudaStream_t st, int grid, const bf16* x, int B, int H, int W, const bf16* wt,
+                       const float* bias, bf16* y, const bf16* mask, const float* resid, float* yf) {
+  const size_t smem = (size_t)9 * COUT * row_stride(CIN) + (size_t)CT_XH * CT_XW * row_stride(CIN);
+  cudaError_t e = cudaFuncSetAttribute(conv_fwd_kernel<CIN, COUT, EPI>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  conv_fwd_kernel<CIN, COUT, EPI><<<grid, CNN_THREADS, smem, st>>>(x, B, H, W, wt, bias, y, mask, resid, yf);
+  return cudaGetLastError();
+}
+
+template <int CIN, int COUTW>
+cudaError_t launch_wgrad(cudaStream_t st, int grid, const bf16* x, const bf16* dy, int B, int H, int W,
+                         float* part) {
+  const size_t smem = (size_t)CT_XH * CT_XW * row_stride(CIN) + (size_t)CT_H * CT_W * row_stride(COUTW);
+  cudaError_t e = cudaFuncSetAttribute(conv_wgrad_kernel<CIN, COUTW>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  conv_wgrad_kernel<CIN, COUTW><<<grid, CNN_THREADS, smem, st>>>(x, dy, B, H, W, part);
+  return cudaGetLastError();
+}
+
+// layer table: real and padded channel counts
+struct LayerSpec {
+  int cin, cout;     // real
+  int cinp, coutp;   // forward padding
+};
+constexpr int NL = 8;
+constexpr LayerSpec LAYERS[NL] = {{4, 48, 16, 48},  {48, 48, 48, 48}, {48, 48, 48, 48}, {48, 48, 48, 48},
+                                  {48, 48, 48, 48}, {48, 48, 48, 48}, {48, 48, 48, 48}, {48, 3, 48, 8}};
+
+}  // namespace
+
+// ----------------------------------------------------------------- network
+
+cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
+                              const void* const* wf, const float* const* bias, const float* rgb, float* out,
+                              int* err);
+
+struct DsCnn {
+  int device = 0;
+  bool use_tc = true;    // inference on tcgen05 (false: the mma.sync kernels)
+  int* err = nullptr;    // device status word of the tcgen05 kernels
+  int max_batch = 0, crop = 0;
+  int n_params = 0;
+  int off[NL + 1] = {};  // offsets of each layer in the flat parameter array
+  float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;
+  bf16* wf[NL] = {};
+  bf16* wd[NL] = {};
+  float* bias[NL] = {};
+  long long step = 0;
+  // training buffers (max_batch crops of crop x crop)
+  bf16* act[NL] = {};   // act[0] = packed input (16 ch), act[l] = output of layer l (48 ch), l = 1..7
+  bf16* gA = nullptr;   // gradient ping
+  bf16* gB = nullptr;   // gradient pong
+  bf16* dy8 = nullptr;  // 16 ch
+  float* out = nullptr;
+  float *wpart = nullptr, *bpart = nullptr, *lpart = nullptr;
+  int wgrid = 0, bgrid = 0;
+  // inference buffers (grown on demand)
+  bf16 *ia = nullptr, *ib = nullptr;
+  size_t infer_px = 0;
+  std::vector<void*> allocs;
+
+  void* alloc(size_t bytes, cudaError_t& e) {
+    void* p = nullptr;
+    e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e == cudaSuccess) allocs.push_back(p);
+    return p;
+  }
+  ~DsCnn() {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+size_t ds_cnn_param_count() {
+  size_t n = 0;
+  for (int l = 0; l < NL; l++) n += (size_t)9 * LAYERS[l].cout * LAYERS[l].cin + LAYERS[l].cout;
+  return n;
+}
+
+cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out) {
+  DsCnn* net = new DsCnn();
+  cudaError_t e = cudaGetDevice(&net->device);
+  if (e != cudaSuccess) {
+    delete net;
+    return e;
+  }
+  net->max_batch = max_batch;
+  net->crop = crop;
+  int o = 0;
+  for (int l = 0; l < NL; l++) {
+    net->off[l] = o;
+    o += 9 * LAYERS[l].cout * LAYERS[l].cin + LAYERS[l].cout;
+  }
+  net->off[NL] = o;
+  net->n_params = o;
+  const size_t pb = (size_t)o * sizeof(float);
+  net->params = (float*)net->alloc(pb, e);
+  if (e == cudaSuccess) net->grads = (float*)net->alloc(pb, e);
+  if (e == cudaSuccess) net->m = (float*)net->alloc(pb, e);
+  if (e == cudaSuccess) net->v = (float*)net->alloc(pb, e);
+  for (int l = 0; l < NL && e == cudaSuccess; l++) {
+    const LayerSpec L = LAYERS[l];
+    net->wf[l] = (bf16*)net->alloc((size_t)9 * L.coutp * L.cinp * sizeof(bf16), e);
+    if (e == cudaSuccess) net->bias[l] = (float*)net->alloc((size_t)L.coutp * sizeof(float), e);
+    if (e == cudaSuccess && l > 0) {
+      const int cd = l == NL - 1 ? 16 : L.coutp;  // the last layer's gradient is stored with 16 channels
+      net->wd[l] = (bf16*)net->alloc((size_t)9 * L.cinp * cd * sizeof(bf16), e);
+    }
+  }
+  if (e == cudaSuccess && max_batch > 0) {
+    const size_t px = (size_t)max_batch * crop * crop;
+    net->act[0] = (bf16*)net->alloc(px * 16 * sizeof(bf16), e);
+    for (int l = 1; l < NL && e == cudaSuccess; l++) net->act[l] = (bf16*)net->alloc(px * 48 * sizeof(bf16), e);
+    if (e == cudaSuccess) net->gA = (bf16*)net->alloc(px * 48 * sizeof(bf16), e);
+    if (e == cudaSuccess) net->gB = (bf16*)net->alloc(px * 48 * sizeof(bf16), e);
+    if (e == cudaSuccess) net->dy8 = (bf16*)net->alloc(px * 16 * sizeof(bf16), e);
+    if (e == cudaSuccess) net->out = (float*)net->alloc(px * 3 * sizeof(float), e);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+    net->wgrid = sms * 2;
+    net->bgrid = sms;
+    if (e == cudaSuccess) net->wpart = (float*)net->alloc((size_t)net->wgrid * 9 * 48 * 48 * sizeof(float), e);
+    if (e == cudaSuccess) net->bpart = (float*)net->alloc((size_t)net->bgrid * 48 * sizeof(float), e);
+    if (e == cudaSuccess) net->lpart = (float*)net->alloc((size_t)1024 * sizeof(float), e);
+  }
+  if (e == cudaSuccess) net->err = (int*)net->alloc(sizeof(int), e);
+  if (e == cudaSuccess) e = cudaMemset(net->err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(net->m, 0, pb);
+  if (e == cudaSuccess) e = cudaMemset(net->v, 0, pb);
+  if (e != cudaSuccess) {
+    delete net;
+    return e;
+  }
+  *out = net;
+  return cudaSuccess;
+}
+
+void ds_cnn_destroy(DsCnn* net) { delete net; }
+
+int ds_cnn_params(const DsCnn* net) { return net->n_params; }
+float* ds_cnn_param_ptr(DsCnn* net) { return net->params; }
+float* ds_cnn_grad_ptr(DsCnn* net) { return net->grads; }
+float* ds_cnn_moment_ptr(DsCnn* net, int which) { return which == 0 ? net->m : net->v; }
+long long* ds_cnn_step_ptr(DsCnn* net) { return &net->step; }
+
+cudaError_t ds_cnn_pack(DsCnn* net, cudaStream_t st) {
+  for (int l = 0; l < NL; l++) {
+    const LayerSpec L = LAYERS[l];
+    const int cd = l == NL - 1 ? 16 : L.coutp;
+    const int n = 9 * L.coutp * L.cinp > 9 * L.cinp * cd ? 9 * L.coutp * L.cinp : 9 * L.cinp * cd;
+    pack_weights_kernel<<<(n + 255) / 256, 256, 0, st>>>(net->params + net->off[l], L.cout, L.cin, L.coutp, L.cinp,
+                                                         net->wf[l], net->bias[l], net->wd[l], L.cinp, cd);
+  }
+  return cudaGetLastError();
+}
+
+// Forward through all layers. x16: packed input; rgb: fp32 input RGB (the
+// residual); out: fp32 RGB. acts: per-layer outputs (act[l] for l=1..7).
+static cudaError_t forward(DsCnn* net, cudaStream_t st, const bf16* x16, const float* rgb, int B, int H, int W,
+                           bf16* const* acts, float* out) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+  const int grid = sms * 3;
+  cudaError_t e = launch_fwd<16, 48, EPI_RELU>(st, grid, x16, B, H, W, net->wf[0], net->bias[0], acts[1], nullptr,
+                                               nullptr, nullptr);
+  for (int l = 1; l < NL - 1 && e == cudaSuccess; l++)
+    e = launch_fwd<48, 48, EPI_RELU>(st, grid, acts[l], B, H, W, net->wf[l], net->bias[l], acts[l + 1], nullptr,
+                                     nullptr, nullptr);
+  if (e == cudaSuccess)
+    e = launch_fwd<48, 8, EPI_RESID>(st, grid, acts[NL - 1], B, H, W, net->wf[NL - 1], net->bias[NL - 1], nullptr,
+                                     nullptr, rgb, out);
+  return e;
+}
+
+// Gradients of the MSE between the network's output on (rgb, strength) and
+// tgt into net->grads (real parameter layout); *loss_sum = sum of squared
+// errors. Inputs are device arrays of B crops of crop x crop pixels.
+cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, const float* strength_map,
+                             float strength, const float* tgt, int B, float* loss_sum_host) {
+  const int H = net->crop, W = net->crop;
+  const size_t n = (size_t)B * H * W;
+  cudaError_t e = ds_cnn_pack(net, st);
+  if (e != cudaSuccess) return e;
+  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, strength_map, strength, net->act[0]);
+  if ((e = forward(net, st, net->act[0], rgb, B, H, W, net->act, net->out)) != cudaSuccess) return e;
+  const int lgrid = 512;
+  mse_kernel<<<lgrid, CNN_THREADS, 0, st>>>(net->out, tgt, n, net->dy8, net->lpart);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+  const int grid = sms * 3;
+  // layer 8: dW from (act7, dy8); dA7 = dgrad(dy8) * [act7 > 0]
+  auto reduce = [&](int l, int coutw, int cinp, int cb) {
+    const LayerSpec L = LAYERS[l];
+    const int nreal = 9 * L.cout * L.cin + L.cout;
+    reduce_grads_kernel<<<(nreal + 255) / 256, 256, 0, st>>>(net->wpart, net->wgrid, coutw, cinp, net->bpart,
+                                                            net->bgrid, cb, L.cout, L.cin, net->grads + net->off[l]);
+  };
+  if ((e = launch_wgrad<48, 16>(st, net->wgrid, net->act[7], net->dy8, B, H, W, net->wpart)) != cudaSuccess) return e;
+  bias_grad_kernel<16><<<net->bgrid, CNN_THREADS, 0, st>>>(net->dy8, n, net->bpart);
+  reduce(7, 16, 48, 16);
+  bf16* g = net->gA;
+  bf16* gnext = net->gB;
+  if ((e = launch_fwd<16, 48, EPI_MASK>(st, grid, net->dy8, B, H, W, net->wd[7], nullptr, g, net->act[7], nullptr,
+                                        nullptr)) != cudaSuccess)
+    return e;
+  for (int l = 6; l >= 1; l--) {  // layers 7..2 (index l): dW from (act[l], g); g_next = dgrad(g) * [act[l] > 0]
+    if ((e = launch_wgrad<48, 48>(st, net->wgrid, net->act[l], g, B, H, W, net->wpart)) != cudaSuccess) return e;
+    bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
+    reduce(l, 48, 48, 48);
+    if ((e = launch_fwd<48, 48, EPI_MASK>(st, grid, g, B, H, W, net->wd[l], nullptr, gnext, net->act[l], nullptr,
+                                          nullptr)) != cudaSuccess)
+      return e;
+    bf16* tmp = g;
+    g = gnext;
+    gnext = tmp;
+  }
+  // layer 1: dW from (packed input, g)
+  if ((e = launch_wgrad<16, 48>(st, net->wgrid, net->act[0], g, B, H, W, net->wpart)) != cudaSuccess) return e;
+  bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
+  reduce(0, 48, 16, 48);
+  if (loss_sum_host) {
+    float part[512];
+    if ((e = cudaMemcpyAsync(part, net->lpart, lgrid * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    double s = 0;
+    for (int i = 0; i < lgrid; i++) s += part[i];
+    *loss_sum_host = (float)s;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  net->step++;
+  const float c1 = 1.0f - (float)pow(b1, (double)net->step), c2 = 1.0f - (float)pow(b2, (double)net->step);
+  adam_kernel<<<(net->n_params + 255) / 256, 256, 0, st>>>(net->params, net->grads, net->m, net->v, net->n_params, lr,
+                                                           b1, b2, eps, c1, c2);
+  return cudaGetLastError();
+}
+
+// Inference on a whole (w x h) RGB image; out = input + network(input).
+cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out) {
+  const size_t n = (size_t)w * h;
+  cudaError_t e = cudaSuccess;
+  if (net->infer_px < n) {
+    if (net->ia) cudaFree(net->ia);
+    if (net->ib) cudaFree(net->ib);
+    net->ia = net->ib = nullptr;
+    net->infer_px = 0;
+    if ((e = cudaMalloc(&net->ia, n * 48 * sizeof(bf16))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&net->ib, n * 48 * sizeof(bf16))) != cudaSuccess) return e;
+    net->infer_px = n;
+  }
+  if ((e = ds_cnn_pack(net, st)) != cudaSuccess) return e;
+  // ping-pong: input packed into ib (16 ch), layers alternate ia/ib
+  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, nullptr, strength, net->ib);
+  if (net->use_tc) {
+    const void* wf[NL];
+    const float* bs[NL];
+    for (int l = 0; l < NL; l++) {
+      wf[l] = net->wf[l];
+      bs[l] = net->bias[l];
+    }
+    return ds_cnn_forward_tc(st, net->ib, net->ia, net->ib, h, w, wf, bs, rgb, out, net->err);
+  }
+  bf16* acts[NL] = {net->ib, net->ia, net->ib, net->ia, net->ib, net->ia, net->ib, net->ia};
+  return forward(net, st, net->ib, rgb, 1, h, w, acts, out);
+}
+
+void ds_cnn_set_engine(DsCnn* net, int use_tc) { net->use_tc = use_tc != 0; }
+
+// DSGPU_OK, or the status the tensor-core kernels left (the word is reset).
+int ds_cnn_take_status(DsCnn* net, cudaStream_t st) {
+  int h = 0;
+  if (cudaMemcpyAsync(&h, net->err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DSGPU_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return DSGPU_ERR_CUDA;
+  if (h != 0) cudaMemsetAsync(net->err, 0, sizeof(int), st);
+  return h;
+}
+
+// The learned stand-in with its fallback: CNN, residual check per NLM tile,
+// NLM on the flagged tiles (written over the CNN output). flags_scratch holds
+// the tile flags followed by a u32 count; *fallback_count_dev receives it.
+cudaError_t ds_cnn_denoise(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float h_param, int search,
+                           int patch, float tau, float strength_scale, float* out, unsigned char* flags_scratch,
+                           unsigned* count_dev) {
+  cudaError_t e = ds_cnn_infer(net, st, rgb, w, h, h_param * strength_scale, out);
+  if (e != cudaSuccess) return e;
+  if (tau <= 0.f) return cudaSuccess;  // no fallback
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  if ((e = cudaMemsetAsync(count_dev, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
+  const float sigma = h_param / 1.5f;
+  residual_check_kernel<<<dim3(tx, ty), CNN_THREADS, 0, st>>>(rgb, out, w, h, tw, th, tau * tau * sigma * sigma,
+                                                              flags_scratch, count_dev);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return ds_launch_nlm_tiles(st, rgb, w, h, 3, h_param, search, patch, flags_scratch, out);
+}

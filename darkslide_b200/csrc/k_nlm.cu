@@ -81,7 +81,11 @@ size_t nlm_smem_bytes(int S, int P) {
 template <int P>
 __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
                                                                   int S, float sigma, const float* __restrict__ h_dev,
-                                                                  float norm2_log2e, float* __restrict__ out) {
+                                                                  float norm2_log2e,
+                                                                  const unsigned char* __restrict__ tile_flags,
+                                                                  float* __restrict__ out) {
+  // tile-list mode (the learned path's fallback): only flagged tiles run
+  if (tile_flags && !tile_flags[blockIdx.y * gridDim.x + blockIdx.x]) return;
   if (h_dev) {  // strength computed on the device (enhance.rs:40 floor included)
     const float hh = *h_dev;
     sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
@@ -226,13 +230,13 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* _
 
 template <int P>
 cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float sigma,
-                         const float* h_dev, float norm2_log2e, float* out) {
+                         const float* h_dev, float norm2_log2e, const unsigned char* flags, float* out) {
   constexpr int TY = HRW - 2 * P;
   const size_t smem = nlm_smem_bytes(S, P);
   cudaError_t e = cudaFuncSetAttribute(nlm_tile_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY, C);
-  nlm_tile_kernel<P><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, out);
+  nlm_tile_kernel<P><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags, out);
   return cudaGetLastError();
 }
 
@@ -241,18 +245,18 @@ cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, 
 namespace {
 
 cudaError_t dispatch_nlm(cudaStream_t st, const float* in, int w, int h, int C, int S, int P, float sigma,
-                         const float* h_dev, float* out) {
+                         const float* h_dev, float* out, const unsigned char* flags = nullptr) {
   const float norm = P == 0 ? 1.0f : 1.0f / (float)(2 * P + 1);
   const float n2l = norm * norm * 1.4426950408889634f;
   switch (P) {
-    case 0: return launch_nlm_p<0>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
-    case 1: return launch_nlm_p<1>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
-    case 2: return launch_nlm_p<2>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
-    case 3: return launch_nlm_p<3>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
-    case 4: return launch_nlm_p<4>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
-    case 5: return launch_nlm_p<5>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
-    case 6: return launch_nlm_p<6>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
-    case 7: return launch_nlm_p<7>(st, in, w, h, C, S, sigma, h_dev, n2l, out);
+    case 0: return launch_nlm_p<0>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 1: return launch_nlm_p<1>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 2: return launch_nlm_p<2>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 3: return launch_nlm_p<3>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 4: return launch_nlm_p<4>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 5: return launch_nlm_p<5>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 6: return launch_nlm_p<6>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 7: return launch_nlm_p<7>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -271,6 +275,25 @@ cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int ch
   const float norm = patch == 0 ? 1.0f : 1.0f / (float)(2 * patch + 1);
   const double sig2 = (double)norm * (double)norm / (double)h2 * 1.4426950408889634;
   return dispatch_nlm(st, in, w, h, channels, search, patch, (float)sqrt(sig2), nullptr, out);
+}
+
+// NLM tile geometry (the fallback's flag grid): tiles_x x tiles_y of 64 x (64 - 2P)
+void ds_nlm_tile_grid(int w, int h, int patch, int* tiles_x, int* tiles_y, int* tile_w, int* tile_h) {
+  const int ty = HRW - 2 * patch;
+  *tile_w = TX;
+  *tile_h = ty;
+  *tiles_x = (w + TX - 1) / TX;
+  *tiles_y = (h + ty - 1) / ty;
+}
+
+// NLM on the flagged tiles only (flags[tiles_y][tiles_x], 1 = recompute).
+cudaError_t ds_launch_nlm_tiles(cudaStream_t st, const float* in, int w, int h, int channels, float h_param,
+                                int search, int patch, const unsigned char* flags, float* out) {
+  if (search <= 0) return cudaErrorInvalidValue;
+  const float h2 = fmaxf(h_param * h_param, 1e-12f);
+  const float norm = patch == 0 ? 1.0f : 1.0f / (float)(2 * patch + 1);
+  const double sig2 = (double)norm * (double)norm / (double)h2 * 1.4426950408889634;
+  return dispatch_nlm(st, in, w, h, channels, search, patch, (float)sqrt(sig2), nullptr, out, flags);
 }
 
 // The same with the strength h read from device memory (search > 0).

@@ -75,7 +75,56 @@ __global__ void __launch_bounds__(256) ffma2_kernel(int iters, float seed, float
   if (s == 12345.678f) sink[0] = s;
 }
 
+// legacy warp-level tensor core: 8 independent mma.sync m16n8k16 bf16 chains
+__global__ void __launch_bounds__(256) mma_sync_kernel(int iters, unsigned seed, float* sink) {
+  float d[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++) d[i][0] = d[i][1] = d[i][2] = d[i][3] = 0.f;
+  const unsigned a0 = seed ^ threadIdx.x, a1 = a0 * 3u, a2 = a0 * 5u, a3 = a0 * 7u, b0 = a0 * 11u, b1 = a0 * 13u;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      asm volatile(
+          "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+          "{%0,%1,%2,%3};"
+          : "+f"(d[i][0]), "+f"(d[i][1]), "+f"(d[i][2]), "+f"(d[i][3])
+          : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s += d[i][0] + d[i][1] + d[i][2] + d[i][3];
+  if (s == 12345.678f) sink[0] = s;
+}
+
 }  // namespace
+
+// BF16 mma.sync throughput (FLOP/s), for the CNN kernels' roofline.
+cudaError_t ds_measure_mma_sync(cudaStream_t st, int device, double* flops) {
+  int sms = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  float* sink = nullptr;
+  if ((e = cudaMallocAsync(&sink, 16, st)) != cudaSuccess) return e;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int blocks = sms * 4, threads = 256, iters = 2048;
+  float ms = 0.f;
+  for (int rep = 0; rep < 2; rep++) {
+    cudaEventRecord(a, st);
+    mma_sync_kernel<<<blocks, threads, 0, st>>>(iters, 12345u, sink);
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+  }
+  *flops = 2.0 * 16 * 8 * 16 * 8.0 * iters * blocks * (threads / 32) / (ms * 1e-3);
+  e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFreeAsync(sink, st);
+  cudaStreamSynchronize(st);
+  return e;
+}
 
 // Times both kernels with CUDA events on `st`; returns FLOP/s and ex2/s.
 cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s,

@@ -4,6 +4,7 @@
     python -m darkslide_b200.profile_case rcd   # 6000x4000 u16 -> RCD (+clip)
     python -m darkslide_b200.profile_case develop [--w W --h H]
     python -m darkslide_b200.profile_case denoise  # enhance::denoise, amount 50
+    python -m darkslide_b200.profile_case cnn      # the learned stand-in (8 conv layers)
 
 Each case does one warm-up call and `--reps` timed calls on cuda:0 and
 prints the mean device time per call (CUDA events).
@@ -22,7 +23,7 @@ from darkslide_b200 import _lib
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise"])
+    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise", "cnn"])
     ap.add_argument("--w", type=int, default=0)
     ap.add_argument("--h", type=int, default=0)
     ap.add_argument("--reps", type=int, default=2)
@@ -59,6 +60,9 @@ def main():
         elif a.case == "rcd":
             r = L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(mul.ctypes.data),
                                  _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(clip.data_ptr()), _lib.DSGPU_ASYNC)
+        elif a.case == "cnn":
+            r = L.dsgpu_cnn_infer(ctx.handle, net.handle, vp(rgb.data_ptr()), w, h, 0.5, vp(out.data_ptr()),
+                                  _lib.DSGPU_ASYNC)
         elif a.case == "denoise":
             r = L.dsgpu_denoise(ctx.handle, vp(rgb.data_ptr()), w, h, 50.0, vp(out.data_ptr()), _lib.DSGPU_ASYNC)
         else:
@@ -67,7 +71,12 @@ def main():
                                     vp(out.data_ptr()), vp(0), _lib.DSGPU_ASYNC)
         ctx.check(r, a.case)
 
-    if a.case in ("nlm", "denoise"):  # input: the demosaiced frame
+    net = None
+    if a.case == "cnn":
+        from darkslide_b200 import cnn
+
+        net = cnn.ResidualCNN(ctx)
+    if a.case in ("nlm", "denoise", "cnn"):  # input: the demosaiced frame
         ctx.check(L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(mul.ctypes.data),
                                    _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(0), 0), "demosaic")
     call()

@@ -90,10 +90,13 @@ const char* dsgpu_last_error(dsgpu_ctx* ctx);
 #define DSGPU_STAGE_DEMOSAIC 0
 #define DSGPU_STAGE_NLM 1
 #define DSGPU_STAGE_COPY 2
+#define DSGPU_STAGE_CNN 3
 int dsgpu_profile(dsgpu_ctx* ctx, int enable);
 int dsgpu_stage_ms(dsgpu_ctx* ctx, int stage, double* total_ms, int* count);
 unsigned long long dsgpu_launch_count(dsgpu_ctx* ctx);
 int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops_per_s, double* ex2_per_s, double* ffma2_flops_per_s);
+/* BF16 mma.sync (m16n8k16, FP32 accumulate) throughput microbenchmark. */
+int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s);
 
 /* CFA normalisation of an integer raw: out = (raw - black) / max(white[c] - black, 1),
  * c the colour of the site; values are not clamped.
@@ -184,6 +187,57 @@ int dsgpu_develop_u16_noalloc(void* cuda_stream, const uint16_t* raw, int w, int
                               const uint8_t cfa[4], float black, const float white[3], const float mul[3],
                               float h_param, int search, int patch, float* out_rgb, float* out_clip,
                               unsigned flags);
+
+/* ------------------------------------------------------------ learned path
+ * A residual CNN standing in for nlm(): 8 conv3x3 layers (4 -> 48 -> ... ->
+ * 48 -> 3, ReLU), input = RGB plus a constant map of the NLM strength h,
+ * output = input + network. BF16 tensor-core kernels, FP32 accumulation,
+ * FP32 master weights and Adam state. Parameters are a flat float array:
+ * for each layer, weights [9 taps][cout][cin] then biases [cout].
+ * No counterpart in the reference (it has no learned denoiser); it is trained
+ * to reproduce enhance.rs:36-72 and falls back to it per tile. */
+typedef struct dsgpu_cnn dsgpu_cnn;
+int dsgpu_cnn_param_count(void);
+/* max_batch crops of crop x crop pixels for training (0, 0: inference only) */
+int dsgpu_cnn_create(dsgpu_ctx* ctx, int max_batch, int crop, dsgpu_cnn** out);
+int dsgpu_cnn_destroy(dsgpu_ctx* ctx, dsgpu_cnn* net);
+/* get (set = 0) or set (set = 1) parameters (which 0) or Adam moments
+ * (which 1, 2); buf may be NULL to move only the step counter. */
+int dsgpu_cnn_state(dsgpu_ctx* ctx, dsgpu_cnn* net, int which, float* buf, int set, long long* step,
+                    unsigned flags);
+/* Gradient of sum-of-squares / (3 n) between the network's output on
+ * (rgb[batch][crop][crop][3], strength map or constant) and target, into
+ * grads (device, param_count floats; may be NULL); loss_sum = sum of squared
+ * errors. Device buffers. */
+int dsgpu_cnn_gradients(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* rgb, const float* strength_map,
+                        float strength, const float* target, int batch, float* grads, float* loss_sum,
+                        unsigned flags);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on the same loss. Device buffers. */
+int dsgpu_cnn_train_step(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* rgb, const float* strength_map,
+                         float strength, const float* target, int batch, float lr, float* loss_sum);
+/* out = in + network(in, strength) on a whole interleaved RGB image
+ * (strength = DSGPU_CNN_STRENGTH_SCALE * h). */
+#define DSGPU_CNN_STRENGTH_SCALE 50.0f
+int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, int h, float strength,
+                    float* out_rgb, unsigned flags);
+/* Inference engine: 1 (default) tcgen05 tensor cores with TMEM
+ * accumulators, 0 the warp-level mma.sync kernels the training uses.
+ * A bounded device wait that gives up makes inference return
+ * DSGPU_ERR_TIMEOUT. */
+int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* net, int tensor_core_gen5);
+/* The learned stand-in for nlm(in, h_param, search, patch) with its per-tile
+ * fallback: the network runs on the whole image, then every NLM tile whose
+ * removed component out - in has an RMS above tau * h / 1.5 (or is not
+ * finite) is recomputed by plain NLM. tau <= 0 disables the fallback.
+ * *fallback_tiles (may be NULL) receives the number of tiles recomputed. */
+int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, int h, float h_param,
+                      int search, int patch, float tau, float* out_rgb, int* fallback_tiles, unsigned flags);
+/* u16 raw -> normalise -> RCD -> learned denoise with NLM fallback (the
+ * learned counterpart of dsgpu_develop_u16; w, h >= 16). */
+int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* net, const uint16_t* raw, int w, int h, size_t pitch_elems,
+                          const uint8_t cfa[4], float black, const float white[3], const float mul[3],
+                          float h_param, int search, int patch, float tau, float* out_rgb, float* out_clip,
+                          unsigned flags);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,82 @@
+"""FP64 numpy reference of the residual CNN (forward and backward).
+
+TEST INFRASTRUCTURE ONLY: the checker for the GPU CNN kernels' gradients.
+Same layer table, padding (zero, "same") and parameter layout as the
+library: per layer weights [9 taps][cout][cin] (tap = ky*3 + kx, offset
+(ky-1, kx-1)) then biases [cout]; loss = sum((out - target)^2) / (3 n).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+LAYERS = [(4, 48)] + [(48, 48)] * 6 + [(48, 3)]
+
+
+def unpack(params):
+    out, o = [], 0
+    for cin, cout in LAYERS:
+        nw = 9 * cout * cin
+        out.append((params[o:o + nw].reshape(9, cout, cin), params[o + nw:o + nw + cout]))
+        o += nw + cout
+    return out
+
+
+def conv(x, w, b):
+    B, H, W, _ = x.shape
+    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    out = np.zeros((B, H, W, w.shape[1]))
+    for t in range(9):
+        ky, kx = divmod(t, 3)
+        out += xp[:, ky:ky + H, kx:kx + W, :] @ w[t].T
+    return out + b
+
+
+def conv_back(x, w, dy):
+    """(dx, dw, db) of conv(x, w, b) given dy."""
+    B, H, W, _ = x.shape
+    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    dxp = np.zeros_like(xp)
+    dw = np.zeros_like(w)
+    for t in range(9):
+        ky, kx = divmod(t, 3)
+        xs = xp[:, ky:ky + H, kx:kx + W, :]
+        dw[t] = np.einsum("bhwo,bhwi->oi", dy, xs)
+        dxp[:, ky:ky + H, kx:kx + W, :] += dy @ w[t]
+    return dxp[:, 1:H + 1, 1:W + 1, :], dw, dy.sum(axis=(0, 1, 2))
+
+
+def forward(params, rgb, strength):
+    layers = unpack(np.asarray(params, np.float64))
+    x = np.concatenate([rgb, np.full(rgb.shape[:3] + (1,), strength)], axis=-1).astype(np.float64)
+    acts = [x]
+    for i, (w, b) in enumerate(layers):
+        y = conv(acts[-1], w, b)
+        acts.append(np.maximum(y, 0) if i < len(layers) - 1 else y)
+    return rgb + acts[-1], acts
+
+
+def gradients(params, rgb, strength, target):
+    """(flat gradient, loss_sum) of sum((out - target)^2) / (3 n)."""
+    layers = unpack(np.asarray(params, np.float64))
+    out, acts = forward(params, rgb, strength)
+    n = rgb.shape[0] * rgb.shape[1] * rgb.shape[2]
+    d = out - target
+    dy = 2.0 * d / (3.0 * n)
+    grads = []
+    for i in range(len(layers) - 1, -1, -1):
+        w, _ = layers[i]
+        dx, dw, db = conv_back(acts[i], w, dy)
+        grads.append((dw, db))
+        if i > 0:
+            dy = dx * (acts[i] > 0)
+    flat = []
+    for dw, db in reversed(grads):
+        flat += [dw.ravel(), db.ravel()]
+    return np.concatenate(flat), float((d ** 2).sum())
+
+
+def bf16_round(a):
+    """Round float32 values to bfloat16 (nearest-even) and back."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32)

@@ -1,0 +1,142 @@
+"""The learned path's tensor-core kernels against the FP64 reference
+(oracle/cnn_ref.py), plus Adam, checkpoint/resume and training.
+
+The GPU keeps weights, inputs, activations and gradients in BF16 (8-bit
+mantissa) with FP32 accumulation, so it is compared with an FP64 reference fed
+the same BF16-rounded weights and inputs: outputs to 2e-2 of their scale,
+gradients per layer by cosine similarity >= 0.995 and relative L2 error
+<= 5e-2."""
+import os
+
+import numpy as np
+import pytest
+
+import darkslide_b200 as ds
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_dev():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from darkslide_b200 import build
+
+    build.build()
+    return torch, torch.device("cuda", 0)
+
+
+def _batch(torch, dev, B, crop, seed):
+    rng = np.random.default_rng(seed)
+    rgb = rng.uniform(0.05, 0.9, (B, crop, crop, 3)).astype(np.float32)
+    tgt = (rgb + rng.normal(0, 0.02, rgb.shape)).astype(np.float32)
+    return rgb, tgt, torch.from_numpy(rgb).to(dev), torch.from_numpy(tgt).to(dev)
+
+
+def test_forward_matches_fp64(torch_dev):
+    import cnn_ref as C
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    p = cnn.init_params(3)
+    p[-1299:] = np.random.default_rng(3).normal(0, 0.05, 1299)  # a non-zero last layer
+    net = cnn.ResidualCNN(params=p)
+    rgb = np.random.default_rng(1).uniform(0.05, 0.9, (37, 45, 3)).astype(np.float32)
+    out = net.infer(ds.Image3(45, 37, rgb), 0.01).data
+    s = 0.01 * cnn.STRENGTH_SCALE
+    ref, _ = C.forward(C.bf16_round(p), C.bf16_round(rgb)[None], float(C.bf16_round(np.float32([s]))[0]))
+    ref = ref[0] - C.bf16_round(rgb) + rgb  # the residual adds the fp32 input
+    scale = np.abs(ref - rgb).max()
+    assert np.abs(out - ref).max() <= 2e-2 * max(scale, 1e-3)
+
+
+@pytest.mark.parametrize("crop", [16, 20])
+def test_gradients_match_fp64(torch_dev, crop):
+    import cnn_ref as C
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    p = cnn.init_params(5)
+    p[-1299:] = np.random.default_rng(5).normal(0, 0.05, 1299)
+    net = cnn.ResidualCNN(max_batch=2, crop=crop, params=p)
+    rgb, tgt, trgb, ttgt = _batch(torch, dev, 2, crop, 7)
+    s = 0.5
+    g, loss = net.gradients(trgb, s, ttgt)
+    g = g.cpu().numpy()
+    gr, loss_r = C.gradients(C.bf16_round(p), C.bf16_round(rgb), float(C.bf16_round(np.float32([s]))[0]), tgt)
+    assert abs(loss - loss_r) <= 2e-2 * loss_r
+    for i, (ws, bs, _) in enumerate(cnn.layer_slices()):
+        for sl in (ws, bs):
+            a, b = g[sl], gr[sl]
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+            rel = float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30))
+            assert cos >= 0.995 and rel <= 5e-2, (i, sl, cos, rel)
+
+
+def test_adam_step_and_bit_identical_resume(torch_dev, tmp_path):
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    batches = [_batch(torch, dev, 2, 16, 20 + k)[2:] for k in range(5)]
+    net = cnn.ResidualCNN(max_batch=2, crop=16, seed=9)
+    p0 = net.get_params()
+    g, _ = net.gradients(*batches[0][:1], 0.5, batches[0][1])
+    net.train_step(batches[0][0], 0.5, batches[0][1], 1e-3)
+    # first Adam step: m = 0.1 g, v = 0.001 g^2 -> update = lr * g / (|g| + eps)
+    g = g.cpu().numpy()
+    exp = p0 - 1e-3 * g / (np.abs(g) + 1e-8)
+    np.testing.assert_allclose(net.get_params(), exp, rtol=1e-5, atol=1e-8)
+    for k in range(1, 3):
+        net.train_step(batches[k][0], 0.5, batches[k][1], 1e-3)
+    path = os.path.join(tmp_path, "ck.bin")
+    net.save(path)
+    for k in range(3, 5):
+        net.train_step(batches[k][0], 0.5, batches[k][1], 1e-3)
+    direct = net.get_params()
+    net2 = cnn.ResidualCNN(max_batch=2, crop=16, seed=1)
+    net2.load(path)
+    assert net2.step == 3
+    for k in range(3, 5):
+        net2.train_step(batches[k][0], 0.5, batches[k][1], 1e-3)
+    np.testing.assert_array_equal(net2.get_params(), direct)
+
+
+def test_training_reduces_loss(torch_dev):
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    rng = np.random.default_rng(0)
+    clean = np.repeat(rng.uniform(0.2, 0.8, (8, 1, 1, 3)), 32, 1).repeat(32, 2).astype(np.float32)
+    noisy = (clean + rng.normal(0, 0.05, clean.shape)).astype(np.float32)
+    x, t = torch.from_numpy(noisy).to(dev), torch.from_numpy(clean).to(dev)
+    net = cnn.ResidualCNN(max_batch=8, crop=32, seed=2)
+    first = net.train_step(x, 0.5, t, 2e-3)
+    for _ in range(300):
+        last = net.train_step(x, 0.5, t, 2e-3)
+    assert last < 0.8 * first, (first, last)
+
+
+@pytest.mark.parametrize("hw", [(37, 45), (130, 300), (256, 129)])
+def test_tensor_core_engine_matches_mma_sync_and_fp64(torch_dev, hw):
+    """tcgen05 inference (default engine) against the mma.sync kernels and the
+    FP64 reference on the same weights."""
+    import cnn_ref as C
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    h, w = hw
+    p = cnn.init_params(11)
+    p[-1299:] = np.random.default_rng(11).normal(0, 0.05, 1299)
+    net = cnn.ResidualCNN(params=p)
+    rgb = np.random.default_rng(h).uniform(0.05, 0.9, (h, w, 3)).astype(np.float32)
+    tc = net.infer(ds.Image3(w, h, rgb), 0.01).data
+    net.set_engine(False)
+    ms = net.infer(ds.Image3(w, h, rgb), 0.01).data
+    ref, _ = C.forward(C.bf16_round(p), C.bf16_round(rgb)[None], float(C.bf16_round(np.float32([0.5]))[0]))
+    ref = ref[0] - C.bf16_round(rgb) + rgb
+    scale = max(np.abs(ref - rgb).max(), 1e-3)
+    assert np.isfinite(tc).all()
+    assert np.abs(tc - ms).max() <= 2e-2 * scale
+    assert np.abs(tc - ref).max() <= 2e-2 * scale

@@ -146,3 +146,21 @@ def test_denoise_reduces_noise(oracle):
     out, sigma = oracle.denoise(noisy, 60)
     assert sigma > 0
     assert ((out - clean) ** 2).sum() < ((noisy - clean) ** 2).sum() * 0.5
+
+
+def test_cnn_reference_gradients_match_finite_differences():
+    """The FP64 CNN reference (oracle/cnn_ref.py) against central differences."""
+    import cnn_ref as C
+
+    rng = np.random.default_rng(0)
+    n = sum(9 * co * ci + co for ci, co in C.LAYERS)
+    p = rng.normal(0, 0.1, n)
+    rgb = rng.uniform(0, 1, (1, 5, 6, 3))
+    tgt = rgb + rng.normal(0, 0.05, rgb.shape)
+    g, _ = C.gradients(p, rgb, 0.5, tgt)
+    loss = lambda q: C.gradients(q, rgb, 0.5, tgt)[1] / (3 * 30)
+    for idx in [0, 100, 1800, 25000, n - 5, n - 1]:
+        e = np.zeros(n)
+        e[idx] = 1e-6
+        fd = (loss(p + e) - loss(p - e)) / 2e-6
+        assert abs(g[idx] - fd) <= 1e-6 + 1e-5 * abs(fd), (idx, g[idx], fd)
