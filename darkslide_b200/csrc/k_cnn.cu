@@ -464,6 +464,7 @@ struct DsCnn {
   bf16* wd[NL] = {};
   float* bias[NL] = {};
   long long step = 0;
+  bool packed = false;   // wf/wd/bias match params (cleared whenever params may change)
   // training buffers (max_batch crops of crop x crop)
   bf16* act[NL] = {};   // act[0] = packed input (16 ch), act[l] = output of layer l (48 ch), l = 1..7
   bf16* gA = nullptr;   // gradient ping
@@ -555,12 +556,16 @@ cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out) {
 void ds_cnn_destroy(DsCnn* net) { delete net; }
 
 int ds_cnn_params(const DsCnn* net) { return net->n_params; }
-float* ds_cnn_param_ptr(DsCnn* net) { return net->params; }
+float* ds_cnn_param_ptr(DsCnn* net) {
+  net->packed = false;  // the caller may write through it
+  return net->params;
+}
 float* ds_cnn_grad_ptr(DsCnn* net) { return net->grads; }
 float* ds_cnn_moment_ptr(DsCnn* net, int which) { return which == 0 ? net->m : net->v; }
 long long* ds_cnn_step_ptr(DsCnn* net) { return &net->step; }
 
 cudaError_t ds_cnn_pack(DsCnn* net, cudaStream_t st) {
+  if (net->packed) return cudaSuccess;
   for (int l = 0; l < NL; l++) {
     const LayerSpec L = LAYERS[l];
     const int cd = l == NL - 1 ? 16 : L.coutp;
@@ -568,7 +573,9 @@ cudaError_t ds_cnn_pack(DsCnn* net, cudaStream_t st) {
     pack_weights_kernel<<<(n + 255) / 256, 256, 0, st>>>(net->params + net->off[l], L.cout, L.cin, L.coutp, L.cinp,
                                                          net->wf[l], net->bias[l], net->wd[l], L.cinp, cd);
   }
-  return cudaGetLastError();
+  const cudaError_t e = cudaGetLastError();
+  net->packed = e == cudaSuccess;
+  return e;
 }
 
 // Forward through all layers. x16: packed input; rgb: fp32 input RGB (the
@@ -650,6 +657,7 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
 cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr) {
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   net->step++;
+  net->packed = false;
   const float c1 = 1.0f - (float)pow(b1, (double)net->step), c2 = 1.0f - (float)pow(b2, (double)net->step);
   adam_kernel<<<(net->n_params + 255) / 256, 256, 0, st>>>(net->params, net->grads, net->m, net->v, net->n_params, lr,
                                                            b1, b2, eps, c1, c2);
