@@ -302,6 +302,28 @@ __global__ void pack_input_kernel(const float* __restrict__ rgb, size_t n, const
   reinterpret_cast<uint4*>(x + p * 16)[1] = reinterpret_cast<uint4*>(v)[1];
 }
 
+// The tensor-core engine's input: [2][h][wp][8] bf16 (channels 0-2 RGB, 3 the
+// strength, 4-15 zero; columns w..wp-1 zero).
+__global__ void pack_input_tc_kernel(const float* __restrict__ rgb, int w, int h, int wp, float strength,
+                                     bf16* __restrict__ x) {
+  const size_t n = (size_t)wp * h;
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int py = (int)(p / wp), px = (int)(p - (size_t)py * wp);
+  __align__(16) bf16 v[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) v[k] = __float2bfloat16_rn(0.f);
+  if (px < w) {
+    const size_t q = (size_t)py * w + px;
+    v[0] = __float2bfloat16_rn(rgb[q * 3]);
+    v[1] = __float2bfloat16_rn(rgb[q * 3 + 1]);
+    v[2] = __float2bfloat16_rn(rgb[q * 3 + 2]);
+    v[3] = __float2bfloat16_rn(strength);
+  }
+  reinterpret_cast<uint4*>(x)[p] = reinterpret_cast<uint4*>(v)[0];
+  reinterpret_cast<uint4*>(x)[n + p] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 // MSE over n pixels x 3 channels: dY = 2 (out - t) / (3n) into NHWC16 bf16
 // (channels 3..15 zero); per-CTA partial sums of (out - t)^2.
 __global__ void mse_kernel(const float* __restrict__ out, const float* __restrict__ tgt, size_t n,
@@ -667,20 +689,22 @@ cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr) {
 // Inference on a whole (w x h) RGB image; out = input + network(input).
 cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out) {
   const size_t n = (size_t)w * h;
+  const int wp = (w + 3) / 4 * 4;  // the tensor-core engine pads rows to 4 pixels
+  const size_t na = (size_t)wp * h;
   cudaError_t e = cudaSuccess;
-  if (net->infer_px < n) {
+  if (net->infer_px < na) {
     if (net->ia) cudaFree(net->ia);
     if (net->ib) cudaFree(net->ib);
     net->ia = net->ib = nullptr;
     net->infer_px = 0;
-    if ((e = cudaMalloc(&net->ia, n * 48 * sizeof(bf16))) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&net->ib, n * 48 * sizeof(bf16))) != cudaSuccess) return e;
-    net->infer_px = n;
+    if ((e = cudaMalloc(&net->ia, na * 48 * sizeof(bf16))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&net->ib, na * 48 * sizeof(bf16))) != cudaSuccess) return e;
+    net->infer_px = na;
   }
   if ((e = ds_cnn_pack(net, st)) != cudaSuccess) return e;
   // ping-pong: input packed into ib (16 ch), layers alternate ia/ib
-  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, nullptr, strength, net->ib);
   if (net->use_tc) {
+    pack_input_tc_kernel<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(rgb, w, h, wp, strength, net->ib);
     const void* wf[NL];
     const float* bs[NL];
     for (int l = 0; l < NL; l++) {
@@ -689,6 +713,7 @@ cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, i
     }
     return ds_cnn_forward_tc(st, net->ib, net->ia, net->ib, h, w, wf, bs, rgb, out, net->err);
   }
+  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, nullptr, strength, net->ib);
   bf16* acts[NL] = {net->ib, net->ia, net->ib, net->ia, net->ib, net->ia, net->ib, net->ia};
   return forward(net, st, net->ib, rgb, 1, h, w, acts, out);
 }

@@ -2,13 +2,22 @@
 // cores (tcgen05). Same network and tensors as k_cnn.cu (NHWC bf16
 // activations, [9][cout][cin] bf16 weights); the difference is the engine.
 //
-// Layout. Operands sit in shared memory in the canonical no-swizzle K-major
-// layout (core matrices of 8 rows x 16 bytes). The input tile (TR+2 rows x
-// 130 pixels, one pixel of halo each side) is stored channel-block-major,
-// [8-channel block][row][pixel][8 channels], so the A operand (M = 128
-// pixels, K = 16 channels) of any tap is the same layout shifted by whole
-// pixels: one descriptor per (input row, kx), no im2col copy. One TMA box per
-// 8-channel block loads it, zero-filled outside the image.
+// Layout. Activations live in HBM channel-block-major, [C/8][H][Wp][8] bf16
+// (16 bytes per pixel and block; Wp = W rounded up to 4, padding columns
+// zero), so one row of a block is contiguous. The operands sit in shared
+// memory in the canonical no-swizzle K-major layout (core matrices of 8 rows
+// x 16 bytes). The input tile (TR+2 rows x 136 pixels, x0-4 .. x0+131) is
+// stored the same way, [block][row][pixel][8 channels], so the A operand
+// (M = 128 pixels, K = 16 channels) of any tap is the layout shifted by whole
+// pixels: one descriptor per (input row, kx), no im2col copy. The TMA tensor
+// map sees a block as 64-byte groups of 4 pixels (a 16-byte innermost box
+// row would move a 32-byte sector per 16 bytes); one box per block loads the
+// tile, zero-filled outside the image. The epilogue's stores of a block are
+// 512 contiguous bytes per warp.
+//
+// Pipeline. The staged input goes through a ring of 6 shared-memory slots,
+// one per (tile, 16-channel K step), so TMA runs up to two tiles ahead of
+// the MMAs and a slot is released after a third of a tile's MMAs.
 //
 // Stacked taps. Input row j feeds output rows j, j-1, j-2 through weight
 // rows ky = 0, 1, 2. The three ky weight blocks are stacked along N, and the
@@ -19,14 +28,15 @@
 // math, so stacking cuts the tensor time per output row by ~1.7x. The first
 // MMA into an output row's accumulator is split off with accumulate = 0.
 //
-// Roles (one persistent CTA of 192 threads per SM, weights staged once):
-//   warp 5  TMA producer: input tile k into shared-memory stage k % 2;
-//   warp 4  MMA issuer: tcgen05.mma.cta_group::1.kind::f16 (BF16 in, FP32
+// Roles (one persistent CTA of 320 threads per SM, weights staged once):
+//   warp 9  TMA producer: the K steps of tile k into ring slots;
+//   warp 8  MMA issuer: tcgen05.mma.cta_group::1.kind::f16 (BF16 in, FP32
 //           accumulate) into TMEM accumulator set k % 2, then tcgen05.commit
 //           to release the smem stage and to hand the set to the epilogue;
-//   warps 0-3  epilogue: tcgen05.ld of their 32 TMEM lanes (pixels), bias,
-//           ReLU or residual, straight to global memory; they release the
-//           accumulator set after reading it.
+//   warps 0-7  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (pixels)
+//           of output rows 2 (w / 4) and 2 (w / 4) + 1 with tcgen05.ld, adds
+//           bias, applies ReLU or the residual and stores straight to global
+//           memory; each warp releases the accumulator set after its reads.
 // Every mbarrier wait is bounded in time (2 s); a wait that gives up sets a
 // CTA-wide abort flag, which every other wait honours, reports
 // DSGPU_ERR_TIMEOUT through `err`, and the CTA waits (bounded) for its copies
@@ -42,13 +52,17 @@ namespace {
 
 typedef __nv_bfloat16 bf16;
 
-constexpr int TC_EPI_WARPS = 4;
+constexpr int TC_EPI_WARPS = 8;                    // two per TMEM lane quarter
 constexpr int TC_THREADS = 32 * (TC_EPI_WARPS + 2);  // + MMA warp + TMA warp
 constexpr int TC_M = 128;                          // pixels per MMA (one output-row segment)
 constexpr int TC_TR = 4;                           // output rows per tile
-constexpr int TC_PW = TC_M + 2;                    // staged pixels per row (1-pixel halo each side)
+constexpr int TC_PG = 4;                           // pixels per TMA element group (64-byte box rows)
+constexpr int TC_PW = TC_M + 2 * TC_PG;            // staged pixels per row: x0-4 .. x0+131
 constexpr int TC_PR = TC_TR + 2;                   // staged rows
-constexpr int TC_SLAB = ((TC_PW * TC_PR * 16 + 127) / 128) * 128;  // bytes per 8-channel block, 128-B aligned
+constexpr int TC_SLAB = TC_PW * TC_PR * 16;        // bytes per 8-channel block (13056, 128-B multiple)
+constexpr int TC_SUB = 2 * TC_SLAB;                // one ring slot: the 16 channels of one K step
+constexpr int TC_RING = 6;                         // ring slots (two tiles of a 48-channel input)
+static_assert(TC_SLAB % 128 == 0, "TMA destinations must stay 128-byte aligned");
 constexpr int TC_TMEM_COLS = 512;                  // accumulator sets at columns 0 and 256
 constexpr size_t TC_MIN_SMEM = 120 * 1024;         // keeps one CTA per SM (the TMEM plan assumes it)
 constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
@@ -134,12 +148,13 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-// TMA load of one 3-D box (channels, x, y) into shared memory, completing on bar
-__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, int c, int x, int y, unsigned bar) {
+// TMA load of one 4-D box (channel within a 4-pixel group, group, y, block) into
+// shared memory, completing on bar
+__device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map, int x, int y, int cb, unsigned bar) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-      "[%5];" ::"r"(dst),
-      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c), "r"(x), "r"(y), "r"(bar)
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(x), "r"(y), "r"(cb), "r"(bar)
       : "memory");
 }
 
@@ -147,8 +162,11 @@ __device__ __forceinline__ void mma_commit(unsigned bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-// x: [H][W][CIN] bf16 through `xmap` (box 8 x TC_PW x TC_PR); wt: [9][COUT_G][CIN]
-// bf16; NK: output channels per ky block (COUT_G padded to a multiple of 16).
+// x: [CIN/8][H][Wp][8] bf16 (Wp = W rounded up to 4; columns W..Wp-1 zero)
+// through `xmap` (4-pixel groups, box 32 x TC_PW/4 x TC_PR x 1); wt:
+// [9][COUT_G][CIN] bf16; NK: output channels per ky block (COUT_G padded to a
+// multiple of 16); y: [COUT_G/8][H][Wp][8] bf16 (ReLU; padding columns
+// written as zero) or yf: [H][W][3] fp32 = resid + conv (residual).
 template <int CIN, int COUT_G, int NK, int EPI>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     conv_tc_kernel(const __grid_constant__ CUtensorMap xmap, int H, int W, const bf16* __restrict__ wt,
@@ -156,24 +174,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                    float* __restrict__ yf, int* __restrict__ err) {
   static_assert(CIN % 16 == 0 && NK % 16 == 0 && NK >= COUT_G && TC_TR * NK <= 256 && 3 * NK <= 256, "shapes");
   constexpr int CB = CIN / 8;              // 8-channel blocks of the input
-  constexpr int A_BYTES = CB * TC_SLAB;    // one staged tile
+  constexpr int KS = CIN / 16;             // K steps (ring slots) per tile
+  constexpr int A_BYTES = TC_RING * TC_SUB;
   constexpr int NS = 3 * NK;               // stacked B rows (ky, co)
   constexpr int B_BYTES = 3 * CB * NS * 16;  // weights, [kx][cb][ky*NK + co][8]
-  constexpr unsigned TX_BYTES = CB * 8 * TC_PW * TC_PR * 2;
+  constexpr unsigned TX_BYTES = 2 * 8 * TC_PW * TC_PR * 2;  // one slot
   extern __shared__ __align__(128) unsigned char sm[];
-  unsigned char* As = sm;                  // two stages
-  unsigned char* Bs = sm + 2 * A_BYTES;
-  float* bias_s = reinterpret_cast<float*>(sm + 2 * A_BYTES + B_BYTES);  // NK floats
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + 2 * A_BYTES + B_BYTES + NK * 4);
-  // bars: full[2], empty[2], tfull[2], tempty[2]
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 8);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 8) + 1;
+  unsigned char* As = sm;                  // ring of TC_RING slots
+  unsigned char* Bs = sm + A_BYTES;
+  float* bias_s = reinterpret_cast<float*>(sm + A_BYTES + B_BYTES);  // NK floats
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + A_BYTES + B_BYTES + NK * 4);
+  // bars: full[TC_RING], empty[TC_RING], tfull[2], tempty[2]
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * TC_RING + 4);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot) + 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned bar0 = smem_u32(bars);
-  auto full = [&](int s) { return bar0 + 8u * s; };
-  auto empty = [&](int s) { return bar0 + 16u + 8u * s; };
-  auto tfull = [&](int s) { return bar0 + 32u + 8u * s; };
-  auto tempty = [&](int s) { return bar0 + 48u + 8u * s; };
+  auto full = [&](int q) { return bar0 + 8u * q; };
+  auto empty = [&](int q) { return bar0 + 8u * (TC_RING + q); };
+  auto tfull = [&](int s) { return bar0 + 8u * (2 * TC_RING + s); };
+  auto tempty = [&](int s) { return bar0 + 8u * (2 * TC_RING + 2 + s); };
+  const int Wp = (W + TC_PG - 1) / TC_PG * TC_PG;
 
   for (int i = tid; i < 3 * CB * NS; i += TC_THREADS) {
     const int kx = i / (CB * NS), r = i - kx * CB * NS, cb = r / NS, n = r - cb * NS;
@@ -190,9 +210,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
+    for (int q = 0; q < TC_RING; q++) {
+      mbar_init(full(q), 1);
+      mbar_init(empty(q), 1);
+    }
     for (int s = 0; s < 2; s++) {
-      mbar_init(full(s), 1);
-      mbar_init(empty(s), 1);
       mbar_init(tfull(s), 1);
       mbar_init(tempty(s), TC_EPI_WARPS);
     }
@@ -219,69 +241,89 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // ---------------- TMA producer
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&xmap)) : "memory");
-      int k = 0;
-      for (; k < my_tiles; k++) {
-        const int s = k & 1;
-        if (!mbar_wait(empty(s), ((k >> 1) & 1) ^ 1, abort_flag)) break;
+      int g = 0;  // ring slot uses so far
+      for (int k = 0; k < my_tiles; k++) {
         int x0, y0;
         tile_xy(k, x0, y0);
-        mbar_expect_tx(full(s), TX_BYTES);
-        const unsigned dst = smem_u32(As) + (unsigned)(s * A_BYTES);
-#pragma unroll
-        for (int cb = 0; cb < CB; cb++) tma_load_3d(dst + cb * TC_SLAB, &xmap, cb * 8, x0 - 1, y0 - 1, full(s));
+        bool ok = true;
+        for (int kc = 0; kc < KS; kc++, g++) {
+          const int q = g % TC_RING;
+          if (!(ok = mbar_wait(empty(q), ((g / TC_RING) & 1) ^ 1, abort_flag))) break;
+          mbar_expect_tx(full(q), TX_BYTES);
+          const unsigned dst = smem_u32(As) + (unsigned)(q * TC_SUB);
+          tma_load_4d(dst, &xmap, x0 / TC_PG - 1, y0 - 1, 2 * kc, full(q));
+          tma_load_4d(dst + TC_SLAB, &xmap, x0 / TC_PG - 1, y0 - 1, 2 * kc + 1, full(q));
+        }
+        if (!ok) break;
       }
-      // loads issued but never consumed (abort only): wait for them to land
-      for (int q = k - 2 < 0 ? 0 : k - 2; q < k; q++) mbar_drain(full(q & 1), (q >> 1) & 1);
+      // loads issued but maybe never consumed (abort only): wait for them to land
+      for (int h = g - TC_RING < 0 ? 0 : g - TC_RING; h < g; h++) mbar_drain(full(h % TC_RING), (h / TC_RING) & 1);
     }
   } else if (warp == TC_EPI_WARPS) {
     // ---------------- MMA issuer
     if (lane == 0) {
       const unsigned long long adesc0 = umma_desc(smem_u32(As), TC_SLAB, 128);
       const unsigned long long bdesc0 = umma_desc(smem_u32(Bs), NS * 16, 128);
-      int k = 0;
-      for (; k < my_tiles; k++) {
+      int g = 0, k = 0;
+      bool ok = true;
+      for (; k < my_tiles && ok; k++) {
         const int s = k & 1;
-        if (!mbar_wait(full(s), (k >> 1) & 1, abort_flag)) break;
-        if (!mbar_wait(tempty(s), ((k >> 1) & 1) ^ 1, abort_flag)) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const unsigned long long adesc = adesc0 + (unsigned long long)(s * (A_BYTES >> 4));
+        if (!(ok = mbar_wait(tempty(s), ((k >> 1) & 1) ^ 1, abort_flag))) break;
         const unsigned dbase = tmem + (unsigned)(s * 256);
-        // descriptor offsets are in 16-byte units on the 14-bit start-address
-        // field; all of shared memory fits in it, so the sums never carry out
+#pragma unroll 1
+        for (int kc = 0; kc < KS; kc++, g++) {
+          const int q = g % TC_RING;
+          if (!(ok = mbar_wait(full(q), (g / TC_RING) & 1, abort_flag))) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          // descriptor offsets are in 16-byte units on the 14-bit start-address
+          // field; all of shared memory fits in it, so the sums never carry out
+          const unsigned long long adesc = adesc0 + (unsigned long long)(q * (TC_SUB >> 4));
+          const unsigned long long bdesc = bdesc0 + (unsigned long long)(2 * kc * NS);
 #pragma unroll
-        for (int j = 0; j < TC_PR; j++) {
-          const int ky_lo = j - (TC_TR - 1) > 0 ? j - (TC_TR - 1) : 0;
-          const int ky_hi = j < 2 ? j : 2;
-          const int nky = ky_hi - ky_lo + 1;
-          const unsigned dcol = dbase + (unsigned)((TC_TR - 1 - j + ky_lo) * NK);  // accumulator of row j - ky_lo
+          for (int j = 0; j < TC_PR; j++) {
+            const int ky_lo = j - (TC_TR - 1) > 0 ? j - (TC_TR - 1) : 0;
+            const int ky_hi = j < 2 ? j : 2;
+            const int nky = ky_hi - ky_lo + 1;
+            const unsigned dcol = dbase + (unsigned)((TC_TR - 1 - j + ky_lo) * NK);  // accumulator of row j - ky_lo
 #pragma unroll
-          for (int kx = 0; kx < 3; kx++) {
-#pragma unroll
-            for (int kc = 0; kc < CIN / 16; kc++) {
-              const unsigned aoff = (unsigned)((2 * kc) * (TC_SLAB / 16) + j * TC_PW + kx);
-              const unsigned boff = (unsigned)((kx * CB + 2 * kc) * NS + ky_lo * NK);
-              if (kx == 0 && kc == 0 && ky_lo == 0) {
-                // first contribution to output row j: start its accumulator
-                mma_bf16<0>(dcol, adesc + aoff, bdesc0 + boff, umma_idesc(TC_M, NK));
-                if (nky == 2) mma_bf16<1>(dcol + NK, adesc + aoff, bdesc0 + boff + NK, umma_idesc(TC_M, NK));
-                if (nky == 3) mma_bf16<1>(dcol + NK, adesc + aoff, bdesc0 + boff + NK, umma_idesc(TC_M, 2 * NK));
+            for (int kx = 0; kx < 3; kx++) {
+              // staged pixel 0 is x0 - 4: output pixel x0 + m reads x0 + m + kx - 1
+              const unsigned aoff = (unsigned)(j * TC_PW + TC_PG - 1 + kx);
+              const unsigned long long b = bdesc + (unsigned)(kx * CB * NS + ky_lo * NK);
+              const unsigned long long a = adesc + aoff;
+              if (kx == 0 && ky_lo == 0) {
+                if (kc == 0) {  // first contribution to output row j: start its accumulator
+                  mma_bf16<0>(dcol, a, b, umma_idesc(TC_M, NK));
+                } else {
+                  mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, NK));
+                }
+                if (nky == 2) mma_bf16<1>(dcol + NK, a, b + NK, umma_idesc(TC_M, NK));
+                if (nky == 3) mma_bf16<1>(dcol + NK, a, b + NK, umma_idesc(TC_M, 2 * NK));
               } else if (nky == 1) {
-                mma_bf16<1>(dcol, adesc + aoff, bdesc0 + boff, umma_idesc(TC_M, NK));
+                mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, NK));
               } else if (nky == 2) {
-                mma_bf16<1>(dcol, adesc + aoff, bdesc0 + boff, umma_idesc(TC_M, 2 * NK));
+                mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, 2 * NK));
               } else {
-                mma_bf16<1>(dcol, adesc + aoff, bdesc0 + boff, umma_idesc(TC_M, 3 * NK));
+                mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, 3 * NK));
               }
             }
           }
+          mma_commit(empty(q));  // ring slot q free once these MMAs have read it
         }
-        mma_commit(empty(s));  // smem stage s free once these MMAs have read it
-        mma_commit(tfull(s));  // accumulator set s complete
+        if (ok) mma_commit(tfull(s));  // accumulator set s complete
       }
-      if (k > 0) mbar_drain(tfull((k - 1) & 1), ((k - 1) >> 1) & 1);  // MMAs in flight (abort only)
+      if (g > 0) {  // MMAs in flight (abort only): the last commit covers all of them
+        const unsigned long long t0 = globaltimer_ns();
+        const int h = g - 1;
+        while (!mbar_test(empty(h % TC_RING), (h / TC_RING) & 1) && globaltimer_ns() - t0 < TC_WAIT_NS) {
+        }
+      }
     }
   } else {
-    // ---------------- epilogue: warp w owns TMEM lanes 32w..32w+31 (pixels)
+    // ---------------- epilogue: warp w owns TMEM lanes 32 (w % 4)..+31 (pixels), rows 2 (w / 4)..+1
+    constexpr int RPW = TC_TR / (TC_EPI_WARPS / 4);  // output rows per epilogue warp
+    const int quarter = warp & 3, r0 = (warp >> 2) * RPW;
+    const size_t plane = (size_t)H * Wp;
     for (int k = 0; k < my_tiles; k++) {
       const int s = k & 1;
       bool ok = true;
@@ -291,34 +333,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       int x0, y0;
       tile_xy(k, x0, y0);
-      const unsigned tbase = tmem + (unsigned)(s * 256) + ((unsigned)(warp * 32) << 16);
-      const int px = x0 + warp * 32 + lane;
-#pragma unroll 1
-      for (int r = 0; r < TC_TR; r++) {
+      const unsigned tbase = tmem + (unsigned)(s * 256) + ((unsigned)(quarter * 32) << 16);
+      const int px = x0 + quarter * 32 + lane;
+#pragma unroll
+      for (int r = r0; r < r0 + RPW; r++) {
         unsigned u[NK];
         const unsigned col = tbase + (unsigned)((TC_TR - 1 - r) * NK);
 #pragma unroll
         for (int c = 0; c < NK / 16; c++) tmem_ld16_async(col + c * 16, u + c * 16);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (r == TC_TR - 1) {  // every read of set s done: hand it back to the MMA warp
+        if (r == r0 + RPW - 1) {  // this warp's reads of set s done: hand it back to the MMA warp
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
           __syncwarp();
           if (lane == 0) mbar_arrive(tempty(s));
         }
         const int gy = y0 + r;
-        if (gy >= H || px >= W) continue;
-        const size_t pix = (size_t)gy * W + px;
+        if (gy >= H || px >= Wp) continue;
         if (EPI == TC_RELU) {
+          const size_t pix = (size_t)gy * Wp + px;
+          const bool in = px < W;  // padding columns are written as zero
 #pragma unroll
           for (int c = 0; c < COUT_G; c += 8) {
             __align__(16) __nv_bfloat162 o[4];
 #pragma unroll
             for (int q = 0; q < 4; q++)
-              o[q] = __floats2bfloat162_rn(fmaxf(__uint_as_float(u[c + 2 * q]) + bias_s[c + 2 * q], 0.f),
-                                           fmaxf(__uint_as_float(u[c + 2 * q + 1]) + bias_s[c + 2 * q + 1], 0.f));
-            *reinterpret_cast<uint4*>(y + pix * COUT_G + c) = *reinterpret_cast<uint4*>(o);
+              o[q] = __floats2bfloat162_rn(
+                  in ? fmaxf(__uint_as_float(u[c + 2 * q]) + bias_s[c + 2 * q], 0.f) : 0.f,
+                  in ? fmaxf(__uint_as_float(u[c + 2 * q + 1]) + bias_s[c + 2 * q + 1], 0.f) : 0.f);
+            *reinterpret_cast<uint4*>(y + ((size_t)(c / 8) * plane + pix) * 8) = *reinterpret_cast<uint4*>(o);
           }
-        } else {
+        } else if (px < W) {
+          const size_t pix = (size_t)gy * W + px;
 #pragma unroll
           for (int c = 0; c < 3; c++) yf[pix * 3 + c] = resid[pix * 3 + c] + (__uint_as_float(u[c]) + bias_s[c]);
         }
@@ -347,18 +392,20 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 template <int CIN, int COUT_G, int NK, int EPI>
 cudaError_t launch_tc(cudaStream_t st, const bf16* x, int H, int W, const bf16* wt, const float* bias, bf16* y,
                       const float* resid, float* yf, int* err) {
-  constexpr size_t need = (size_t)2 * (CIN / 8) * TC_SLAB + (size_t)3 * (CIN / 8) * 3 * NK * 16 + NK * 4 + 8 * 8 + 16;
+  constexpr size_t need = (size_t)TC_RING * TC_SUB + (size_t)3 * (CIN / 8) * 3 * NK * 16 + NK * 4 +
+                         (2 * TC_RING + 4) * 8 + 16;
   constexpr size_t smem = need > TC_MIN_SMEM ? need : TC_MIN_SMEM;
   static_assert(need <= 227 * 1024, "shared memory");
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc) return cudaErrorNotSupported;
   if ((reinterpret_cast<uintptr_t>(x) & 15) != 0) return cudaErrorInvalidValue;
   CUtensorMap map;
-  const cuuint64_t dims[3] = {(cuuint64_t)CIN, (cuuint64_t)W, (cuuint64_t)H};
-  const cuuint64_t strides[2] = {(cuuint64_t)CIN * 2, (cuuint64_t)W * CIN * 2};
-  const cuuint32_t box[3] = {8, (cuuint32_t)TC_PW, (cuuint32_t)TC_PR};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(x), dims, strides, box, estr,
+  const int Wp = (W + TC_PG - 1) / TC_PG * TC_PG;
+  const cuuint64_t dims[4] = {8 * TC_PG, (cuuint64_t)(Wp / TC_PG), (cuuint64_t)H, (cuuint64_t)(CIN / 8)};
+  const cuuint64_t strides[3] = {16 * TC_PG, (cuuint64_t)Wp * 16, (cuuint64_t)Wp * H * 16};
+  const cuuint32_t box[4] = {8 * TC_PG, (cuuint32_t)(TC_PW / TC_PG), (cuuint32_t)TC_PR, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), dims, strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
@@ -377,7 +424,7 @@ cudaError_t launch_tc(cudaStream_t st, const bf16* x, int H, int W, const bf16* 
 }  // namespace
 
 // One image through the 8 layers on the tensor cores. x16: packed input
-// (16 ch); a, b: ping-pong activations (48 ch); wf/bias: per-layer forward
+// (16 ch, [2][H][Wp][8]); a, b: ping-pong activations (48 ch, [6][H][Wp][8]); wf/bias: per-layer forward
 // weights (layer 8's with 8 output channels); rgb/out: fp32 RGB.
 cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
                               const void* const* wf, const float* const* bias, const float* rgb, float* out,
