@@ -38,7 +38,7 @@ EXPORTS = [
     "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_estimate_noise", "dsgpu_guided_filter",
     "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_cnn_param_count", "dsgpu_cnn_create", "dsgpu_cnn_destroy",
     "dsgpu_cnn_state", "dsgpu_cnn_gradients", "dsgpu_cnn_train_step", "dsgpu_cnn_infer", "dsgpu_cnn_denoise",
-    "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
+    "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
     "dsgpu_measure_mma_sync",
     "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render",
 ]
@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_develop_u16_cnn.argtypes = [vp, vp, vp, i, i, sz, vp, f, vp, vp, f, i, i, f, vp, vp, u]
             L.dsgpu_measure_mma_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
             L.dsgpu_cnn_set_engine.argtypes = [vp, vp, i]
+            L.dsgpu_cnn_set_clip.argtypes = [vp, vp, f]
             L.dsgpu_profile.argtypes = [vp, i]
             L.dsgpu_stage_ms.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i)]
             L.dsgpu_launch_count.argtypes = [vp]

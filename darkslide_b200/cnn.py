@@ -88,6 +88,20 @@ class ResidualCNN:
     def step(self) -> int:
         return self._state(0, None, False)
 
+    def snapshot(self):
+        """(params, m, v, step) on the host: the full training state."""
+        m = np.empty(param_count(), np.float32)
+        v = np.empty(param_count(), np.float32)
+        self._state(1, m, False)
+        self._state(2, v, False)
+        return self.get_params(), m, v, self.step
+
+    def restore(self, snap) -> None:
+        p, m, v, step = snap
+        self.set_params(p)
+        self._state(1, np.ascontiguousarray(m), True)
+        self._state(2, np.ascontiguousarray(v), True, step)
+
     def save(self, path: str) -> None:
         m = np.empty(param_count(), np.float32)
         v = np.empty(param_count(), np.float32)
@@ -165,6 +179,10 @@ class ResidualCNN:
                                             int(patch), float(tau), po, ctypes.byref(nf), c.flags),
                     "dsgpu_cnn_denoise")
         return Image3(img.w, img.h, out), int(nf.value)
+
+    def set_clip(self, max_norm: float) -> None:
+        """Clip the global gradient norm to max_norm in train_step (0: off)."""
+        self.ctx.check(lib().dsgpu_cnn_set_clip(self.ctx.handle, self.handle, float(max_norm)), "dsgpu_cnn_set_clip")
 
     def set_engine(self, tensor_core_gen5: bool) -> None:
         """Inference on tcgen05 (default) or on the mma.sync kernels."""

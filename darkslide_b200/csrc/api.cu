@@ -28,6 +28,7 @@ long long* ds_cnn_step_ptr(DsCnn* net);
 cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, const float* strength_map,
                              float strength, const float* tgt, int B, float* loss_sum_host);
 cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr);
+void ds_cnn_set_clip(DsCnn* net, float clip);
 cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out);
 void ds_cnn_set_engine(DsCnn* net, int use_tc);
 int ds_cnn_take_status(DsCnn* net, cudaStream_t st);
@@ -713,6 +714,12 @@ int dsgpu_cnn_train_step(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* rgb, const f
   DS_TRY(ds_cnn_gradients(c->net, ctx->stream, rgb, strength_map, strength, target, batch, loss_sum ? &loss : nullptr));
   DS_TRY(ds_cnn_adam(c->net, ctx->stream, lr));
   if (loss_sum) *loss_sum = loss;
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_set_clip(dsgpu_ctx* ctx, dsgpu_cnn* c, float max_norm) {
+  if (!ctx || !c || !(max_norm >= 0.f)) return DSGPU_ERR_ARG;
+  ds_cnn_set_clip(c->net, max_norm);
   return DSGPU_OK;
 }
 

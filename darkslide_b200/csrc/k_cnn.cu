@@ -353,12 +353,32 @@ __global__ void mse_kernel(const float* __restrict__ out, const float* __restric
   if (threadIdx.x == 0) part[blockIdx.x] = s[0];
 }
 
+// Sum of squares of the n gradients into *out (one CTA, fixed order: deterministic).
+__global__ void grad_sqsum_kernel(const float* __restrict__ gr, int n, float* __restrict__ out) {
+  __shared__ float s[1024];
+  float acc = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += gr[i] * gr[i];
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0];
+}
+
+// Adam; with clip > 0 the gradient is first scaled by min(1, clip / |g|)
+// (global L2 norm from grad_sqsum_kernel).
 __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ gr, float* __restrict__ m,
                             float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1,
-                            float c2) {
+                            float c2, const float* __restrict__ gsq, float clip) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float gi = gr[i];
+  float gi = gr[i];
+  if (clip > 0.f) {
+    const float norm = sqrtf(*gsq);
+    if (norm > clip) gi *= clip / norm;
+  }
   const float mi = b1 * m[i] + (1.f - b1) * gi;
   const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
   m[i] = mi;
@@ -487,6 +507,8 @@ struct DsCnn {
   float* bias[NL] = {};
   long long step = 0;
   bool packed = false;   // wf/wd/bias match params (cleared whenever params may change)
+  float clip = 0.f;      // global gradient-norm clip of the Adam step (0: off)
+  float* gsq = nullptr;  // device: sum of squared gradients
   // training buffers (max_batch crops of crop x crop)
   bf16* act[NL] = {};   // act[0] = packed input (16 ch), act[l] = output of layer l (48 ch), l = 1..7
   bf16* gA = nullptr;   // gradient ping
@@ -564,6 +586,7 @@ cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out) {
     if (e == cudaSuccess) net->lpart = (float*)net->alloc((size_t)1024 * sizeof(float), e);
   }
   if (e == cudaSuccess) net->err = (int*)net->alloc(sizeof(int), e);
+  if (e == cudaSuccess) net->gsq = (float*)net->alloc(sizeof(float), e);
   if (e == cudaSuccess) e = cudaMemset(net->err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(net->m, 0, pb);
   if (e == cudaSuccess) e = cudaMemset(net->v, 0, pb);
@@ -681,8 +704,9 @@ cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr) {
   net->step++;
   net->packed = false;
   const float c1 = 1.0f - (float)pow(b1, (double)net->step), c2 = 1.0f - (float)pow(b2, (double)net->step);
+  if (net->clip > 0.f) grad_sqsum_kernel<<<1, 1024, 0, st>>>(net->grads, net->n_params, net->gsq);
   adam_kernel<<<(net->n_params + 255) / 256, 256, 0, st>>>(net->params, net->grads, net->m, net->v, net->n_params, lr,
-                                                           b1, b2, eps, c1, c2);
+                                                           b1, b2, eps, c1, c2, net->gsq, net->clip);
   return cudaGetLastError();
 }
 
@@ -719,6 +743,8 @@ cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, i
 }
 
 void ds_cnn_set_engine(DsCnn* net, int use_tc) { net->use_tc = use_tc != 0; }
+
+void ds_cnn_set_clip(DsCnn* net, float clip) { net->clip = clip > 0.f ? clip : 0.f; }
 
 // DSGPU_OK, or the status the tensor-core kernels left (the word is reset).
 int ds_cnn_take_status(DsCnn* net, cudaStream_t st) {

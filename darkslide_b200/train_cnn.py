@@ -4,11 +4,21 @@ Data: seeded synthetic Bayer frames (darkslide_b200.Scene) with read noise
 uniform in 2..12 DN, gain 0.25..1 e/DN, random CFA layout and 12/14-bit
 levels, demosaiced on the GPU (RCD); the target is plain GPU NLM of the same
 image (7x7 patch, 21x21 search, h = 1.5 x the noise sigma at mid grey).
-Random crop x crop windows of (RCD output, NLM output, strength map) form the
-batches. Everything runs on the GPU through the library; torch only moves
-tensors.
+The data set is a fixed set of `dataset` crop x crop windows of (RCD output,
+NLM output, strength map): crops_per_frame windows of each of
+dataset / crops_per_frame frames, frame f drawn from seed `seed * 100003 + 1 +
+f` (its scene and its window positions), so the same crops come back in every
+epoch. Training runs `crops` crop visits (crops / dataset epochs); every epoch
+visits the frames in a new order, `mix` frames at a time, and every batch
+mixes crops of those frames (so of several noise levels). The learning rate
+warms up linearly and then follows a cosine, and the global gradient norm is
+clipped at `clip_factor` x the median norm of the first batches. A logged
+loss above 5x its running mean (a divergence, after which ReLU units die
+and the residual collapses to zero) rolls the whole state (weights and Adam
+moments) back to the last healthy snapshot and halves the learning rate. Everything
+runs on the GPU through the library; torch only moves tensors.
 
-    python -m darkslide_b200.train_cnn --crops 200000 --out darkslide_b200/weights/cnn_nlm.bin
+    python -m darkslide_b200.train_cnn --dataset 200000 --crops 2000000 --out darkslide_b200/weights/cnn_nlm.bin
 """
 from __future__ import annotations
 
@@ -47,8 +57,8 @@ def psnr(a, b, peak=1.0):
     return 10.0 * math.log10(peak * peak / max(mse, 1e-20))
 
 
-def train(crops=200000, batch=32, crop=128, lr=1e-3, frame=1024, crops_per_frame=256, seed=0, out=None,
-          resume=None, log_every=200, verbose=True):
+def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=64, mix=8, warmup=500,
+          clip_factor=3.0, seed=0, out=None, resume=None, log_every=200, verbose=True, dataset=200000):
     import torch
 
     dev = torch.device("cuda", 0)
@@ -59,43 +69,79 @@ def train(crops=200000, batch=32, crop=128, lr=1e-3, frame=1024, crops_per_frame
     if resume:
         net.load(resume)
     steps = max(1, crops // batch)
+    n_frames = max(mix, dataset // crops_per_frame)
     rng = np.random.default_rng(seed + 12345)
     pool = []
     t0 = time.time()
     losses = []
+    queue = []  # frames still to visit in this epoch
+
+    def refill():
+        if len(queue) < mix:
+            queue.extend(int(f) for f in rng.permutation(n_frames))
+        for _ in range(mix):
+            fseed = seed * 100003 + 1 + queue.pop()
+            rgb, tgt, hp, _ = make_frame(fseed, frame, frame, dev, ctx)
+            pos = np.random.default_rng(fseed ^ 0x5EED).integers(0, frame - crop + 1, (crops_per_frame, 2))
+            pool.extend((rgb, tgt, hp, int(y), int(x)) for y, x in pos)
+        order = rng.permutation(len(pool))
+        pool[:] = [pool[i] for i in order]
+
+    def next_batch():
+        if len(pool) < batch:
+            pool.clear()
+            refill()
+        take = [pool.pop() for _ in range(batch)]
+        xb = torch.stack([r[y:y + crop, x:x + crop] for (r, _, _, y, x) in take]).contiguous()
+        tb = torch.stack([t[y:y + crop, x:x + crop] for (_, t, _, y, x) in take]).contiguous()
+        smap = torch.stack([torch.full((crop, crop), hp * cnn.STRENGTH_SCALE, device=dev)
+                            for (_, _, hp, _, _) in take]).contiguous()
+        return xb, tb, smap
+
     with torch.cuda.stream(stream):
-        frame_seed = seed * 100003 + 1
-        for step in range(net.step, steps):
-            if not pool:  # a new frame: crops_per_frame random windows
-                rgb, tgt, hp, _ = make_frame(frame_seed, frame, frame, dev, ctx)
-                frame_seed += 1
-                ys = rng.integers(0, frame - crop + 1, crops_per_frame)
-                xs = rng.integers(0, frame - crop + 1, crops_per_frame)
-                pool = [(rgb, tgt, hp, int(y), int(x)) for y, x in zip(ys, xs)]
-            take = [pool.pop() for _ in range(min(batch, len(pool)))]
-            while len(take) < batch:
-                take.append(take[len(take) % max(len(take), 1)])
-            xb = torch.stack([r[y:y + crop, x:x + crop] for (r, _, _, y, x) in take]).contiguous()
-            tb = torch.stack([t[y:y + crop, x:x + crop] for (_, t, _, y, x) in take]).contiguous()
-            smap = torch.stack([torch.full((crop, crop), hp * cnn.STRENGTH_SCALE, device=dev)
-                                for (_, _, hp, _, _) in take]).contiguous()
-            cur = lr * 0.5 * (1 + math.cos(math.pi * step / steps))  # cosine decay
+        if clip_factor > 0:  # clip at a multiple of the typical gradient norm at the start
+            norms = []
+            for _ in range(8):
+                xb, tb, smap = next_batch()
+                g, _ = net.gradients(xb, 0.0, tb, strength_map=smap)
+                norms.append(float(torch.linalg.vector_norm(g)))
+            net.set_clip(clip_factor * float(np.median(norms)))
+        scale, ema, snap, rollbacks = 1.0, None, None, 0
+        step = net.step
+        while step < steps:
+            xb, tb, smap = next_batch()
+            cur = scale * lr * 0.5 * (1 + math.cos(math.pi * step / steps))  # cosine decay
+            if step < warmup:
+                cur *= (step + 1) / warmup
             want = (step % log_every == 0) or step == steps - 1
             loss = net.train_step(xb, 0.0, tb, cur, strength_map=smap, want_loss=want)
+            step += 1
             if want:
                 mse = loss / (batch * crop * crop * 3)
-                losses.append((step, mse))
+                if ema is not None and mse > 5.0 * ema and snap is not None:
+                    net.restore(snap)
+                    step = net.step
+                    scale *= 0.5
+                    rollbacks += 1
+                    if verbose:
+                        print(f"loss spike {mse:.3e} (mean {ema:.3e}): back to step {step}, lr x{scale}", flush=True)
+                    continue
+                ema = mse if ema is None else 0.9 * ema + 0.1 * mse
+                losses.append((step - 1, mse))
+                if (step - 1) % (5 * log_every) == 0:
+                    snap = net.snapshot()
                 if verbose:
-                    print(f"step {step}/{steps} lr {cur:.2e} mse {mse:.3e} ({time.time() - t0:.1f} s)", flush=True)
+                    print(f"step {step - 1}/{steps} lr {cur:.2e} mse {mse:.3e} ({time.time() - t0:.1f} s)", flush=True)
     stream.synchronize()
     if out:
         net.save(out)
     return net, losses, time.time() - t0
 
 
-def evaluate(net, n_frames=4, w=1024, h=1024, seed=999, verbose=True):
+def evaluate(net, n_frames=4, w=1024, h=1024, seed=10_000_999, verbose=True):
     """PSNR (dB) against the noise-free scene of the noisy RCD output, plain
-    NLM and the CNN, and PSNR of the CNN against NLM, averaged over frames."""
+    NLM and the CNN, and PSNR of the CNN against NLM, averaged over frames.
+    The frame seeds lie far outside the training set's."""
     import torch
 
     dev = torch.device("cuda", 0)
@@ -118,17 +164,23 @@ def evaluate(net, n_frames=4, w=1024, h=1024, seed=999, verbose=True):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--crops", type=int, default=200000)
+    ap.add_argument("--crops", type=int, default=2000000, help="crop visits (epochs = crops / dataset)")
+    ap.add_argument("--dataset", type=int, default=200000, help="distinct crops in the training set")
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--crop", type=int, default=128)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=5e-4)
+    ap.add_argument("--frame", type=int, default=512)
+    ap.add_argument("--mix", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=500)
+    ap.add_argument("--clip", type=float, default=3.0, help="clip factor x initial median gradient norm (0: off)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     ap.add_argument("--resume", default=None)
     ap.add_argument("--eval", type=int, default=4)
     a = ap.parse_args()
-    net, losses, secs = train(a.crops, a.batch, a.crop, a.lr, seed=a.seed, out=a.out, resume=a.resume)
-    print(f"trained {a.crops} crops in {secs:.1f} s", flush=True)
+    net, losses, secs = train(a.crops, a.batch, a.crop, a.lr, frame=a.frame, mix=a.mix, warmup=a.warmup,
+                              clip_factor=a.clip, seed=a.seed, out=a.out, resume=a.resume, dataset=a.dataset)
+    print(f"trained {a.crops} crop visits of a {a.dataset}-crop set in {secs:.1f} s", flush=True)
     if a.eval:
         evaluate(net, a.eval)
 

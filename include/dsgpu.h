@@ -215,6 +215,9 @@ int dsgpu_cnn_gradients(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* rgb, const 
 /* One Adam step (beta 0.9/0.999, eps 1e-8) on the same loss. Device buffers. */
 int dsgpu_cnn_train_step(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* rgb, const float* strength_map,
                          float strength, const float* target, int batch, float lr, float* loss_sum);
+/* Clip the global L2 norm of the gradient to max_norm before each Adam step
+ * of dsgpu_cnn_train_step (0, the default: no clipping). */
+int dsgpu_cnn_set_clip(dsgpu_ctx* ctx, dsgpu_cnn* net, float max_norm);
 /* out = in + network(in, strength) on a whole interleaved RGB image
  * (strength = DSGPU_CNN_STRENGTH_SCALE * h). */
 #define DSGPU_CNN_STRENGTH_SCALE 50.0f

@@ -103,6 +103,35 @@ def test_adam_step_and_bit_identical_resume(torch_dev, tmp_path):
     np.testing.assert_array_equal(net2.get_params(), direct)
 
 
+def test_adam_gradient_norm_clip(torch_dev):
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    b1, b2 = (_batch(torch, dev, 2, 16, 40 + k)[2:] for k in range(2))
+    net = cnn.ResidualCNN(max_batch=2, crop=16, seed=4)
+    p0 = net.get_params().astype(np.float64)
+    g1, _ = net.gradients(b1[0], 0.5, b1[1])
+    g1 = g1.cpu().numpy().astype(np.float64)
+    clip = 0.5 * np.linalg.norm(g1)
+    net.set_clip(clip)
+    net.train_step(b1[0], 0.5, b1[1], 1e-3)
+    p1 = net.get_params().astype(np.float64)
+    g2, _ = net.gradients(b2[0], 0.5, b2[1])
+    g2 = g2.cpu().numpy().astype(np.float64)
+    net.train_step(b2[0], 0.5, b2[1], 1e-3)
+
+    def clipped(g):
+        n = np.linalg.norm(g)
+        return g * min(1.0, clip / n)
+
+    c1, c2 = clipped(g1), clipped(g2)
+    m1, v1 = 0.1 * c1, 0.001 * c1 * c1
+    m2, v2 = 0.9 * m1 + 0.1 * c2, 0.999 * v1 + 0.001 * c2 * c2
+    exp = p1 - 1e-3 * (m2 / (1 - 0.9 ** 2)) / (np.sqrt(v2 / (1 - 0.999 ** 2)) + 1e-8)
+    assert np.abs(p1 - p0).max() > 0
+    np.testing.assert_allclose(net.get_params(), exp, rtol=1e-4, atol=1e-7)
+
+
 def test_training_reduces_loss(torch_dev):
     from darkslide_b200 import cnn
 
