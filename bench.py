@@ -1,11 +1,18 @@
-"""Benchmark of the RCD demosaic + NLM denoise path on B200.
+"""Benchmark of the RCD demosaic + NLM denoise path on B200: plain and learned.
 
 One step = one 6000x4000 (24 MP) RGGB 14-bit mosaic (black 512, white 16383,
-read noise 6 DN, gain 0.5 e/DN) through u16 -> normalise -> RCD -> NLM
-(7x7 patch, 21x21 search, h = 1.5 x noise sigma at mid grey) on each RGB
-channel, with the raw already resident in HBM. The working set (48 MB raw,
-288 MB demosaiced, 288 MB output) is larger than the 126 MB L2, so no flush is
-needed between steps.
+read noise 6 DN, gain 0.5 e/DN) developed from u16 with the raw already
+resident in HBM, by two paths through the C ABI:
+  plain    u16 -> normalise -> RCD -> NLM (7x7 patch, 21x21 search, h = 1.5 x
+           noise sigma at mid grey) on each RGB channel (dsgpu_develop_u16);
+  learned  u16 -> normalise -> RCD -> residual CNN (8 conv3x3, 48 channels,
+           BF16 tcgen05, weights darkslide_b200/weights/cnn_nlm.bin) -> NLM on
+           the tiles failing the residual check (dsgpu_develop_u16_cnn).
+Both are timed the same way; the learned path is the headline when its PSNR
+against the noise-free scene (central 2048x2048 crop) is within 0.1 dB of
+plain NLM's, else the plain path is. The working set (48 MB raw, 288 MB
+demosaiced, 288 MB output, 2.3 GB of CNN activations) is larger than the
+126 MB L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -36,6 +43,10 @@ GAIN, READ_SIGMA = 0.5, 6.0
 SEARCH, PATCH = 10, 3
 WB = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
 CPU_SAMPLE = (1536, 1024)  # oracle crop (w, h) of the same frame for the CPU baseline
+WEIGHTS = os.path.join(ROOT, "darkslide_b200", "weights", "cnn_nlm.bin")
+TAU = 3.0                  # residual check of the learned path: NLM on tiles removing > TAU x sigma
+QUALITY_CROP = 2048        # central crop for PSNR against the noise-free scene
+QUALITY_BOUND_DB = 0.1     # allowed PSNR loss of the learned path against plain NLM
 
 
 def workload_config(n_gpus: int) -> dict:
@@ -194,7 +205,14 @@ def run_reference(args):
     return 0
 
 
+def psnr(a, b) -> float:
+    mse = float(np.mean((a.astype(np.float64) - b.astype(np.float64)) ** 2))
+    return 10.0 * float(np.log10(1.0 / max(mse, 1e-30)))
+
+
 def run_ours(args):
+    import ctypes
+
     import torch
 
     ws, rank, local = dist_env()
@@ -209,18 +227,18 @@ def run_ours(args):
     dev = torch.device("cuda", torch.cuda.current_device())
 
     import darkslide_b200 as ds
-    from darkslide_b200 import _lib
+    from darkslide_b200 import _lib, cnn
 
     ctx = ds.Context(dev.index)
     stream = torch.cuda.Stream(dev)
-    ctx.set_stream(stream.cuda_stream)
     L = _lib.lib()
-    import ctypes
-
     vp = ctypes.c_void_p
     hp = h_param()
     white = np.full(3, WHITE, np.float32)
     pat = ds.RGGB.codes()
+    net = cnn.ResidualCNN(ctx)
+    net.load(WEIGHTS)
+    ctx.set_stream(stream.cuda_stream)
 
     sc = ds.Scene(seed=1 + rank, w=W, h=H, pattern=ds.RGGB, black=BLACK, white=WHITE, gain=GAIN,
                   read_sigma=READ_SIGMA)
@@ -228,11 +246,18 @@ def run_ours(args):
         raw = sc.render(dev, ctx=ctx)
         out = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
     stream.synchronize()
+    ctx.set_stream(stream.cuda_stream)
 
-    def step(flags=_lib.DSGPU_ASYNC, raw_p=None, out_p=None):
+    def step_plain(flags=_lib.DSGPU_ASYNC, raw_p=None, out_p=None):
         ctx.check(L.dsgpu_develop_u16(ctx.handle, raw_p or vp(raw.data_ptr()), W, H, W, vp(pat.ctypes.data),
                                       float(BLACK), vp(white.ctypes.data), vp(WB.ctypes.data), float(hp), SEARCH,
                                       PATCH, out_p or vp(out.data_ptr()), vp(0), flags), "dsgpu_develop_u16")
+
+    def step_learned(flags=_lib.DSGPU_ASYNC, raw_p=None, out_p=None):
+        ctx.check(L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, raw_p or vp(raw.data_ptr()), W, H, W,
+                                          vp(pat.ctypes.data), float(BLACK), vp(white.ctypes.data),
+                                          vp(WB.ctypes.data), float(hp), SEARCH, PATCH, float(TAU),
+                                          out_p or vp(out.data_ptr()), vp(0), flags), "dsgpu_develop_u16_cnn")
 
     def barrier():
         if ws > 1:
@@ -240,69 +265,103 @@ def run_ours(args):
 
             dist.barrier()
 
-    for _ in range(args.warmup):
-        step()
-    stream.synchronize()
-
-    # ---- device-resident timed region
-    clocks = Clocks(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev.index)).split(",")[dev.index])
-                    if os.environ.get("CUDA_VISIBLE_DEVICES") else dev.index)
-    ctx.profile(True)
-    n0 = ctx.launch_count()
-    barrier()
-    torch.cuda.synchronize(dev)
-    clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize(dev)
-    barrier()
-    clk = clocks.stop()
-    launches = ctx.launch_count() - n0
-    ms = e0.elapsed_time(e1)
-    nlm_ms, nlm_n = ctx.stage_ms(_lib.DSGPU_STAGE_NLM)
-    dem_ms, dem_n = ctx.stage_ms(_lib.DSGPU_STAGE_DEMOSAIC)
-    ctx.profile(False)
-    t_max = ms
-    if ws > 1:
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
         import torch.distributed as dist
 
-        t = torch.tensor([ms], device=dev)
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    ms_step = t_max / args.steps
-    value = ws * W * H * args.steps / (t_max * 1e-3) / 1e6
+        return float(t.item())
 
-    # ---- end to end through the C ABI with pinned host buffers
+    gpu_index = (int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[dev.index])
+                 if os.environ.get("CUDA_VISIBLE_DEVICES") else dev.index)
+
+    def device_timed(step):
+        """K steps with the raw frame resident in HBM: CUDA events on the
+        launching stream, clocks sampled during the region, per-stage marks."""
+        ctx.set_stream(stream.cuda_stream)
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+        clocks = Clocks(gpu_index)
+        ctx.profile(True)
+        n0 = ctx.launch_count()
+        barrier()
+        torch.cuda.synchronize(dev)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize(dev)
+        barrier()
+        clk = clocks.stop()
+        r = {"ms": max_over_ranks(e0.elapsed_time(e1)), "launches": ctx.launch_count() - n0, "clocks": clk}
+        for name, st in (("demosaic", _lib.DSGPU_STAGE_DEMOSAIC), ("nlm", _lib.DSGPU_STAGE_NLM),
+                         ("cnn", _lib.DSGPU_STAGE_CNN), ("cnn_hidden", _lib.DSGPU_STAGE_CNN_HIDDEN)):
+            r[name] = ctx.stage_ms(st)
+        ctx.profile(False)
+        r["ms_per_step"] = r["ms"] / args.steps
+        r["value"] = ws * W * H * args.steps / (r["ms"] * 1e-3) / 1e6
+        return r
+
     raw_h = torch.empty((H, W), dtype=torch.uint16).pin_memory()
     raw_h.copy_(raw.cpu())
     out_h = torch.empty((H, W, 3), dtype=torch.float32).pin_memory()
-    ctx.set_stream(None)
-    ctx.profile(True)
-    for _ in range(2):
-        step(_lib.DSGPU_HOST, vp(raw_h.data_ptr()), vp(out_h.data_ptr()))
-    ctx.profile(True)  # discard warm-up marks
-    barrier()
-    k_e2e = max(2, min(args.steps, 5))
-    t0 = time.perf_counter()
-    for _ in range(k_e2e):
-        step(_lib.DSGPU_HOST, vp(raw_h.data_ptr()), vp(out_h.data_ptr()))
-    t_e2e = time.perf_counter() - t0
-    copy_ms, _ = ctx.stage_ms(_lib.DSGPU_STAGE_COPY)
-    ctx.profile(False)
-    if ws > 1:
-        import torch.distributed as dist
 
-        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e = ws * W * H * k_e2e / t_e2e / 1e6
+    def e2e_timed(step):
+        """The same call with HOST buffers: H2D of the raw frame and D2H of the
+        RGB result inside every step (DSGPU_HOST; the call returns when the
+        result is in host memory)."""
+        ctx.set_stream(None)
+        for _ in range(2):
+            step(_lib.DSGPU_HOST, vp(raw_h.data_ptr()), vp(out_h.data_ptr()))
+        ctx.profile(True)
+        barrier()
+        k = max(2, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(k):
+            step(_lib.DSGPU_HOST, vp(raw_h.data_ptr()), vp(out_h.data_ptr()))
+        t = max_over_ranks(time.perf_counter() - t0)
+        copy_ms, _ = ctx.stage_ms(_lib.DSGPU_STAGE_COPY)
+        ctx.profile(False)
+        ctx.set_stream(stream.cuda_stream)
+        return {"value": ws * W * H * k / t / 1e6, "unit": "Mpix/s", "h2d_bytes_per_step": W * H * 2,
+                "d2h_bytes_per_step": W * H * 12, "copy_ms_per_step": copy_ms / k}
+
+    plain = device_timed(step_plain)
+    learned = device_timed(step_learned)
+    plain_e2e = e2e_timed(step_plain)
+    learned_e2e = e2e_timed(step_learned)
+
+    # ---- quality on a central crop: PSNR against the noise-free scene
+    cw = ch = QUALITY_CROP
+    qx, qy = (W - cw) // 2, (H - ch) // 2
+    truth = sc.truth_host(qx, qy, cw, ch) * WB
+    with torch.cuda.stream(stream):
+        step_plain()
+        q_plain = out[qy:qy + ch, qx:qx + cw].cpu().numpy()
+        step_learned()
+        q_learned = out[qy:qy + ch, qx:qx + cw].cpu().numpy()
+        # the RCD output alone (search 0 copies it), then the learned denoise with its fallback count
+        rgb = torch.empty_like(out)
+        ctx.check(L.dsgpu_develop_u16(ctx.handle, vp(raw.data_ptr()), W, H, W, vp(pat.ctypes.data), float(BLACK),
+                                      vp(white.ctypes.data), vp(WB.ctypes.data), float(hp), 0, PATCH,
+                                      vp(rgb.data_ptr()), vp(0), 0), "dsgpu_develop_u16")
+        q_noisy = rgb[qy:qy + ch, qx:qx + cw].cpu().numpy()
+        nf = ctypes.c_int()
+        ctx.check(L.dsgpu_cnn_denoise(ctx.handle, net.handle, vp(rgb.data_ptr()), W, H, float(hp), SEARCH, PATCH,
+                                      float(TAU), vp(out.data_ptr()), ctypes.byref(nf), 0), "dsgpu_cnn_denoise")
+    stream.synchronize()
+    p_plain, p_learned, p_noisy = psnr(q_plain, truth), psnr(q_learned, truth), psnr(q_noisy, truth)
+    loss_db = p_plain - p_learned
+    meets = loss_db <= QUALITY_BOUND_DB
+    tiles = -(-W // 64) * -(-H // (64 - 2 * PATCH))
 
     if rank == 0:
-        fl, ex2, fl2 = ctx.measure_peaks()
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -310,39 +369,83 @@ def run_ours(args):
             pass
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
-        # NLM: one exp per (pixel, channel, search offset) -- enhance.rs:58
+        tc_peak = peaks.get("bf16_tflops_sustained", 1400.0)
+        tc_src = "measured, sustained" if "bf16_tflops_sustained" in peaks else "fallback, sustained"
+        traffic = read_traffic()
+        fl, ex2, fl2 = ctx.measure_peaks()
+        # plain path: NLM, one exp per (pixel, channel, search offset) -- enhance.rs:58
         updates = W * H * 3 * (2 * SEARCH + 1) ** 2
+        nlm_ms, nlm_n = plain["nlm"]
         nlm_launch_ms = nlm_ms / max(nlm_n, 1)
         achieved_ex2 = updates / (nlm_launch_ms * 1e-3) / 1e9
+        dem_ms, dem_n = plain["demosaic"]
         dem_launch_ms = dem_ms / max(dem_n, 1)
         rcd_bytes = W * H * (2 + 12)  # u16 in, RGB f32 out
-        traffic = read_traffic()
+        roof_nlm = {
+            "kernel": "nlm_tile_kernel<3>", "bound": "sfu", "achieved": achieved_ex2, "peak": ex2 / 1e9,
+            "unit": "Gexp/s", "frac": achieved_ex2 / (ex2 / 1e9),
+            "traffic": traffic.get("nlm_bytes_per_launch"),
+            "algorithmic": f"{updates:.4g} exp per launch (W*H*3*(2S+1)^2, one exp per pixel, channel and offset)",
+            "peak_source": "ex2.approx throughput microbenchmark on this GPU (dsgpu_measure_peaks)",
+            "launch_ms": nlm_launch_ms, "fp32_peak_tflops": fl / 1e12, "fp32x2_peak_tflops": fl2 / 1e12,
+        }
+        roof_rcd = {
+            "kernel": "rcd_tile_kernel<SrcU16>", "bound": "hbm", "achieved": rcd_bytes / (dem_launch_ms * 1e-3) / 1e9,
+            "peak": hbm_peak, "unit": "GB/s", "frac": rcd_bytes / (dem_launch_ms * 1e-3) / 1e9 / hbm_peak,
+            "traffic": traffic.get("rcd_bytes_per_launch"),
+            "algorithmic": "14 B/px (u16 in, 3xf32 out)", "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)",
+            "launch_ms": dem_launch_ms,
+        }
+        # learned path: the hidden conv layer (48 -> 48, 3x3) on the tensor cores
+        hid_ms, hid_n = learned["cnn_hidden"]
+        conv_ms = hid_ms / max(6 * hid_n, 1)
+        conv_flops = 2.0 * W * H * 9 * 48 * 48
+        conv_bytes = W * H * 96 * 2  # bf16 48-channel activations in and out
+        roof_conv = {
+            "kernel": "conv_tc_kernel<48,48,48,0>", "bound": "tensor",
+            "achieved": conv_flops / (conv_ms * 1e-3) / 1e12, "peak": tc_peak, "unit": "TFLOP/s",
+            "frac": conv_flops / (conv_ms * 1e-3) / 1e12 / tc_peak,
+            "traffic": traffic.get("conv48_bytes_per_launch"),
+            "algorithmic": f"{conv_flops:.4g} FLOP per launch (2*W*H*9*48*48); {conv_bytes:.4g} B of activations "
+                           f"in+out ({conv_bytes / (conv_ms * 1e-3) / 1e9:.0f} GB/s, "
+                           f"{conv_bytes / (conv_ms * 1e-3) / 1e9 / hbm_peak:.3f} of measured HBM)",
+            "peak_source": f"{tc_src} cuBLAS bf16 (MEASURED_PEAKS.json)", "launch_ms": conv_ms,
+        }
+        learned_info = {
+            "value": learned["value"], "ms_per_step": learned["ms_per_step"], "e2e": learned_e2e,
+            "speedup_vs_plain": learned["value"] / plain["value"],
+            "e2e_speedup_vs_plain": learned_e2e["value"] / plain_e2e["value"],
+            "stage_ms_per_step": {"demosaic": learned["demosaic"][0] / args.steps,
+                                  "cnn_with_fallback": learned["cnn"][0] / args.steps},
+            "gpu_launches": learned["launches"], "fallback_tiles": nf.value, "tiles": tiles, "tau": TAU,
+            "psnr_db_vs_truth": {"noisy_rcd": p_noisy, "plain_nlm": p_plain, "learned": p_learned},
+            "psnr_loss_db": loss_db, "quality_bound_db": QUALITY_BOUND_DB, "meets_quality_bound": meets,
+            "quality_sample": f"central {cw}x{ch} crop of the frame, PSNR against the noise-free scene (x WB); "
+                              "plain GPU NLM stands for the FP64 oracle (they agree within 2e-4 max-abs)",
+            "roofline": roof_conv, "weights": "darkslide_b200/weights/cnn_nlm.bin", "dtype": "bf16 (fp32 accumulate)",
+            "clocks": learned["clocks"],
+        }
+        plain_info = {
+            "value": plain["value"], "ms_per_step": plain["ms_per_step"], "e2e": plain_e2e,
+            "gpu_launches": plain["launches"], "roofline": roof_nlm, "roofline_hbm": roof_rcd, "dtype": "f32",
+            "clocks": plain["clocks"],
+        }
+        head, head_info = (learned, learned_info) if meets else (plain, plain_info)
         line = {
-            "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded gradient+edge scene, Poisson-Gaussian noise)",
+            "metric": METRIC, "value": head["value"], "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": head_info["dtype"].split()[0],
+            "data": "synthetic (seeded gradient+edge scene, Poisson-Gaussian noise)",
             "config": workload_config(ws),
-            "path": "plain GPU RCD+NLM (the learned path is not built yet)",
-            "roofline": {
-                "kernel": "nlm_tile_kernel<3>", "bound": "sfu", "achieved": achieved_ex2, "peak": ex2 / 1e9,
-                "unit": "Gexp/s", "frac": achieved_ex2 / (ex2 / 1e9),
-                "traffic": (traffic or {}).get("nlm_bytes_per_launch"),
-                "algorithmic": f"{updates:.4g} exp per launch (W*H*3*(2S+1)^2, one exp per pixel, channel and offset)",
-                "peak_source": "ex2.approx throughput microbenchmark on this GPU (dsgpu_measure_peaks)",
-                "launch_ms": nlm_launch_ms, "fp32_peak_tflops": fl / 1e12, "fp32x2_peak_tflops": fl2 / 1e12,
-            },
-            "roofline_hbm": {
-                "kernel": "rcd_tile_kernel<SrcU16>", "bound": "hbm", "achieved": rcd_bytes / (dem_launch_ms * 1e-3) / 1e9,
-                "peak": hbm_peak, "unit": "GB/s", "frac": rcd_bytes / (dem_launch_ms * 1e-3) / 1e9 / hbm_peak,
-                "traffic": (traffic or {}).get("rcd_bytes_per_launch"),
-                "algorithmic": "14 B/px (u16 in, 3xf32 out)", "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)",
-                "launch_ms": dem_launch_ms,
-            },
-            "e2e": {"value": e2e, "unit": "Mpix/s", "h2d_bytes_per_step": W * H * 2,
-                    "d2h_bytes_per_step": W * H * 12, "copy_ms_per_step": copy_ms / k_e2e,
-                    "api": "dsgpu_develop_u16 with DSGPU_HOST, pinned host buffers"},
-            "gpu_launches": launches,
-            "clocks": clk,
+            "path": ("learned: RCD + residual CNN on tcgen05 + NLM on tiles failing the residual check" if meets else
+                     "plain: RCD + NLM (the learned path missed the quality bound on this frame)"),
+            "roofline": head_info["roofline"],
+            "roofline_hbm": roof_rcd,
+            "e2e": head_info["e2e"],
+            "gpu_launches": head["launches"],
+            "clocks": head["clocks"],
+            "learned": learned_info,
+            "plain": plain_info,
         }
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}

@@ -29,6 +29,7 @@ DSGPU_STAGE_DEMOSAIC = 0
 DSGPU_STAGE_NLM = 1
 DSGPU_STAGE_COPY = 2
 DSGPU_STAGE_CNN = 3
+DSGPU_STAGE_CNN_HIDDEN = 4
 
 # every symbol include/dsgpu.h and include/dsgpu_scene.h declare
 EXPORTS = [

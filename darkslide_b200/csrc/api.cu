@@ -29,6 +29,7 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
                              float strength, const float* tgt, int B, float* loss_sum_host);
 cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr);
 void ds_cnn_set_clip(DsCnn* net, float clip);
+void ds_cnn_set_marks(DsCnn* net, cudaEvent_t a, cudaEvent_t b);
 cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out);
 void ds_cnn_set_engine(DsCnn* net, int use_tc);
 int ds_cnn_take_status(DsCnn* net, cudaStream_t st);
@@ -143,6 +144,34 @@ struct StageMark {
     }
     cudaEventRecord(b, ctx->stream);
     ctx->marks.push_back({stage, a, b});
+  }
+};
+
+// Profiling mark around the hidden conv layers of one CNN call (events
+// recorded by the network's own driver).
+struct HiddenMark {
+  dsgpu_ctx* ctx;
+  DsCnn* net;
+  cudaEvent_t a = nullptr, b = nullptr;
+  bool done = false;  // set once the call has been queued (both events recorded)
+  HiddenMark(dsgpu_ctx* c, DsCnn* n) : ctx(c), net(n) {
+    if (!ctx->profiling || !(a = take_event(ctx))) return;
+    if (!(b = take_event(ctx))) {
+      ctx->pool.push_back(a);
+      a = nullptr;
+      return;
+    }
+    ds_cnn_set_marks(net, a, b);
+  }
+  ~HiddenMark() {
+    if (!a) return;
+    ds_cnn_set_marks(net, nullptr, nullptr);
+    if (done) {
+      ctx->marks.push_back({DSGPU_STAGE_CNN_HIDDEN, a, b});
+    } else {
+      ctx->pool.push_back(a);
+      ctx->pool.push_back(b);
+    }
   }
 };
 
@@ -737,7 +766,9 @@ int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, in
   DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &dout));
   {
     StageMark mark(ctx, DSGPU_STAGE_CNN);
+    HiddenMark hidden(ctx, c->net);
     DS_TRY(ds_cnn_infer(c->net, ctx->stream, (const float*)din, w, h, strength, (float*)dout));
+    hidden.done = true;
   }
   ctx->launches += 2 + 8 + 8;
   DS_CHECK(finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float)));
@@ -780,8 +811,10 @@ int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, 
   DS_CHECK(fallback_scratch(ctx, w, h, patch, &fl, &cnt));
   {
     StageMark mark(ctx, DSGPU_STAGE_CNN);
+    HiddenMark hidden(ctx, c->net);
     DS_TRY(ds_cnn_denoise(c->net, ctx->stream, (const float*)din, w, h, h_param, search, patch, tau,
                           DSGPU_CNN_STRENGTH_SCALE, (float*)dout, fl, cnt));
+    hidden.done = true;
   }
   ctx->launches += 2 + 8 + 8 + (tau > 0.f ? 2 : 0);
   if (!(flags & DSGPU_ASYNC)) DS_CHECK(ds_cnn_take_status(c->net, ctx->stream));
@@ -826,8 +859,10 @@ int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* c, const uint16_t* raw, int
   }
   {
     StageMark mark(ctx, DSGPU_STAGE_CNN);
+    HiddenMark hidden(ctx, c->net);
     DS_TRY(ds_cnn_denoise(c->net, ctx->stream, (const float*)mid, w, h, h_param, search, patch, tau,
                           DSGPU_CNN_STRENGTH_SCALE, (float*)drgb, fl, cnt));
+    hidden.done = true;
     ctx->launches += 2 + 8 + 8 + (tau > 0.f ? 2 : 0);
   }
   return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));

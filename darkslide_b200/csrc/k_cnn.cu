@@ -492,7 +492,7 @@ constexpr LayerSpec LAYERS[NL] = {{4, 48, 16, 48},  {48, 48, 48, 48}, {48, 48, 4
 
 cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
                               const void* const* wf, const float* const* bias, const float* rgb, float* out,
-                              int* err);
+                              int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end);
 
 struct DsCnn {
   int device = 0;
@@ -508,6 +508,7 @@ struct DsCnn {
   long long step = 0;
   bool packed = false;   // wf/wd/bias match params (cleared whenever params may change)
   float clip = 0.f;      // global gradient-norm clip of the Adam step (0: off)
+  cudaEvent_t mark_a = nullptr, mark_b = nullptr;  // profiling: around the hidden layers of inference
   float* gsq = nullptr;  // device: sum of squared gradients
   // training buffers (max_batch crops of crop x crop)
   bf16* act[NL] = {};   // act[0] = packed input (16 ch), act[l] = output of layer l (48 ch), l = 1..7
@@ -626,15 +627,18 @@ cudaError_t ds_cnn_pack(DsCnn* net, cudaStream_t st) {
 // Forward through all layers. x16: packed input; rgb: fp32 input RGB (the
 // residual); out: fp32 RGB. acts: per-layer outputs (act[l] for l=1..7).
 static cudaError_t forward(DsCnn* net, cudaStream_t st, const bf16* x16, const float* rgb, int B, int H, int W,
-                           bf16* const* acts, float* out) {
+                           bf16* const* acts, float* out, cudaEvent_t hidden_begin = nullptr,
+                           cudaEvent_t hidden_end = nullptr) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
   const int grid = sms * 3;
   cudaError_t e = launch_fwd<16, 48, EPI_RELU>(st, grid, x16, B, H, W, net->wf[0], net->bias[0], acts[1], nullptr,
                                                nullptr, nullptr);
+  if (e == cudaSuccess && hidden_begin) e = cudaEventRecord(hidden_begin, st);
   for (int l = 1; l < NL - 1 && e == cudaSuccess; l++)
     e = launch_fwd<48, 48, EPI_RELU>(st, grid, acts[l], B, H, W, net->wf[l], net->bias[l], acts[l + 1], nullptr,
                                      nullptr, nullptr);
+  if (e == cudaSuccess && hidden_end) e = cudaEventRecord(hidden_end, st);
   if (e == cudaSuccess)
     e = launch_fwd<48, 8, EPI_RESID>(st, grid, acts[NL - 1], B, H, W, net->wf[NL - 1], net->bias[NL - 1], nullptr,
                                      nullptr, rgb, out);
@@ -735,16 +739,22 @@ cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, i
       wf[l] = net->wf[l];
       bs[l] = net->bias[l];
     }
-    return ds_cnn_forward_tc(st, net->ib, net->ia, net->ib, h, w, wf, bs, rgb, out, net->err);
+    return ds_cnn_forward_tc(st, net->ib, net->ia, net->ib, h, w, wf, bs, rgb, out, net->err, net->mark_a,
+                             net->mark_b);
   }
   pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, nullptr, strength, net->ib);
   bf16* acts[NL] = {net->ib, net->ia, net->ib, net->ia, net->ib, net->ia, net->ib, net->ia};
-  return forward(net, st, net->ib, rgb, 1, h, w, acts, out);
+  return forward(net, st, net->ib, rgb, 1, h, w, acts, out, net->mark_a, net->mark_b);
 }
 
 void ds_cnn_set_engine(DsCnn* net, int use_tc) { net->use_tc = use_tc != 0; }
 
 void ds_cnn_set_clip(DsCnn* net, float clip) { net->clip = clip > 0.f ? clip : 0.f; }
+
+void ds_cnn_set_marks(DsCnn* net, cudaEvent_t a, cudaEvent_t b) {
+  net->mark_a = a;
+  net->mark_b = b;
+}
 
 // DSGPU_OK, or the status the tensor-core kernels left (the word is reset).
 int ds_cnn_take_status(DsCnn* net, cudaStream_t st) {

@@ -425,15 +425,17 @@ cudaError_t launch_tc(cudaStream_t st, const bf16* x, int H, int W, const bf16* 
 
 // One image through the 8 layers on the tensor cores. x16: packed input
 // (16 ch, [2][H][Wp][8]); a, b: ping-pong activations (48 ch, [6][H][Wp][8]); wf/bias: per-layer forward
-// weights (layer 8's with 8 output channels); rgb/out: fp32 RGB.
+// weights (layer 8's with 8 output channels); rgb/out: fp32 RGB;
+// hidden_begin/end (may be null): events recorded around layers 2-7.
 cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
                               const void* const* wf, const float* const* bias, const float* rgb, float* out,
-                              int* err) {
+                              int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end) {
   const bf16* in = static_cast<const bf16*>(x16);
   bf16* pa = static_cast<bf16*>(a);
   bf16* pb = static_cast<bf16*>(b);
   cudaError_t e = launch_tc<16, 48, 48, TC_RELU>(st, in, H, W, static_cast<const bf16*>(wf[0]), bias[0], pa, nullptr,
                                                  nullptr, err);
+  if (e == cudaSuccess && hidden_begin) e = cudaEventRecord(hidden_begin, st);
   for (int l = 1; l < 7 && e == cudaSuccess; l++) {
     e = launch_tc<48, 48, 48, TC_RELU>(st, pa, H, W, static_cast<const bf16*>(wf[l]), bias[l], pb, nullptr, nullptr,
                                        err);
@@ -441,6 +443,7 @@ cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b
     pa = pb;
     pb = t;
   }
+  if (e == cudaSuccess && hidden_end) e = cudaEventRecord(hidden_end, st);
   if (e == cudaSuccess)
     e = launch_tc<48, 8, 16, TC_RESID>(st, pa, H, W, static_cast<const bf16*>(wf[7]), bias[7], nullptr, rgb, out,
                                        err);

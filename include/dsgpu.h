@@ -91,6 +91,8 @@ const char* dsgpu_last_error(dsgpu_ctx* ctx);
 #define DSGPU_STAGE_NLM 1
 #define DSGPU_STAGE_COPY 2
 #define DSGPU_STAGE_CNN 3
+/* the six hidden 48 -> 48 conv layers of the learned path, one mark per call */
+#define DSGPU_STAGE_CNN_HIDDEN 4
 int dsgpu_profile(dsgpu_ctx* ctx, int enable);
 int dsgpu_stage_ms(dsgpu_ctx* ctx, int stage, double* total_ms, int* count);
 unsigned long long dsgpu_launch_count(dsgpu_ctx* ctx);
