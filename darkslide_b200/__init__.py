@@ -348,16 +348,23 @@ class Scene:
             raise DsgpuError(st, "dsgpu_scene_truth_host")
         return out
 
-    def render(self, device=None, ctx: Context | None = None):
-        """GPU render of the whole frame into a CUDA uint16 tensor (h, w)."""
+    def render(self, device=None, ctx: Context | None = None, window=None):
+        """GPU render into a CUDA uint16 tensor: the whole frame (h, w), or
+        window = (x0, y0, cw, ch), that crop of it (ch, cw)."""
         import torch
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-        t = torch.empty((self.h, self.w), dtype=torch.uint16, device=dev)
         cx = ctx or default_context(dev.index or 0)
         cx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
         d = self.desc()
-        cx.check(lib().dsgpu_scene_render(cx.handle, ctypes.byref(d), ctypes.c_void_p(t.data_ptr()), 0),
-                 "dsgpu_scene_render")
+        if window is None:
+            t = torch.empty((self.h, self.w), dtype=torch.uint16, device=dev)
+            cx.check(lib().dsgpu_scene_render(cx.handle, ctypes.byref(d), ctypes.c_void_p(t.data_ptr()), 0),
+                     "dsgpu_scene_render")
+            return t
+        x0, y0, cw, ch = (int(v) for v in window)
+        t = torch.empty((ch, cw), dtype=torch.uint16, device=dev)
+        cx.check(lib().dsgpu_scene_render_window(cx.handle, ctypes.byref(d), x0, y0, cw, ch,
+                                                 ctypes.c_void_p(t.data_ptr()), 0), "dsgpu_scene_render_window")
         return t
 
     def sigma_norm(self, level: float = 0.5) -> float:

@@ -39,9 +39,9 @@ EXPORTS = [
     "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_estimate_noise", "dsgpu_guided_filter",
     "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_cnn_param_count", "dsgpu_cnn_create", "dsgpu_cnn_destroy",
     "dsgpu_cnn_state", "dsgpu_cnn_gradients", "dsgpu_cnn_train_step", "dsgpu_cnn_infer", "dsgpu_cnn_denoise",
-    "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
+    "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_cnn_set_loss", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
     "dsgpu_measure_mma_sync",
-    "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render",
+    "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render", "dsgpu_scene_render_window",
 ]
 
 
@@ -118,6 +118,7 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_measure_mma_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
             L.dsgpu_cnn_set_engine.argtypes = [vp, vp, i]
             L.dsgpu_cnn_set_clip.argtypes = [vp, vp, f]
+            L.dsgpu_cnn_set_loss.argtypes = [vp, vp, i]
             L.dsgpu_profile.argtypes = [vp, i]
             L.dsgpu_stage_ms.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i)]
             L.dsgpu_launch_count.argtypes = [vp]
@@ -125,6 +126,7 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_scene_render_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
             L.dsgpu_scene_truth_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
             L.dsgpu_scene_render.argtypes = [vp, ctypes.POINTER(SceneDesc), vp, u]
+            L.dsgpu_scene_render_window.argtypes = [vp, ctypes.POINTER(SceneDesc), i, i, i, i, vp, u]
             for name in EXPORTS:
                 if name not in ("dsgpu_strerror", "dsgpu_get_stream", "dsgpu_last_error", "dsgpu_launch_count"):
                     getattr(L, name).restype = i

@@ -184,6 +184,12 @@ class ResidualCNN:
         """Clip the global gradient norm to max_norm in train_step (0: off)."""
         self.ctx.check(lib().dsgpu_cnn_set_clip(self.ctx.handle, self.handle, float(max_norm)), "dsgpu_cnn_set_clip")
 
+    def set_loss(self, relative: bool) -> None:
+        """Training loss: plain MSE, or (relative) squared errors weighted by
+        1 / strength^2, the error relative to the frame's noise level."""
+        self.ctx.check(lib().dsgpu_cnn_set_loss(self.ctx.handle, self.handle, int(bool(relative))),
+                       "dsgpu_cnn_set_loss")
+
     def set_engine(self, tensor_core_gen5: bool) -> None:
         """Inference on tcgen05 (default) or on the mma.sync kernels."""
         self.ctx.check(lib().dsgpu_cnn_set_engine(self.ctx.handle, self.handle, int(bool(tensor_core_gen5))),

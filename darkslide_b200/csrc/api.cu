@@ -11,6 +11,8 @@
 
 ds_scene ds_scene_make(const dsgpu_scene_desc* d);
 cudaError_t ds_launch_scene(cudaStream_t st, const ds_scene& s, uint16_t* out);
+cudaError_t ds_launch_scene_window(cudaStream_t st, const ds_scene& s, int x0, int y0, int cw, int ch,
+                                   uint16_t* out);
 void ds_scene_host(const ds_scene& s, int x0, int y0, int cw, int ch, uint16_t* out);
 void ds_scene_truth(const ds_scene& s, int x0, int y0, int cw, int ch, float* out);
 cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, double* ex2_per_s,
@@ -29,6 +31,7 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
                              float strength, const float* tgt, int B, float* loss_sum_host);
 cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr);
 void ds_cnn_set_clip(DsCnn* net, float clip);
+void ds_cnn_set_loss(DsCnn* net, int relative);
 void ds_cnn_set_marks(DsCnn* net, cudaEvent_t a, cudaEvent_t b);
 cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out);
 void ds_cnn_set_engine(DsCnn* net, int use_tc);
@@ -752,6 +755,12 @@ int dsgpu_cnn_set_clip(dsgpu_ctx* ctx, dsgpu_cnn* c, float max_norm) {
   return DSGPU_OK;
 }
 
+int dsgpu_cnn_set_loss(dsgpu_ctx* ctx, dsgpu_cnn* c, int relative) {
+  if (!ctx || !c || relative < 0 || relative > 1) return DSGPU_ERR_ARG;
+  ds_cnn_set_loss(c->net, relative);
+  return DSGPU_OK;
+}
+
 int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, int h, float strength, float* out_rgb,
                     unsigned flags) {
   if (!ctx || !c) return DSGPU_ERR_ARG;
@@ -899,6 +908,24 @@ int dsgpu_scene_render(dsgpu_ctx* ctx, const dsgpu_scene_desc* d, uint16_t* out,
   DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, bytes, &dout));
   ds_scene s = ds_scene_make(d);
   DS_TRY(ds_launch_scene(ctx->stream, s, (uint16_t*)dout));
+  ctx->launches += 1;
+  return finish(ctx, flags, out, dout, bytes);
+}
+
+int dsgpu_scene_render_window(dsgpu_ctx* ctx, const dsgpu_scene_desc* d, int x0, int y0, int cw, int ch,
+                              uint16_t* out, unsigned flags) {
+  if (!ctx || !d || !out || d->w <= 0 || d->h <= 0 || cw < 0 || ch < 0) return DSGPU_ERR_ARG;
+  if (x0 < 0 || y0 < 0 || x0 + cw > d->w || y0 + ch > d->h) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(d->w, d->h));
+  ds_pat pat;
+  DS_CHECK(check_pat(d->cfa, &pat));
+  DeviceGuard g(ctx->device);
+  const size_t bytes = (size_t)cw * ch * sizeof(uint16_t);
+  if (bytes == 0) return DSGPU_OK;
+  void* dout;
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, bytes, &dout));
+  ds_scene s = ds_scene_make(d);
+  DS_TRY(ds_launch_scene_window(ctx->stream, s, x0, y0, cw, ch, (uint16_t*)dout));
   ctx->launches += 1;
   return finish(ctx, flags, out, dout, bytes);
 }

@@ -326,8 +326,12 @@ __global__ void pack_input_tc_kernel(const float* __restrict__ rgb, int w, int h
 
 // MSE over n pixels x 3 channels: dY = 2 (out - t) / (3n) into NHWC16 bf16
 // (channels 3..15 zero); per-CTA partial sums of (out - t)^2.
+// relative != 0: every pixel's squared error is weighted by 1 / s^2, s its
+// strength input (smap[p], or s_const without a map), so frames of every
+// noise level count by their error relative to the noise.
 __global__ void mse_kernel(const float* __restrict__ out, const float* __restrict__ tgt, size_t n,
-                           bf16* __restrict__ dy, float* __restrict__ part) {
+                           const float* __restrict__ smap, float s_const, int relative, bf16* __restrict__ dy,
+                           float* __restrict__ part) {
   __shared__ float s[CNN_THREADS];
   const float scale = 2.0f / (3.0f * (float)n);
   float acc = 0.f;
@@ -335,11 +339,16 @@ __global__ void mse_kernel(const float* __restrict__ out, const float* __restric
     __align__(16) bf16 v[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) v[k] = __float2bfloat16_rn(0.f);
+    float w = 1.f;
+    if (relative) {
+      const float sp = smap ? smap[p] : s_const;
+      if (sp > 0.f) w = 1.f / (sp * sp);
+    }
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const float d = out[p * 3 + k] - tgt[p * 3 + k];
-      acc += d * d;
-      v[k] = __float2bfloat16_rn(d * scale);
+      acc += w * d * d;
+      v[k] = __float2bfloat16_rn(w * d * scale);
     }
     reinterpret_cast<uint4*>(dy + p * 16)[0] = reinterpret_cast<uint4*>(v)[0];
     reinterpret_cast<uint4*>(dy + p * 16)[1] = reinterpret_cast<uint4*>(v)[1];
@@ -508,6 +517,7 @@ struct DsCnn {
   long long step = 0;
   bool packed = false;   // wf/wd/bias match params (cleared whenever params may change)
   float clip = 0.f;      // global gradient-norm clip of the Adam step (0: off)
+  int relative_loss = 0; // 1: squared errors weighted by 1 / strength^2
   cudaEvent_t mark_a = nullptr, mark_b = nullptr;  // profiling: around the hidden layers of inference
   float* gsq = nullptr;  // device: sum of squared gradients
   // training buffers (max_batch crops of crop x crop)
@@ -657,7 +667,8 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
   pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, strength_map, strength, net->act[0]);
   if ((e = forward(net, st, net->act[0], rgb, B, H, W, net->act, net->out)) != cudaSuccess) return e;
   const int lgrid = 512;
-  mse_kernel<<<lgrid, CNN_THREADS, 0, st>>>(net->out, tgt, n, net->dy8, net->lpart);
+  mse_kernel<<<lgrid, CNN_THREADS, 0, st>>>(net->out, tgt, n, strength_map, strength, net->relative_loss, net->dy8,
+                                            net->lpart);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
   const int grid = sms * 3;
@@ -750,6 +761,8 @@ cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, i
 void ds_cnn_set_engine(DsCnn* net, int use_tc) { net->use_tc = use_tc != 0; }
 
 void ds_cnn_set_clip(DsCnn* net, float clip) { net->clip = clip > 0.f ? clip : 0.f; }
+
+void ds_cnn_set_loss(DsCnn* net, int relative) { net->relative_loss = relative != 0; }
 
 void ds_cnn_set_marks(DsCnn* net, cudaEvent_t a, cudaEvent_t b) {
   net->mark_a = a;

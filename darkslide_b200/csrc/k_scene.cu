@@ -10,11 +10,12 @@
 
 namespace {
 
-__global__ void scene_kernel(ds_scene s, uint16_t* __restrict__ out) {
+// The window [x0, x0+cw) x [y0, y0+ch) of the frame into out (cw*ch).
+__global__ void scene_kernel(ds_scene s, int x0, int y0, int cw, uint16_t* __restrict__ out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
-  if (x >= s.w) return;
-  out[(size_t)y * s.w + x] = ds_scene_pixel(&s, x, y);
+  if (x >= cw) return;
+  out[(size_t)y * cw + x] = ds_scene_pixel(&s, x0 + x, y0 + y);
 }
 
 template <class F>
@@ -38,10 +39,16 @@ ds_scene ds_scene_make(const dsgpu_scene_desc* d) {
   return s;
 }
 
-cudaError_t ds_launch_scene(cudaStream_t st, const ds_scene& s, uint16_t* out) {
-  dim3 grid((s.w + 255) / 256, s.h);
-  scene_kernel<<<grid, 256, 0, st>>>(s, out);
+cudaError_t ds_launch_scene_window(cudaStream_t st, const ds_scene& s, int x0, int y0, int cw, int ch,
+                                   uint16_t* out) {
+  if (cw <= 0 || ch <= 0) return cudaSuccess;
+  dim3 grid((cw + 255) / 256, ch);
+  scene_kernel<<<grid, 256, 0, st>>>(s, x0, y0, cw, out);
   return cudaGetLastError();
+}
+
+cudaError_t ds_launch_scene(cudaStream_t st, const ds_scene& s, uint16_t* out) {
+  return ds_launch_scene_window(st, s, 0, 0, s.w, s.h, out);
 }
 
 void ds_scene_host(const ds_scene& s, int x0, int y0, int cw, int ch, uint16_t* out) {

@@ -10,7 +10,13 @@ dataset / crops_per_frame frames, frame f drawn from seed `seed * 100003 + 1 +
 f` (its scene and its window positions), so the same crops come back in every
 epoch. Training runs `crops` crop visits (crops / dataset epochs); every epoch
 visits the frames in a new order, `mix` frames at a time, and every batch
-mixes crops of those frames (so of several noise levels). The learning rate
+mixes crops of those frames (so of several noise levels). Each frame is a
+512 x 512 window (at an even position) of a scene whose size is drawn
+log-uniformly between 512 and 9504 px on the long side: the generator lays
+its sinusoids and edges out over the whole scene, so windows of large scenes
+are as smooth as a crop of a camera-size frame. The loss is plain MSE
+(--relative-loss weights each pixel's squared error by 1 / strength^2). The
+learning rate
 warms up linearly and then follows a cosine, and the global gradient norm is
 clipped at `clip_factor` x the median norm of the first batches. A logged
 loss above 5x its running mean (a divergence, after which ReLU units die
@@ -35,19 +41,43 @@ PATTERNS = [ds.RGGB, ds.BGGR, ds.GRBG, ds.GBRG]
 SEARCH, PATCH = 10, 3
 
 
-def make_frame(seed: int, w: int, h: int, dev, ctx=None):
-    """(rgb, target, h_param, scene) of one synthetic frame, device tensors."""
+def draw_virtual(seed: int, w: int, h: int):
+    """A frame size log-uniform in 512..9504 px on the long side (aspect 1,
+    4:3 or 3:2) holding a w x h window at an even position: (W, H, x0, y0)."""
+    rng = np.random.default_rng(seed ^ 0xF00D)
+    L = float(np.exp(rng.uniform(np.log(512), np.log(9504))))
+    aspect = (1.0, 4 / 3, 1.5)[rng.integers(3)]
+    W, H = max(w, int(L)), max(h, int(L / aspect))
+    x0 = 2 * int(rng.integers(0, (W - w) // 2 + 1))
+    y0 = 2 * int(rng.integers(0, (H - h) // 2 + 1))
+    return W, H, x0, y0
+
+
+def make_frame(seed: int, w: int, h: int, dev, ctx=None, bits=None, gain=None, read_sigma=None, virtual=None):
+    """(rgb, target, h_param, scene, (x0, y0)) of a w x h synthetic frame,
+    device tensors. bits / gain / read_sigma default to draws from the seed.
+    virtual = (W, H, x0, y0): the frame is that window of a W x H scene (the
+    generator lays its sinusoids and edges out over the whole W x H, so large
+    scenes are smooth at the pixel scale); "draw" draws one (draw_virtual)."""
     rng = np.random.default_rng(seed)
-    bits = 12 if rng.random() < 0.5 else 14
+    b_draw = 12 if rng.random() < 0.5 else 14
+    pattern = PATTERNS[rng.integers(4)]
+    g_draw, r_draw = float(rng.uniform(0.25, 1.0)), float(rng.uniform(2.0, 12.0))
+    bits = bits or b_draw
     black, white = (256, 4095) if bits == 12 else (512, 16383)
-    sc = ds.Scene(seed=seed, w=w, h=h, pattern=PATTERNS[rng.integers(4)], black=black, white=white,
-                  gain=float(rng.uniform(0.25, 1.0)), read_sigma=float(rng.uniform(2.0, 12.0)))
-    raw = sc.render(dev, ctx=ctx)
+    if virtual == "draw":
+        virtual = draw_virtual(seed, w, h)
+    W, H, x0, y0 = virtual or (w, h, 0, 0)
+    sc = ds.Scene(seed=seed, w=W, h=H, pattern=pattern, black=black, white=white,
+                  gain=gain if gain is not None else g_draw,
+                  read_sigma=read_sigma if read_sigma is not None else r_draw)
+    raw = sc.render(dev, ctx=ctx, window=(x0, y0, w, h))
+    # x0, y0 are even, so the window has the frame's CFA layout
     cfa = ds.normalize_u16(raw, sc.pattern, black, np.full(3, white, np.float32), ctx=ctx)
     rgb = ds.rcd_bayer(cfa, [2.0, 1.0, 1.0 / 0.7], ctx=ctx).data
     hp = 1.5 * sc.sigma_norm()
     tgt = ds.nlm(ds.Image3(w, h, rgb), hp, SEARCH, PATCH, ctx=ctx).data
-    return rgb, tgt, hp, sc
+    return rgb, tgt, hp, sc, (x0, y0)
 
 
 def psnr(a, b, peak=1.0):
@@ -58,7 +88,8 @@ def psnr(a, b, peak=1.0):
 
 
 def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=64, mix=8, warmup=500,
-          clip_factor=3.0, seed=0, out=None, resume=None, log_every=200, verbose=True, dataset=200000):
+          clip_factor=3.0, seed=0, out=None, resume=None, log_every=200, verbose=True, dataset=200000,
+          relative=False):
     import torch
 
     dev = torch.device("cuda", 0)
@@ -68,6 +99,7 @@ def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=
     net = cnn.ResidualCNN(ctx, max_batch=batch, crop=crop, seed=seed)
     if resume:
         net.load(resume)
+    net.set_loss(relative)
     steps = max(1, crops // batch)
     n_frames = max(mix, dataset // crops_per_frame)
     rng = np.random.default_rng(seed + 12345)
@@ -81,7 +113,7 @@ def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=
             queue.extend(int(f) for f in rng.permutation(n_frames))
         for _ in range(mix):
             fseed = seed * 100003 + 1 + queue.pop()
-            rgb, tgt, hp, _ = make_frame(fseed, frame, frame, dev, ctx)
+            rgb, tgt, hp, _, _ = make_frame(fseed, frame, frame, dev, ctx, virtual="draw")
             pos = np.random.default_rng(fseed ^ 0x5EED).integers(0, frame - crop + 1, (crops_per_frame, 2))
             pool.extend((rgb, tgt, hp, int(y), int(x)) for y, x in pos)
         order = rng.permutation(len(pool))
@@ -138,27 +170,43 @@ def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=
     return net, losses, time.time() - t0
 
 
-def evaluate(net, n_frames=4, w=1024, h=1024, seed=10_000_999, verbose=True):
+# (bits, gain e/DN, read sigma DN, scene size) of the fixed evaluation grid:
+# whole 1024 x 1024 scenes, and central windows of 6000 x 4000 scenes
+EVAL_GRID = [(b, 0.5, r, sz) for sz in ((1024, 1024), (6000, 4000)) for b in (12, 14) for r in (2.0, 6.0, 12.0)]
+
+
+def evaluate(net, n_frames=4, w=1024, h=1024, seed=10_000_999, verbose=True, grid=True):
     """PSNR (dB) against the noise-free scene of the noisy RCD output, plain
-    NLM and the CNN, and PSNR of the CNN against NLM, averaged over frames.
-    The frame seeds lie far outside the training set's."""
+    NLM and the CNN, and PSNR of the CNN against NLM, averaged over n_frames
+    random frames and (grid) the frames of EVAL_GRID; also the mean and the
+    worst PSNR loss of the CNN against NLM. The frame seeds lie far outside
+    the training set's."""
     import torch
 
     dev = torch.device("cuda", 0)
     res = {"noisy": [], "nlm": [], "cnn": [], "cnn_vs_nlm": []}
-    for k in range(n_frames):
-        rgb, tgt, hp, sc = make_frame(seed + k, w, h, dev)
+    cases = [dict()] * n_frames
+    if grid:
+        for b, g, r, (W, H) in EVAL_GRID:
+            virt = (W, H, (W - w) // 2 & ~1, (H - h) // 2 & ~1)
+            cases.append(dict(bits=b, gain=g, read_sigma=r, virtual=virt))
+    for k, kw in enumerate(cases):
+        rgb, tgt, hp, sc, (x0, y0) = make_frame(seed + k, w, h, dev, **kw)
         out = net.infer(ds.Image3(w, h, rgb), hp).data
-        truth = torch.from_numpy(sc.truth_host() * np.array([2.0, 1.0, 1.0 / 0.7], np.float32)).to(dev)
+        truth = torch.from_numpy(sc.truth_host(x0, y0, w, h) * np.array([2.0, 1.0, 1.0 / 0.7], np.float32)).to(dev)
         m = 16  # ignore the frame border
         sl = (slice(m, h - m), slice(m, w - m))
         res["noisy"].append(psnr(rgb[sl], truth[sl]))
         res["nlm"].append(psnr(tgt[sl], truth[sl]))
         res["cnn"].append(psnr(out[sl], truth[sl]))
         res["cnn_vs_nlm"].append(psnr(out[sl], tgt[sl]))
+        if verbose and kw:
+            print(f"  {kw['bits']}-bit read {kw['read_sigma']} scene {sc.w}x{sc.h}: nlm {res['nlm'][-1]:.2f} cnn {res['cnn'][-1]:.2f} dB", flush=True)
     avg = {k: float(np.mean(v)) for k, v in res.items()}
+    loss = np.array(res["nlm"]) - np.array(res["cnn"])
+    avg["loss_mean"], avg["loss_max"] = float(loss.mean()), float(loss.max())
     if verbose:
-        print("PSNR dB:", {k: round(v, 2) for k, v in avg.items()}, flush=True)
+        print("PSNR dB:", {k: round(v, 3) for k, v in avg.items()}, flush=True)
     return avg
 
 
@@ -173,13 +221,15 @@ def main():
     ap.add_argument("--mix", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=500)
     ap.add_argument("--clip", type=float, default=3.0, help="clip factor x initial median gradient norm (0: off)")
+    ap.add_argument("--relative-loss", action="store_true", help="weight squared errors by 1 / strength^2")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     ap.add_argument("--resume", default=None)
     ap.add_argument("--eval", type=int, default=4)
     a = ap.parse_args()
     net, losses, secs = train(a.crops, a.batch, a.crop, a.lr, frame=a.frame, mix=a.mix, warmup=a.warmup,
-                              clip_factor=a.clip, seed=a.seed, out=a.out, resume=a.resume, dataset=a.dataset)
+                              clip_factor=a.clip, seed=a.seed, out=a.out, resume=a.resume, dataset=a.dataset,
+                              relative=a.relative_loss)
     print(f"trained {a.crops} crop visits of a {a.dataset}-crop set in {secs:.1f} s", flush=True)
     if a.eval:
         evaluate(net, a.eval)

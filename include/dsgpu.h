@@ -220,6 +220,11 @@ int dsgpu_cnn_train_step(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* rgb, const
 /* Clip the global L2 norm of the gradient to max_norm before each Adam step
  * of dsgpu_cnn_train_step (0, the default: no clipping). */
 int dsgpu_cnn_set_clip(dsgpu_ctx* ctx, dsgpu_cnn* net, float max_norm);
+/* Loss of dsgpu_cnn_gradients / dsgpu_cnn_train_step: relative = 0 (default)
+ * sum((out - target)^2) / (3 n); relative = 1 weights every pixel's squared
+ * error by 1 / strength^2 (its strength input), so that low-noise frames
+ * weigh as much as noisy ones. */
+int dsgpu_cnn_set_loss(dsgpu_ctx* ctx, dsgpu_cnn* net, int relative);
 /* out = in + network(in, strength) on a whole interleaved RGB image
  * (strength = DSGPU_CNN_STRENGTH_SCALE * h). */
 #define DSGPU_CNN_STRENGTH_SCALE 50.0f

@@ -38,6 +38,11 @@ int dsgpu_scene_truth_host(const dsgpu_scene_desc* d, int x0, int y0, int cw, in
 /* GPU render of the whole frame (w*h u16) on the context stream. */
 int dsgpu_scene_render(dsgpu_ctx* ctx, const dsgpu_scene_desc* d, uint16_t* out, unsigned flags);
 
+/* GPU render of the crop [x0, x0+cw) x [y0, y0+ch) of the frame (cw*ch u16),
+ * equal to the same window of the whole-frame render. */
+int dsgpu_scene_render_window(dsgpu_ctx* ctx, const dsgpu_scene_desc* d, int x0, int y0, int cw, int ch,
+                              uint16_t* out, unsigned flags);
+
 #ifdef __cplusplus
 }
 #endif

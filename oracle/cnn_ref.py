@@ -46,8 +46,10 @@ def conv_back(x, w, dy):
 
 
 def forward(params, rgb, strength):
+    """strength: a scalar or a [B, H, W] map."""
     layers = unpack(np.asarray(params, np.float64))
-    x = np.concatenate([rgb, np.full(rgb.shape[:3] + (1,), strength)], axis=-1).astype(np.float64)
+    smap = np.broadcast_to(np.asarray(strength, np.float64)[..., None], rgb.shape[:3] + (1,))
+    x = np.concatenate([rgb, smap], axis=-1).astype(np.float64)
     acts = [x]
     for i, (w, b) in enumerate(layers):
         y = conv(acts[-1], w, b)
@@ -55,13 +57,15 @@ def forward(params, rgb, strength):
     return rgb + acts[-1], acts
 
 
-def gradients(params, rgb, strength, target):
-    """(flat gradient, loss_sum) of sum((out - target)^2) / (3 n)."""
+def gradients(params, rgb, strength, target, weight=None):
+    """(flat gradient, loss_sum) of sum(weight * (out - target)^2) / (3 n);
+    weight: None (1), a scalar or a [B, H, W] map."""
     layers = unpack(np.asarray(params, np.float64))
     out, acts = forward(params, rgb, strength)
     n = rgb.shape[0] * rgb.shape[1] * rgb.shape[2]
     d = out - target
-    dy = 2.0 * d / (3.0 * n)
+    wt = 1.0 if weight is None else np.broadcast_to(np.asarray(weight, np.float64)[..., None], d.shape)
+    dy = 2.0 * wt * d / (3.0 * n)
     grads = []
     for i in range(len(layers) - 1, -1, -1):
         w, _ = layers[i]
@@ -72,7 +76,7 @@ def gradients(params, rgb, strength, target):
     flat = []
     for dw, db in reversed(grads):
         flat += [dw.ravel(), db.ravel()]
-    return np.concatenate(flat), float((d ** 2).sum())
+    return np.concatenate(flat), float((wt * d ** 2).sum())
 
 
 def bf16_round(a):

@@ -75,6 +75,32 @@ def test_gradients_match_fp64(torch_dev, crop):
             assert cos >= 0.995 and rel <= 5e-2, (i, sl, cos, rel)
 
 
+def test_relative_loss_gradients_match_fp64(torch_dev):
+    """Loss weighted by 1 / strength^2 with a strength map that differs per crop."""
+    import cnn_ref as C
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    crop = 16
+    p = cnn.init_params(6)
+    p[-1299:] = np.random.default_rng(6).normal(0, 0.05, 1299)
+    net = cnn.ResidualCNN(max_batch=2, crop=crop, params=p)
+    net.set_loss(True)
+    rgb, tgt, trgb, ttgt = _batch(torch, dev, 2, crop, 8)
+    smap = np.stack([np.full((crop, crop), 0.3, np.float32), np.full((crop, crop), 1.7, np.float32)])
+    g, loss = net.gradients(trgb, 0.0, ttgt, strength_map=torch.from_numpy(smap).to(dev))
+    g = g.cpu().numpy()
+    gr, loss_r = C.gradients(C.bf16_round(p), C.bf16_round(rgb), C.bf16_round(smap), tgt,
+                             weight=1.0 / smap.astype(np.float64) ** 2)
+    assert abs(loss - loss_r) <= 2e-2 * loss_r
+    for i, (ws, bs, _) in enumerate(cnn.layer_slices()):
+        for sl in (ws, bs):
+            a, b = g[sl], gr[sl]
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+            rel = float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30))
+            assert cos >= 0.995 and rel <= 5e-2, (i, sl, cos, rel)
+
+
 def test_adam_step_and_bit_identical_resume(torch_dev, tmp_path):
     from darkslide_b200 import cnn
 

@@ -50,6 +50,16 @@ def test_scene_gpu_render_equals_host(ctx, wh):
     np.testing.assert_array_equal(gpu, sc.render_host())
 
 
+def test_scene_gpu_window_equals_frame(ctx):
+    sc = ds.Scene(seed=7, w=3001, h=2003, pattern=ds.RGGB, black=256, white=4095, gain=0.6, read_sigma=5)
+    full = sc.render().cpu().numpy()
+    for win in [(0, 0, 512, 512), (1234, 777, 300, 211), (2489, 1491, 512, 512)]:
+        x0, y0, cw, ch = win
+        got = sc.render(window=win).cpu().numpy()
+        np.testing.assert_array_equal(got, full[y0:y0 + ch, x0:x0 + cw])
+    np.testing.assert_array_equal(sc.render(window=(5, 9, 40, 30)).cpu().numpy(), sc.render_host(5, 9, 40, 30))
+
+
 @pytest.mark.parametrize("name", list(PATTERNS))
 def test_normalize_u16_bitexact(ctx, oracle, name):
     rng = np.random.default_rng(1)
