@@ -1,6 +1,7 @@
 // The learned stand-in for NLM: a residual CNN of 8 conv3x3 layers
-// (4 -> 48 -> ... -> 48 -> 3, ReLU between), input = demosaiced RGB plus a
-// constant map of the NLM strength, output = input RGB + network output.
+// (4 -> 48 -> ... -> 48 -> 3, ReLU between; dilations 1,2,3,4,3,2,1,1),
+// input = demosaiced RGB plus a constant map of the NLM strength, output =
+// input RGB + network output.
 // It is trained on the GPU to reproduce plain NLM (enhance.rs:36-72) and
 // runs with NLM as the per-tile fallback.
 //
@@ -26,7 +27,9 @@ namespace {
 typedef __nv_bfloat16 bf16;
 
 constexpr int CT_W = 16, CT_H = 8;             // output tile: 8 rows of 16 pixels
-constexpr int CT_XW = CT_W + 2, CT_XH = CT_H + 2;  // with the 1-pixel halo
+// staged input tile of a conv with dilation D: the output tile plus a D-pixel halo
+__host__ __device__ constexpr int ct_xw(int D) { return CT_W + 2 * D; }
+__host__ __device__ constexpr int ct_xh(int D) { return CT_H + 2 * D; }
 constexpr int CNN_THREADS = 256;
 
 enum { EPI_RELU = 0, EPI_MASK = 1, EPI_RESID = 2 };
@@ -71,7 +74,7 @@ __device__ __forceinline__ TileIdx tile_of(int t, int tiles_x, int tiles_y) {
   return r;
 }
 
-// stage an NHWC tile with a 1-pixel halo (zero outside the image)
+// stage an NHWC tile (zero outside the image)
 template <int C, int PW, int PH>
 __device__ __forceinline__ void stage_tile(unsigned char* dst, const bf16* __restrict__ src, int b, int H, int W,
                                            int x0, int y0) {
@@ -87,7 +90,7 @@ __device__ __forceinline__ void stage_tile(unsigned char* dst, const bf16* __res
   }
 }
 
-template <int CIN, int COUT, int EPI>
+template <int CIN, int COUT, int EPI, int D>
 __global__ void __launch_bounds__(CNN_THREADS) conv_fwd_kernel(const bf16* __restrict__ x, int B, int H, int W,
                                                                const bf16* __restrict__ wt,
                                                                const float* __restrict__ bias, bf16* __restrict__ y,
@@ -98,7 +101,8 @@ __global__ void __launch_bounds__(CNN_THREADS) conv_fwd_kernel(const bf16* __res
   constexpr int RSX = row_stride(CIN), RSW = row_stride(CIN), NT = COUT / 8;
   extern __shared__ __align__(16) unsigned char sm[];
   unsigned char* ws = sm;                    // [9][COUT] rows of CIN bf16
-  unsigned char* xs = sm + 9 * COUT * RSW;   // [CT_XH][CT_XW] pixels of CIN bf16
+  unsigned char* xs = sm + 9 * COUT * RSW;   // [ct_xh(D)][ct_xw(D)] pixels of CIN bf16
+  constexpr int XW = ct_xw(D), XH = ct_xh(D);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   {
     constexpr int CH = CIN * 2 / 16;
@@ -113,7 +117,7 @@ __global__ void __launch_bounds__(CNN_THREADS) conv_fwd_kernel(const bf16* __res
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const TileIdx ti = tile_of(t, tiles_x, tiles_y);
     __syncthreads();  // weights staged / previous tile consumed
-    stage_tile<CIN, CT_XW, CT_XH>(xs, x, ti.b, H, W, ti.x0 - 1, ti.y0 - 1);
+    stage_tile<CIN, XW, XH>(xs, x, ti.b, H, W, ti.x0 - D, ti.y0 - D);
     __syncthreads();
     float acc[NT][4];
 #pragma unroll
@@ -124,8 +128,8 @@ __global__ void __launch_bounds__(CNN_THREADS) conv_fwd_kernel(const bf16* __res
 #pragma unroll
       for (int kc = 0; kc < CIN / 16; kc++) {
         unsigned a0, a1, a2, a3;
-        ldsm_x4(smem_u32(xs + ((warp + ky) * CT_XW + (lane & 15) + kx) * RSX + (kc * 16 + (lane >> 4) * 8) * 2), a0,
-                a1, a2, a3);
+        ldsm_x4(smem_u32(xs + ((warp + ky * D) * XW + (lane & 15) + kx * D) * RSX + (kc * 16 + (lane >> 4) * 8) * 2),
+                a0, a1, a2, a3);
 #pragma unroll
         for (int j = 0; j + 1 < NT; j += 2) {
           const int co = (j + (lane >> 4)) * 8 + (lane & 7);
@@ -176,15 +180,16 @@ __global__ void __launch_bounds__(CNN_THREADS) conv_fwd_kernel(const bf16* __res
 // Weight gradient: dW[tap][co][ci] = sum_p dY[p][co] X[p + tap][ci]. A warp
 // owns up to 4 (tap, 16-channel block of co) units; K runs over the 16
 // pixels of each tile row. Partial sums per CTA go to `part`.
-template <int CIN, int COUTW>
+template <int CIN, int COUTW, int D>
 __global__ void __launch_bounds__(CNN_THREADS) conv_wgrad_kernel(const bf16* __restrict__ x,
                                                                  const bf16* __restrict__ dy, int B, int H, int W,
                                                                  float* __restrict__ part) {
   constexpr int RSX = row_stride(CIN), RSD = row_stride(COUTW);
   constexpr int MT = COUTW / 16, UNITS = 9 * MT, UPW = (UNITS + 7) / 8, NT = CIN / 8;
   extern __shared__ __align__(16) unsigned char sm[];
-  unsigned char* xs = sm;                          // [CT_XH][CT_XW] x CIN
-  unsigned char* ds = sm + CT_XH * CT_XW * RSX;    // [CT_H][CT_W] x COUTW
+  constexpr int XW = ct_xw(D), XH = ct_xh(D);
+  unsigned char* xs = sm;                          // [XH][XW] x CIN
+  unsigned char* ds = sm + XH * XW * RSX;          // [CT_H][CT_W] x COUTW
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, c = lane & 3;
   float acc[UPW][NT][4];
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(CNN_THREADS) conv_wgrad_kernel(const bf16* __r
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const TileIdx ti = tile_of(t, tiles_x, tiles_y);
     __syncthreads();
-    stage_tile<CIN, CT_XW, CT_XH>(xs, x, ti.b, H, W, ti.x0 - 1, ti.y0 - 1);
+    stage_tile<CIN, XW, XH>(xs, x, ti.b, H, W, ti.x0 - D, ti.y0 - D);
     stage_tile<COUTW, CT_W, CT_H>(ds, dy, ti.b, H, W, ti.x0, ti.y0);  // zero outside the image
     __syncthreads();
 #pragma unroll
@@ -221,7 +226,7 @@ __global__ void __launch_bounds__(CNN_THREADS) conv_wgrad_kernel(const bf16* __r
           const int pix = (lane & 7) + ((lane >> 3) & 1) * 8;
           const int cj = (j + (lane >> 4)) * 8;
           unsigned b0, b1, b2, b3;
-          ldsm_x4_t(smem_u32(xs + ((r + ky) * CT_XW + pix + kx) * RSX + cj * 2), b0, b1, b2, b3);
+          ldsm_x4_t(smem_u32(xs + ((r + ky * D) * XW + pix + kx * D) * RSX + cj * 2), b0, b1, b2, b3);
           mma16816(acc[u][j], a0, a1, a2, a3, b0, b1);
           if (j + 1 < NT) mma16816(acc[u][j + 1], a0, a1, a2, a3, b2, b3);
         }
@@ -302,18 +307,18 @@ __global__ void pack_input_kernel(const float* __restrict__ rgb, size_t n, const
   reinterpret_cast<uint4*>(x + p * 16)[1] = reinterpret_cast<uint4*>(v)[1];
 }
 
-// The tensor-core engine's input: [2][h][wp][8] bf16 (channels 0-2 RGB, 3 the
-// strength, 4-15 zero; columns w..wp-1 zero).
-__global__ void pack_input_tc_kernel(const float* __restrict__ rgb, int w, int h, int wp, float strength,
+// The tensor-core engine's input: [2][hp][wp][8] bf16 (channels 0-2 RGB, 3 the
+// strength, 4-15 zero; columns w..wp-1 and rows h..hp-1 zero).
+__global__ void pack_input_tc_kernel(const float* __restrict__ rgb, int w, int h, int wp, int hp, float strength,
                                      bf16* __restrict__ x) {
-  const size_t n = (size_t)wp * h;
+  const size_t n = (size_t)wp * hp;
   const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const int py = (int)(p / wp), px = (int)(p - (size_t)py * wp);
   __align__(16) bf16 v[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) v[k] = __float2bfloat16_rn(0.f);
-  if (px < w) {
+  if (px < w && py < h) {
     const size_t q = (size_t)py * w + px;
     v[0] = __float2bfloat16_rn(rgb[q * 3]);
     v[1] = __float2bfloat16_rn(rgb[q * 3 + 1]);
@@ -464,44 +469,73 @@ __global__ void residual_check_kernel(const float* __restrict__ in, const float*
 
 // ------------------------------------------------------------------ host side
 
-template <int CIN, int COUT, int EPI>
-cudaError_t launch_fwd(cudaStream_t st, int grid, const bf16* x, int B, int H, int W, const bf16* wt,
-                       const float* bias, bf16* y, const bf16* mask, const float* resid, float* yf) {
-  const size_t smem = (size_t)9 * COUT * row_stride(CIN) + (size_t)CT_XH * CT_XW * row_stride(CIN);
-  cudaError_t e = cudaFuncSetAttribute(conv_fwd_kernel<CIN, COUT, EPI>,
+template <int CIN, int COUT, int EPI, int D>
+cudaError_t launch_fwd_d(cudaStream_t st, int grid, const bf16* x, int B, int H, int W, const bf16* wt,
+                         const float* bias, bf16* y, const bf16* mask, const float* resid, float* yf) {
+  const size_t smem = (size_t)9 * COUT * row_stride(CIN) + (size_t)ct_xh(D) * ct_xw(D) * row_stride(CIN);
+  cudaError_t e = cudaFuncSetAttribute(conv_fwd_kernel<CIN, COUT, EPI, D>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  conv_fwd_kernel<CIN, COUT, EPI><<<grid, CNN_THREADS, smem, st>>>(x, B, H, W, wt, bias, y, mask, resid, yf);
+  conv_fwd_kernel<CIN, COUT, EPI, D><<<grid, CNN_THREADS, smem, st>>>(x, B, H, W, wt, bias, y, mask, resid, yf);
+  return cudaGetLastError();
+}
+
+// conv with dilation d (1..4) over the per-dilation instantiations
+template <int CIN, int COUT, int EPI>
+cudaError_t launch_fwd(cudaStream_t st, int grid, int d, const bf16* x, int B, int H, int W, const bf16* wt,
+                       const float* bias, bf16* y, const bf16* mask, const float* resid, float* yf) {
+  switch (d) {
+    case 1: return launch_fwd_d<CIN, COUT, EPI, 1>(st, grid, x, B, H, W, wt, bias, y, mask, resid, yf);
+    case 2: return launch_fwd_d<CIN, COUT, EPI, 2>(st, grid, x, B, H, W, wt, bias, y, mask, resid, yf);
+    case 3: return launch_fwd_d<CIN, COUT, EPI, 3>(st, grid, x, B, H, W, wt, bias, y, mask, resid, yf);
+    case 4: return launch_fwd_d<CIN, COUT, EPI, 4>(st, grid, x, B, H, W, wt, bias, y, mask, resid, yf);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int CIN, int COUTW, int D>
+cudaError_t launch_wgrad_d(cudaStream_t st, int grid, const bf16* x, const bf16* dy, int B, int H, int W,
+                           float* part) {
+  const size_t smem = (size_t)ct_xh(D) * ct_xw(D) * row_stride(CIN) + (size_t)CT_H * CT_W * row_stride(COUTW);
+  cudaError_t e = cudaFuncSetAttribute(conv_wgrad_kernel<CIN, COUTW, D>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  conv_wgrad_kernel<CIN, COUTW, D><<<grid, CNN_THREADS, smem, st>>>(x, dy, B, H, W, part);
   return cudaGetLastError();
 }
 
 template <int CIN, int COUTW>
-cudaError_t launch_wgrad(cudaStream_t st, int grid, const bf16* x, const bf16* dy, int B, int H, int W,
+cudaError_t launch_wgrad(cudaStream_t st, int grid, int d, const bf16* x, const bf16* dy, int B, int H, int W,
                          float* part) {
-  const size_t smem = (size_t)CT_XH * CT_XW * row_stride(CIN) + (size_t)CT_H * CT_W * row_stride(COUTW);
-  cudaError_t e = cudaFuncSetAttribute(conv_wgrad_kernel<CIN, COUTW>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  conv_wgrad_kernel<CIN, COUTW><<<grid, CNN_THREADS, smem, st>>>(x, dy, B, H, W, part);
-  return cudaGetLastError();
+  switch (d) {
+    case 1: return launch_wgrad_d<CIN, COUTW, 1>(st, grid, x, dy, B, H, W, part);
+    case 2: return launch_wgrad_d<CIN, COUTW, 2>(st, grid, x, dy, B, H, W, part);
+    case 3: return launch_wgrad_d<CIN, COUTW, 3>(st, grid, x, dy, B, H, W, part);
+    case 4: return launch_wgrad_d<CIN, COUTW, 4>(st, grid, x, dy, B, H, W, part);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // layer table: real and padded channel counts
 struct LayerSpec {
   int cin, cout;     // real
   int cinp, coutp;   // forward padding
+  int dil;           // dilation of the 3x3 taps (offsets (ky-1)*dil, (kx-1)*dil)
 };
 constexpr int NL = 8;
-constexpr LayerSpec LAYERS[NL] = {{4, 48, 16, 48},  {48, 48, 48, 48}, {48, 48, 48, 48}, {48, 48, 48, 48},
-                                  {48, 48, 48, 48}, {48, 48, 48, 48}, {48, 48, 48, 48}, {48, 3, 48, 8}};
+// Dilations 1, 2, 3, 4, 3, 2, 1, 1: a 35 x 35 receptive field (8 undilated
+// layers see 17 x 17), covering NLM's 27 x 27 support at 7x7 / 21x21.
+constexpr LayerSpec LAYERS[NL] = {{4, 48, 16, 48, 1},  {48, 48, 48, 48, 2}, {48, 48, 48, 48, 3},
+                                  {48, 48, 48, 48, 4}, {48, 48, 48, 48, 3}, {48, 48, 48, 48, 2},
+                                  {48, 48, 48, 48, 1}, {48, 3, 48, 8, 1}};
 
 }  // namespace
 
 // ----------------------------------------------------------------- network
 
 cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
-                              const void* const* wf, const float* const* bias, const float* rgb, float* out,
-                              int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end);
+                              const void* const* wf, const float* const* bias, const int* dil, const float* rgb,
+                              float* out, int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end);
 
 struct DsCnn {
   int device = 0;
@@ -642,16 +676,16 @@ static cudaError_t forward(DsCnn* net, cudaStream_t st, const bf16* x16, const f
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
   const int grid = sms * 3;
-  cudaError_t e = launch_fwd<16, 48, EPI_RELU>(st, grid, x16, B, H, W, net->wf[0], net->bias[0], acts[1], nullptr,
-                                               nullptr, nullptr);
+  cudaError_t e = launch_fwd<16, 48, EPI_RELU>(st, grid, LAYERS[0].dil, x16, B, H, W, net->wf[0], net->bias[0],
+                                               acts[1], nullptr, nullptr, nullptr);
   if (e == cudaSuccess && hidden_begin) e = cudaEventRecord(hidden_begin, st);
   for (int l = 1; l < NL - 1 && e == cudaSuccess; l++)
-    e = launch_fwd<48, 48, EPI_RELU>(st, grid, acts[l], B, H, W, net->wf[l], net->bias[l], acts[l + 1], nullptr,
-                                     nullptr, nullptr);
+    e = launch_fwd<48, 48, EPI_RELU>(st, grid, LAYERS[l].dil, acts[l], B, H, W, net->wf[l], net->bias[l],
+                                     acts[l + 1], nullptr, nullptr, nullptr);
   if (e == cudaSuccess && hidden_end) e = cudaEventRecord(hidden_end, st);
   if (e == cudaSuccess)
-    e = launch_fwd<48, 8, EPI_RESID>(st, grid, acts[NL - 1], B, H, W, net->wf[NL - 1], net->bias[NL - 1], nullptr,
-                                     nullptr, rgb, out);
+    e = launch_fwd<48, 8, EPI_RESID>(st, grid, LAYERS[NL - 1].dil, acts[NL - 1], B, H, W, net->wf[NL - 1],
+                                     net->bias[NL - 1], nullptr, nullptr, rgb, out);
   return e;
 }
 
@@ -679,27 +713,33 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
     reduce_grads_kernel<<<(nreal + 255) / 256, 256, 0, st>>>(net->wpart, net->wgrid, coutw, cinp, net->bpart,
                                                             net->bgrid, cb, L.cout, L.cin, net->grads + net->off[l]);
   };
-  if ((e = launch_wgrad<48, 16>(st, net->wgrid, net->act[7], net->dy8, B, H, W, net->wpart)) != cudaSuccess) return e;
+  if ((e = launch_wgrad<48, 16>(st, net->wgrid, LAYERS[7].dil, net->act[7], net->dy8, B, H, W, net->wpart)) !=
+      cudaSuccess)
+    return e;
   bias_grad_kernel<16><<<net->bgrid, CNN_THREADS, 0, st>>>(net->dy8, n, net->bpart);
   reduce(7, 16, 48, 16);
   bf16* g = net->gA;
   bf16* gnext = net->gB;
-  if ((e = launch_fwd<16, 48, EPI_MASK>(st, grid, net->dy8, B, H, W, net->wd[7], nullptr, g, net->act[7], nullptr,
-                                        nullptr)) != cudaSuccess)
+  if ((e = launch_fwd<16, 48, EPI_MASK>(st, grid, LAYERS[7].dil, net->dy8, B, H, W, net->wd[7], nullptr, g,
+                                        net->act[7], nullptr, nullptr)) != cudaSuccess)
     return e;
   for (int l = 6; l >= 1; l--) {  // layers 7..2 (index l): dW from (act[l], g); g_next = dgrad(g) * [act[l] > 0]
-    if ((e = launch_wgrad<48, 48>(st, net->wgrid, net->act[l], g, B, H, W, net->wpart)) != cudaSuccess) return e;
+    if ((e = launch_wgrad<48, 48>(st, net->wgrid, LAYERS[l].dil, net->act[l], g, B, H, W, net->wpart)) !=
+        cudaSuccess)
+      return e;
     bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
     reduce(l, 48, 48, 48);
-    if ((e = launch_fwd<48, 48, EPI_MASK>(st, grid, g, B, H, W, net->wd[l], nullptr, gnext, net->act[l], nullptr,
-                                          nullptr)) != cudaSuccess)
+    if ((e = launch_fwd<48, 48, EPI_MASK>(st, grid, LAYERS[l].dil, g, B, H, W, net->wd[l], nullptr, gnext,
+                                          net->act[l], nullptr, nullptr)) != cudaSuccess)
       return e;
     bf16* tmp = g;
     g = gnext;
     gnext = tmp;
   }
   // layer 1: dW from (packed input, g)
-  if ((e = launch_wgrad<16, 48>(st, net->wgrid, net->act[0], g, B, H, W, net->wpart)) != cudaSuccess) return e;
+  if ((e = launch_wgrad<16, 48>(st, net->wgrid, LAYERS[0].dil, net->act[0], g, B, H, W, net->wpart)) !=
+      cudaSuccess)
+    return e;
   bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
   reduce(0, 48, 16, 48);
   if (loss_sum_host) {
@@ -728,8 +768,10 @@ cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr) {
 // Inference on a whole (w x h) RGB image; out = input + network(input).
 cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out) {
   const size_t n = (size_t)w * h;
-  const int wp = (w + 3) / 4 * 4;  // the tensor-core engine pads rows to 4 pixels
-  const size_t na = (size_t)wp * h;
+  // the tensor-core engine pads rows to 4 pixels and planes to 12 rows (a
+  // multiple of every dilation)
+  const int wp = (w + 3) / 4 * 4, hp = (h + 11) / 12 * 12;
+  const size_t na = (size_t)wp * hp;
   cudaError_t e = cudaSuccess;
   if (net->infer_px < na) {
     if (net->ia) cudaFree(net->ia);
@@ -743,14 +785,22 @@ cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, i
   if ((e = ds_cnn_pack(net, st)) != cudaSuccess) return e;
   // ping-pong: input packed into ib (16 ch), layers alternate ia/ib
   if (net->use_tc) {
-    pack_input_tc_kernel<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(rgb, w, h, wp, strength, net->ib);
+    if (hp > h) {  // padding rows of all 6 planes of both activation buffers read as zero
+      const size_t plane = na * 8 * sizeof(bf16), pad = (size_t)(hp - h) * wp * 8 * sizeof(bf16);
+      const size_t off = (size_t)h * wp * 8;
+      if ((e = cudaMemset2DAsync(net->ia + off, plane, 0, pad, 6, st)) != cudaSuccess) return e;
+      if ((e = cudaMemset2DAsync(net->ib + off, plane, 0, pad, 6, st)) != cudaSuccess) return e;
+    }
+    pack_input_tc_kernel<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(rgb, w, h, wp, hp, strength, net->ib);
     const void* wf[NL];
     const float* bs[NL];
     for (int l = 0; l < NL; l++) {
       wf[l] = net->wf[l];
       bs[l] = net->bias[l];
     }
-    return ds_cnn_forward_tc(st, net->ib, net->ia, net->ib, h, w, wf, bs, rgb, out, net->err, net->mark_a,
+    int dil[NL];
+    for (int l = 0; l < NL; l++) dil[l] = LAYERS[l].dil;
+    return ds_cnn_forward_tc(st, net->ib, net->ia, net->ib, h, w, wf, bs, dil, rgb, out, net->err, net->mark_a,
                              net->mark_b);
   }
   pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, nullptr, strength, net->ib);

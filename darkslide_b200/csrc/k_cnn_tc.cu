@@ -148,13 +148,14 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-// TMA load of one 4-D box (channel within a 4-pixel group, group, y, block) into
-// shared memory, completing on bar
-__device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map, int x, int y, int cb, unsigned bar) {
+// TMA load of one 5-D box (channel within a 4-pixel group, group, row residue
+// y mod D, row quotient y div D, block) into shared memory, completing on bar
+__device__ __forceinline__ void tma_load_5d(unsigned dst, const CUtensorMap* map, int x, int yr, int yq, int cb,
+                                            unsigned bar) {
   asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];" ::"r"(dst),
-      "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(x), "r"(y), "r"(cb), "r"(bar)
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(x), "r"(yr), "r"(yq), "r"(cb), "r"(bar)
       : "memory");
 }
 
@@ -162,12 +163,17 @@ __device__ __forceinline__ void mma_commit(unsigned bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-// x: [CIN/8][H][Wp][8] bf16 (Wp = W rounded up to 4; columns W..Wp-1 zero)
-// through `xmap` (4-pixel groups, box 32 x TC_PW/4 x TC_PR x 1); wt:
-// [9][COUT_G][CIN] bf16; NK: output channels per ky block (COUT_G padded to a
-// multiple of 16); y: [COUT_G/8][H][Wp][8] bf16 (ReLU; padding columns
-// written as zero) or yf: [H][W][3] fp32 = resid + conv (residual).
-template <int CIN, int COUT_G, int NK, int EPI>
+// x: [CIN/8][Hp][Wp][8] bf16 (Wp = W rounded up to 4, Hp = H rounded up to
+// 12; padding columns and rows zero) through `xmap` (4-pixel groups, rows
+// split into residue and quotient by DIL; box 32 x TC_PW/4 x 1 x TC_PR x 1);
+// wt: [9][COUT_G][CIN] bf16; NK: output channels per ky block (COUT_G padded
+// to a multiple of 16); y: [COUT_G/8][Hp][Wp][8] bf16 (ReLU; padding columns
+// written as zero, padding rows left alone) or yf: [H][W][3] fp32 = resid +
+// conv (residual). DIL: dilation of the taps. A tile is TC_TR output rows
+// DIL apart (y0, y0 + DIL, ...) by 128 pixels; on that subsampled row grid a
+// dilated conv is an undilated one, so the staging and the stacked-tap MMAs
+// are the same for every DIL.
+template <int CIN, int COUT_G, int NK, int EPI, int DIL>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     conv_tc_kernel(const __grid_constant__ CUtensorMap xmap, int H, int W, const bf16* __restrict__ wt,
                    const float* __restrict__ bias, bf16* __restrict__ y, const float* __restrict__ resid,
@@ -227,14 +233,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const unsigned tmem = *tmem_slot;
 
-  const int tiles_x = (W + TC_M - 1) / TC_M, tiles_y = (H + TC_TR - 1) / TC_TR;
+  // row bands of DIL * TC_TR rows, each split into DIL tiles by row residue
+  const int tiles_x = (W + TC_M - 1) / TC_M, tiles_y = (H + DIL * TC_TR - 1) / (DIL * TC_TR) * DIL;
   const int ntiles = tiles_x * tiles_y;
   const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  // tile k of this CTA: first pixel x0, first output row y0 (then y0 + DIL, ...)
   auto tile_xy = [&](int k, int& x0, int& y0) {
     const int t = blockIdx.x + k * gridDim.x;
     const int ty = t / tiles_x;
     x0 = (t - ty * tiles_x) * TC_M;
-    y0 = ty * TC_TR;
+    const int band = ty / DIL;
+    y0 = band * DIL * TC_TR + (ty - band * DIL);
   };
 
   if (warp == TC_EPI_WARPS + 1) {
@@ -251,8 +260,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           if (!(ok = mbar_wait(empty(q), ((g / TC_RING) & 1) ^ 1, abort_flag))) break;
           mbar_expect_tx(full(q), TX_BYTES);
           const unsigned dst = smem_u32(As) + (unsigned)(q * TC_SUB);
-          tma_load_4d(dst, &xmap, x0 / TC_PG - 1, y0 - 1, 2 * kc, full(q));
-          tma_load_4d(dst + TC_SLAB, &xmap, x0 / TC_PG - 1, y0 - 1, 2 * kc + 1, full(q));
+          // staged rows y0 - DIL, y0, ..., y0 + TC_TR * DIL: residue y0 % DIL, quotients from y0 / DIL - 1
+          const int yr = y0 % DIL, yq = y0 / DIL - 1;
+          tma_load_5d(dst, &xmap, x0 / TC_PG - 1, yr, yq, 2 * kc, full(q));
+          tma_load_5d(dst + TC_SLAB, &xmap, x0 / TC_PG - 1, yr, yq, 2 * kc + 1, full(q));
         }
         if (!ok) break;
       }
@@ -287,8 +298,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const unsigned dcol = dbase + (unsigned)((TC_TR - 1 - j + ky_lo) * NK);  // accumulator of row j - ky_lo
 #pragma unroll
             for (int kx = 0; kx < 3; kx++) {
-              // staged pixel 0 is x0 - 4: output pixel x0 + m reads x0 + m + kx - 1
-              const unsigned aoff = (unsigned)(j * TC_PW + TC_PG - 1 + kx);
+              // staged pixel 0 is x0 - 4: output pixel x0 + m reads x0 + m + (kx - 1) DIL
+              const unsigned aoff = (unsigned)(j * TC_PW + TC_PG - DIL + kx * DIL);
               const unsigned long long b = bdesc + (unsigned)(kx * CB * NS + ky_lo * NK);
               const unsigned long long a = adesc + aoff;
               if (kx == 0 && ky_lo == 0) {
@@ -323,7 +334,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // ---------------- epilogue: warp w owns TMEM lanes 32 (w % 4)..+31 (pixels), rows 2 (w / 4)..+1
     constexpr int RPW = TC_TR / (TC_EPI_WARPS / 4);  // output rows per epilogue warp
     const int quarter = warp & 3, r0 = (warp >> 2) * RPW;
-    const size_t plane = (size_t)H * Wp;
+    const int Hp = (H + 11) / 12 * 12;
+    const size_t plane = (size_t)Hp * Wp;
     for (int k = 0; k < my_tiles; k++) {
       const int s = k & 1;
       bool ok = true;
@@ -347,7 +359,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(tempty(s));
         }
-        const int gy = y0 + r;
+        const int gy = y0 + r * DIL;
         if (gy >= H || px >= Wp) continue;
         if (EPI == TC_RELU) {
           const size_t pix = (size_t)gy * Wp + px;
@@ -389,9 +401,10 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-template <int CIN, int COUT_G, int NK, int EPI>
-cudaError_t launch_tc(cudaStream_t st, const bf16* x, int H, int W, const bf16* wt, const float* bias, bf16* y,
-                      const float* resid, float* yf, int* err) {
+template <int CIN, int COUT_G, int NK, int EPI, int DIL>
+cudaError_t launch_tc_d(cudaStream_t st, const bf16* x, int H, int W, const bf16* wt, const float* bias, bf16* y,
+                        const float* resid, float* yf, int* err) {
+  static_assert(DIL >= 1 && DIL <= TC_PG && 12 % DIL == 0, "the staged row holds a halo of up to 4 pixels");
   constexpr size_t need = (size_t)TC_RING * TC_SUB + (size_t)3 * (CIN / 8) * 3 * NK * 16 + NK * 4 +
                          (2 * TC_RING + 4) * 8 + 16;
   constexpr size_t smem = need > TC_MIN_SMEM ? need : TC_MIN_SMEM;
@@ -400,52 +413,69 @@ cudaError_t launch_tc(cudaStream_t st, const bf16* x, int H, int W, const bf16* 
   if (!enc) return cudaErrorNotSupported;
   if ((reinterpret_cast<uintptr_t>(x) & 15) != 0) return cudaErrorInvalidValue;
   CUtensorMap map;
-  const int Wp = (W + TC_PG - 1) / TC_PG * TC_PG;
-  const cuuint64_t dims[4] = {8 * TC_PG, (cuuint64_t)(Wp / TC_PG), (cuuint64_t)H, (cuuint64_t)(CIN / 8)};
-  const cuuint64_t strides[3] = {16 * TC_PG, (cuuint64_t)Wp * 16, (cuuint64_t)Wp * H * 16};
-  const cuuint32_t box[4] = {8 * TC_PG, (cuuint32_t)(TC_PW / TC_PG), (cuuint32_t)TC_PR, 1};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), dims, strides, box, estr,
+  const int Wp = (W + TC_PG - 1) / TC_PG * TC_PG, Hp = (H + 11) / 12 * 12;
+  // row y = q * DIL + r; Hp is a multiple of DIL, so every (r, q) is a row of the plane
+  const cuuint64_t dims[5] = {8 * TC_PG, (cuuint64_t)(Wp / TC_PG), (cuuint64_t)DIL, (cuuint64_t)(Hp / DIL),
+                              (cuuint64_t)(CIN / 8)};
+  const cuuint64_t strides[4] = {16 * TC_PG, (cuuint64_t)Wp * 16, (cuuint64_t)Wp * 16 * DIL,
+                                 (cuuint64_t)Wp * Hp * 16};
+  const cuuint32_t box[5] = {8 * TC_PG, (cuuint32_t)(TC_PW / TC_PG), 1, (cuuint32_t)TC_PR, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(x), dims, strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT_G, NK, EPI>,
+  cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT_G, NK, EPI, DIL>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int tiles = ((W + TC_M - 1) / TC_M) * ((H + TC_TR - 1) / TC_TR);
+  const int tiles = ((W + TC_M - 1) / TC_M) * ((H + DIL * TC_TR - 1) / (DIL * TC_TR) * DIL);
   const int grid = tiles < sms ? tiles : sms;
-  conv_tc_kernel<CIN, COUT_G, NK, EPI><<<grid, TC_THREADS, smem, st>>>(map, H, W, wt, bias, y, resid, yf, err);
+  conv_tc_kernel<CIN, COUT_G, NK, EPI, DIL><<<grid, TC_THREADS, smem, st>>>(map, H, W, wt, bias, y, resid, yf, err);
   return cudaGetLastError();
+}
+
+template <int CIN, int COUT_G, int NK, int EPI>
+cudaError_t launch_tc(cudaStream_t st, int dil, const bf16* x, int H, int W, const bf16* wt, const float* bias,
+                      bf16* y, const float* resid, float* yf, int* err) {
+  switch (dil) {
+    case 1: return launch_tc_d<CIN, COUT_G, NK, EPI, 1>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 2: return launch_tc_d<CIN, COUT_G, NK, EPI, 2>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 3: return launch_tc_d<CIN, COUT_G, NK, EPI, 3>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 4: return launch_tc_d<CIN, COUT_G, NK, EPI, 4>(st, x, H, W, wt, bias, y, resid, yf, err);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
 
 // One image through the 8 layers on the tensor cores. x16: packed input
-// (16 ch, [2][H][Wp][8]); a, b: ping-pong activations (48 ch, [6][H][Wp][8]); wf/bias: per-layer forward
-// weights (layer 8's with 8 output channels); rgb/out: fp32 RGB;
-// hidden_begin/end (may be null): events recorded around layers 2-7.
+// (16 ch, [2][Hp][Wp][8]); a, b: ping-pong activations (48 ch,
+// [6][Hp][Wp][8]; the padding rows H..Hp-1 must be zero); wf/bias: per-layer
+// forward weights (layer 8's with 8 output channels); dil: per-layer
+// dilations; rgb/out: fp32 RGB; hidden_begin/end (may be null): events
+// recorded around layers 2-7.
 cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
-                              const void* const* wf, const float* const* bias, const float* rgb, float* out,
-                              int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end) {
+                              const void* const* wf, const float* const* bias, const int* dil, const float* rgb,
+                              float* out, int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end) {
   const bf16* in = static_cast<const bf16*>(x16);
   bf16* pa = static_cast<bf16*>(a);
   bf16* pb = static_cast<bf16*>(b);
-  cudaError_t e = launch_tc<16, 48, 48, TC_RELU>(st, in, H, W, static_cast<const bf16*>(wf[0]), bias[0], pa, nullptr,
-                                                 nullptr, err);
+  cudaError_t e = launch_tc<16, 48, 48, TC_RELU>(st, dil[0], in, H, W, static_cast<const bf16*>(wf[0]), bias[0], pa,
+                                                 nullptr, nullptr, err);
   if (e == cudaSuccess && hidden_begin) e = cudaEventRecord(hidden_begin, st);
   for (int l = 1; l < 7 && e == cudaSuccess; l++) {
-    e = launch_tc<48, 48, 48, TC_RELU>(st, pa, H, W, static_cast<const bf16*>(wf[l]), bias[l], pb, nullptr, nullptr,
-                                       err);
+    e = launch_tc<48, 48, 48, TC_RELU>(st, dil[l], pa, H, W, static_cast<const bf16*>(wf[l]), bias[l], pb, nullptr,
+                                       nullptr, err);
     bf16* t = pa;
     pa = pb;
     pb = t;
   }
   if (e == cudaSuccess && hidden_end) e = cudaEventRecord(hidden_end, st);
   if (e == cudaSuccess)
-    e = launch_tc<48, 8, 16, TC_RESID>(st, pa, H, W, static_cast<const bf16*>(wf[7]), bias[7], nullptr, rgb, out,
-                                       err);
+    e = launch_tc<48, 8, 16, TC_RESID>(st, dil[7], pa, H, W, static_cast<const bf16*>(wf[7]), bias[7], nullptr, rgb,
+                                       out, err);
   return e;
 }

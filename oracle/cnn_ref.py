@@ -3,13 +3,15 @@
 TEST INFRASTRUCTURE ONLY: the checker for the GPU CNN kernels' gradients.
 Same layer table, padding (zero, "same") and parameter layout as the
 library: per layer weights [9 taps][cout][cin] (tap = ky*3 + kx, offset
-(ky-1, kx-1)) then biases [cout]; loss = sum((out - target)^2) / (3 n).
+((ky-1) d, (kx-1) d) for the layer's dilation d) then biases [cout];
+loss = sum((out - target)^2) / (3 n).
 """
 from __future__ import annotations
 
 import numpy as np
 
 LAYERS = [(4, 48)] + [(48, 48)] * 6 + [(48, 3)]
+DILATIONS = [1, 2, 3, 4, 3, 2, 1, 1]
 
 
 def unpack(params):
@@ -21,28 +23,28 @@ def unpack(params):
     return out
 
 
-def conv(x, w, b):
+def conv(x, w, b, d=1):
     B, H, W, _ = x.shape
-    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    xp = np.pad(x, ((0, 0), (d, d), (d, d), (0, 0)))
     out = np.zeros((B, H, W, w.shape[1]))
     for t in range(9):
         ky, kx = divmod(t, 3)
-        out += xp[:, ky:ky + H, kx:kx + W, :] @ w[t].T
+        out += xp[:, ky * d:ky * d + H, kx * d:kx * d + W, :] @ w[t].T
     return out + b
 
 
-def conv_back(x, w, dy):
-    """(dx, dw, db) of conv(x, w, b) given dy."""
+def conv_back(x, w, dy, d=1):
+    """(dx, dw, db) of conv(x, w, b, d) given dy."""
     B, H, W, _ = x.shape
-    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    xp = np.pad(x, ((0, 0), (d, d), (d, d), (0, 0)))
     dxp = np.zeros_like(xp)
     dw = np.zeros_like(w)
     for t in range(9):
         ky, kx = divmod(t, 3)
-        xs = xp[:, ky:ky + H, kx:kx + W, :]
+        xs = xp[:, ky * d:ky * d + H, kx * d:kx * d + W, :]
         dw[t] = np.einsum("bhwo,bhwi->oi", dy, xs)
-        dxp[:, ky:ky + H, kx:kx + W, :] += dy @ w[t]
-    return dxp[:, 1:H + 1, 1:W + 1, :], dw, dy.sum(axis=(0, 1, 2))
+        dxp[:, ky * d:ky * d + H, kx * d:kx * d + W, :] += dy @ w[t]
+    return dxp[:, d:H + d, d:W + d, :], dw, dy.sum(axis=(0, 1, 2))
 
 
 def forward(params, rgb, strength):
@@ -52,7 +54,7 @@ def forward(params, rgb, strength):
     x = np.concatenate([rgb, smap], axis=-1).astype(np.float64)
     acts = [x]
     for i, (w, b) in enumerate(layers):
-        y = conv(acts[-1], w, b)
+        y = conv(acts[-1], w, b, DILATIONS[i])
         acts.append(np.maximum(y, 0) if i < len(layers) - 1 else y)
     return rgb + acts[-1], acts
 
@@ -69,7 +71,7 @@ def gradients(params, rgb, strength, target, weight=None):
     grads = []
     for i in range(len(layers) - 1, -1, -1):
         w, _ = layers[i]
-        dx, dw, db = conv_back(acts[i], w, dy)
+        dx, dw, db = conv_back(acts[i], w, dy, DILATIONS[i])
         grads.append((dw, db))
         if i > 0:
             dy = dx * (acts[i] > 0)

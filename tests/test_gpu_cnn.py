@@ -195,3 +195,65 @@ def test_tensor_core_engine_matches_mma_sync_and_fp64(torch_dev, hw):
     assert np.isfinite(tc).all()
     assert np.abs(tc - ms).max() <= 2e-2 * scale
     assert np.abs(tc - ref).max() <= 2e-2 * scale
+
+
+def test_trained_network_gain(torch_dev):
+    """The committed network against the method without it, on a held-out
+    14-bit frame (read noise 6 DN): it removes most of the noise that plain
+    NLM removes (>= 5 dB over the undenoised RCD output, within 1 dB of NLM)
+    and the learned develop is faster than the plain one."""
+    from darkslide_b200 import _lib, cnn, train_cnn
+
+    torch, dev = torch_dev
+    ctx = ds.Context(0)
+    net = cnn.ResidualCNN(ctx)
+    net.load(os.path.join(os.path.dirname(cnn.__file__), "weights", "cnn_nlm.bin"))
+    w = h = 1024
+    stream = torch.cuda.Stream(dev)
+    with torch.cuda.stream(stream):
+        rgb, tgt, hp, sc, _ = train_cnn.make_frame(77_000_001, w, h, dev, ctx, bits=14, gain=0.5, read_sigma=6.0)
+        out = net.infer(ds.Image3(w, h, rgb), hp).data
+    stream.synchronize()
+    truth = torch.from_numpy(sc.truth_host() * np.array([2.0, 1.0, 1.0 / 0.7], np.float32)).to(dev)
+    sl = (slice(16, h - 16), slice(16, w - 16))
+    p_noisy, p_nlm, p_cnn = (train_cnn.psnr(a[sl], truth[sl]) for a in (rgb, tgt, out))
+    assert p_cnn >= p_noisy + 5.0, (p_noisy, p_cnn)
+    assert p_cnn >= p_nlm - 1.0, (p_nlm, p_cnn)
+
+    # speed at 2048 x 2048: learned develop (RCD + CNN + fallback check) vs plain (RCD + NLM)
+    W = H = 2048
+    scene = ds.Scene(seed=5, w=W, h=H, pattern=ds.RGGB, black=512, white=16383, gain=0.5, read_sigma=6)
+    L = _lib.lib()
+    vp = __import__("ctypes").c_void_p
+    pat = ds.RGGB.codes()
+    white = np.full(3, 16383, np.float32)
+    mul = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
+    hpar = 1.5 * scene.sigma_norm()
+    with torch.cuda.stream(stream):
+        raw = scene.render(dev, ctx=ctx)
+        o = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    def plain():
+        ctx.check(L.dsgpu_develop_u16(ctx.handle, vp(raw.data_ptr()), W, H, W, vp(pat.ctypes.data), 512.0,
+                                      vp(white.ctypes.data), vp(mul.ctypes.data), float(hpar), 10, 3,
+                                      vp(o.data_ptr()), vp(0), _lib.DSGPU_ASYNC), "develop")
+
+    def learned():
+        ctx.check(L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, vp(raw.data_ptr()), W, H, W, vp(pat.ctypes.data),
+                                          512.0, vp(white.ctypes.data), vp(mul.ctypes.data), float(hpar), 10, 3,
+                                          3.0, vp(o.data_ptr()), vp(0), _lib.DSGPU_ASYNC), "develop_cnn")
+
+    def timed(f, n=10):
+        for _ in range(3):
+            f()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            f()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    t_plain, t_learned = timed(plain), timed(learned)
+    assert t_learned * 1.3 < t_plain, (t_plain, t_learned)
