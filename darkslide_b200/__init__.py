@@ -36,7 +36,8 @@ from ._lib import Context, DsgpuError, SceneDesc, default_context, lib
 
 __all__ = [
     "CfaPattern", "CfaImage", "Plane", "Image3", "Quality", "demosaic", "rcd_bayer", "mhc_bayer", "clip_plane",
-    "box_blur", "nlm", "normalize_u16", "develop_u16", "estimate_noise", "guided_filter", "denoise", "Oklab", "Context", "DsgpuError", "default_context", "Scene",
+    "box_blur", "nlm", "normalize_u16", "develop_u16", "BatchFrame", "develop_batch", "batch_frame_ms",
+    "autotune", "autotune_get", "autotune_set", "estimate_noise", "guided_filter", "denoise", "Oklab", "Context", "DsgpuError", "default_context", "Scene",
     "RGGB", "BGGR", "GRBG", "GBRG",
 ]
 
@@ -245,6 +246,84 @@ def nlm(p, h_param: float, search: int, patch: int, ctx: Context | None = None):
     c.ctx.check(lib().dsgpu_nlm(c.ctx.handle, pi, p.w, p.h, chans, float(h_param), int(search), int(patch), po,
                                 c.flags), "dsgpu_nlm")
     return Image3(p.w, p.h, out) if chans == 3 else Plane(p.w, p.h, out)
+
+
+@dataclass
+class BatchFrame:
+    """One frame of develop_batch: a CUDA uint16 tensor (h, w), its CFA
+    pattern, levels, white balance and NLM strength; `out` (h, w, 3) and
+    optional `clip` (h, w) float32 CUDA tensors receive the result."""
+    raw: object
+    pattern: "CfaPattern"
+    black: float
+    white: object
+    mul: object
+    h_param: float
+    out: object
+    clip: object = None
+
+
+def develop_batch(frames, search: int, patch: int, ctx: Context | None = None, sync: bool = True) -> None:
+    """u16 raw -> normalise -> RCD -> NLM for many frames (different sizes,
+    CFA layouts, levels and strengths) in one CUDA graph launch
+    (dsgpu_rcd_nlm_batch). Work goes on torch's current stream."""
+    import torch
+
+    frames = list(frames)
+    dev = frames[0].raw.device
+    cx = ctx or default_context(dev.index or 0)
+    cx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    arr = (_lib.Frame * len(frames))()
+    for d, f in zip(arr, frames):
+        h, w = f.raw.shape
+        d.raw = f.raw.data_ptr()
+        d.pitch_elems = f.raw.stride(0)
+        d.w, d.h = w, h
+        d.cfa[:] = [int(v) for v in f.pattern.codes()]
+        d.black = float(f.black)
+        d.white[:] = [float(v) for v in _f3(f.white)]
+        d.mul[:] = [float(v) for v in _f3(f.mul)]
+        d.h_param = float(f.h_param)
+        d.out_rgb = f.out.data_ptr()
+        d.out_clip = f.clip.data_ptr() if f.clip is not None else None
+    flags = 0 if sync else _lib.DSGPU_ASYNC
+    cx.check(lib().dsgpu_rcd_nlm_batch(cx.handle, arr, len(frames), int(search), int(patch), flags),
+             "dsgpu_rcd_nlm_batch")
+
+
+def batch_frame_ms(n: int, ctx: Context | None = None) -> np.ndarray:
+    """Completion time (ms after the batch started on the device) of each of
+    the first n frames of the last develop_batch."""
+    cx = ctx or default_context(0)
+    out = np.zeros(n, np.float64)
+    cx.check(lib().dsgpu_batch_frame_ms(cx.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n),
+             "dsgpu_batch_frame_ms")
+    return out
+
+
+def autotune(sizes, search: int, patch: int, ctx: Context | None = None) -> None:
+    """Tune the batched kernels for each (w, h) size class (dsgpu_autotune)."""
+    cx = ctx or default_context(0)
+    flat = np.ascontiguousarray(np.asarray(sizes, np.int32).reshape(-1))
+    cx.check(lib().dsgpu_autotune(cx.handle, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), flat.size // 2,
+                                  int(search), int(patch)), "dsgpu_autotune")
+
+
+def autotune_get(w: int, h: int, ctx: Context | None = None) -> dict:
+    """The table entry used for a w x h frame: RCD tile shape, NLM CTAs per
+    SM and (exact classes) the tuned RCD time of every shape."""
+    cx = ctx or default_context(0)
+    tw, th, k = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    ms = (ctypes.c_double * 5)()
+    cx.check(lib().dsgpu_autotune_get(cx.handle, int(w), int(h), ctypes.byref(tw), ctypes.byref(th),
+                                      ctypes.byref(k), ms), "dsgpu_autotune_get")
+    return {"rcd_tile": (tw.value, th.value), "nlm_ctas_per_sm": k.value, "rcd_ms": list(ms)}
+
+
+def autotune_set(w: int, h: int, rcd_tile, nlm_ctas_per_sm: int, ctx: Context | None = None) -> None:
+    cx = ctx or default_context(0)
+    cx.check(lib().dsgpu_autotune_set(cx.handle, int(w), int(h), int(rcd_tile[0]), int(rcd_tile[1]),
+                                      int(nlm_ctas_per_sm)), "dsgpu_autotune_set")
 
 
 def develop_u16(raw, pattern: CfaPattern, black: float, white, mul, h_param: float, search: int, patch: int,

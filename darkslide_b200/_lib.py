@@ -42,6 +42,7 @@ EXPORTS = [
     "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_cnn_set_loss", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
     "dsgpu_measure_mma_sync",
     "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render", "dsgpu_scene_render_window",
+    "dsgpu_rcd_nlm_batch", "dsgpu_batch_frame_ms", "dsgpu_autotune", "dsgpu_autotune_get", "dsgpu_autotune_set",
 ]
 
 
@@ -52,6 +53,23 @@ class DsgpuError(RuntimeError):
         if detail:
             msg += f": {detail}"
         super().__init__(msg)
+
+
+class Frame(ctypes.Structure):
+    """dsgpu_frame: one frame of a batched develop (device pointers)."""
+    _fields_ = [
+        ("raw", ctypes.c_void_p),
+        ("pitch_elems", ctypes.c_size_t),
+        ("w", ctypes.c_int),
+        ("h", ctypes.c_int),
+        ("cfa", ctypes.c_uint8 * 4),
+        ("black", ctypes.c_float),
+        ("white", ctypes.c_float * 3),
+        ("mul", ctypes.c_float * 3),
+        ("h_param", ctypes.c_float),
+        ("out_rgb", ctypes.c_void_p),
+        ("out_clip", ctypes.c_void_p),
+    ]
 
 
 class SceneDesc(ctypes.Structure):
@@ -127,6 +145,12 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_scene_truth_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
             L.dsgpu_scene_render.argtypes = [vp, ctypes.POINTER(SceneDesc), vp, u]
             L.dsgpu_scene_render_window.argtypes = [vp, ctypes.POINTER(SceneDesc), i, i, i, i, vp, u]
+            L.dsgpu_rcd_nlm_batch.argtypes = [vp, ctypes.POINTER(Frame), i, i, i, u]
+            L.dsgpu_batch_frame_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_double), i]
+            L.dsgpu_autotune.argtypes = [vp, ctypes.POINTER(i), i, i, i]
+            L.dsgpu_autotune_get.argtypes = [vp, i, i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(i),
+                                             ctypes.POINTER(ctypes.c_double)]
+            L.dsgpu_autotune_set.argtypes = [vp, i, i, i, i, i]
             for name in EXPORTS:
                 if name not in ("dsgpu_strerror", "dsgpu_get_stream", "dsgpu_last_error", "dsgpu_launch_count"):
                     getattr(L, name).restype = i
@@ -156,7 +180,11 @@ class Context:
             raise DsgpuError(status, where, detail.decode() if detail else "")
 
     def set_stream(self, stream_ptr: int | None) -> None:
-        self.check(lib().dsgpu_set_stream(self.handle, ctypes.c_void_p(stream_ptr or 0)), "dsgpu_set_stream")
+        """Order the context's work on a CUDA stream handle: None = the
+        context's own stream; 0 (torch's default stream) = CUDA's legacy
+        default stream (handle 1), which orders with torch's work on it."""
+        handle = 0 if stream_ptr is None else (1 if stream_ptr == 0 else stream_ptr)
+        self.check(lib().dsgpu_set_stream(self.handle, ctypes.c_void_p(handle)), "dsgpu_set_stream")
 
     def synchronize(self) -> None:
         self.check(lib().dsgpu_synchronize(self.handle), "dsgpu_synchronize")

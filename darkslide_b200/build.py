@@ -34,6 +34,7 @@ UNITS = [
     ("k_cnn.cu", []),
     ("k_cnn_tc.cu", []),
     ("api.cu", []),
+    ("batch.cu", []),
     ("noalloc.cu", []),
 ]
 

@@ -28,6 +28,35 @@ struct ds_src_u16 {  // integer raw + the normalisation of decode.rs:303
   float white[3];
 };
 
+// One frame of a batched develop (u16 raw -> RCD -> NLM), as the batched
+// kernels read it from device memory. Tiles of all frames are numbered
+// consecutively: frame f owns RCD tiles [rcd_tile0, rcd_tile0 + rcd tiles)
+// and NLM tiles [nlm_tile0, nlm_tile0 + nlm_tiles_x * nlm_tiles_y * 3).
+struct ds_batch_frame {
+  ds_src_u16 src;
+  int w, h;
+  ds_pat pat;
+  float mul[3];
+  float sigma;      // NLM pre-scale of the frame's strength h
+  float* rgb;       // RCD output (scratch), w*h*3
+  float* clip;      // clip plane or null
+  float* out;       // NLM output, w*h*3
+  int rcd_shape;    // index into the RCD tile shapes (ds_rcd_batch_shape)
+  int rcd_tiles_x;
+  int rcd_tile0;
+  int nlm_tiles_x, nlm_tiles_y;
+  int nlm_tile0;
+};
+
+// batched kernels: one persistent launch each over all frames' tiles
+constexpr int DS_RCD_SHAPES = 5;
+void ds_rcd_batch_shape(int s, int* tile_w, int* tile_h);
+cudaError_t ds_launch_rcd_batch(cudaStream_t st, const ds_batch_frame* frames, int n, int total_tiles, int grid);
+cudaError_t ds_launch_nlm_batch(cudaStream_t st, const ds_batch_frame* frames, int n, int total_tiles, int search,
+                                int patch, int grid, unsigned* done, unsigned long long* stamps);
+cudaError_t ds_launch_stamp(cudaStream_t st, unsigned long long* t);
+float ds_nlm_sigma(float h_param, int patch);
+
 // kernel launchers (return cudaGetLastError() of the launch)
 cudaError_t ds_launch_normalize_u16(cudaStream_t st, const uint16_t* raw, int w, int h, size_t pitch, ds_pat pat,
                                     float black, const float white[3], float* out);

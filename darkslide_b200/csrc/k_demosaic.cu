@@ -132,12 +132,14 @@ __global__ void superpixel_kernel(const float* __restrict__ cfa, int w, int h, d
 // read c at +-3. So the tile loads a 10-sample halo (local stage regions:
 // m [0,52), b* and lpf [3,49), vh/pq [4,48), g [5,47), r43/b43 [7,45),
 // output [10,42)).
-constexpr int RT = 32;
-constexpr int RH = 10;
-constexpr int RS = RT + 2 * RH;  // 52
-constexpr int RA = RS * RS;      // one stage array
+constexpr int RT = 32;  // tile of the one-frame kernel: 32 x 32
+constexpr int RH = 10;  // halo
 constexpr int RCD_THREADS = 256;
-constexpr size_t RCD_SMEM = (size_t)8 * RA * sizeof(float) + RA;
+// shared bytes of a TX x TY tile: 8 stage arrays of (TX+20) x (TY+20) floats + the clip bytes
+__host__ __device__ constexpr size_t rcd_smem(int tx, int ty) {
+  return (size_t)8 * (tx + 2 * RH) * (ty + 2 * RH) * sizeof(float) + (size_t)(tx + 2 * RH) * (ty + 2 * RH);
+}
+constexpr size_t RCD_SMEM = rcd_smem(RT, RT);
 
 struct SrcF32 {
   ds_src_f32 s;
@@ -153,12 +155,17 @@ struct SrcU16 {
 
 __device__ __forceinline__ float sq(float v) { return v * v; }
 
-template <class Src>
-__global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
-                                                               float m1, float m2, float* __restrict__ out_rgb,
-                                                               float* __restrict__ out_clip) {
-  extern __shared__ float4 smem4[];
-  float* M = reinterpret_cast<float*>(smem4);  // data*mul (clamped-site load), not max(0)
+// One TXT x TYT output tile (tile_x, tile_y) of a W x H frame; smem holds
+// rcd_smem(TXT, TYT) bytes. The value at every site depends only on the
+// frame and the site's global coordinates, so any tiling gives the same
+// output bit for bit.
+template <class Src, int TXT, int TYT>
+__device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
+                                         float* __restrict__ out_rgb, float* __restrict__ out_clip, int tile_x,
+                                         int tile_y, float* smem) {
+  static_assert(TXT % 2 == 0 && TYT % 2 == 0, "tile sides must be even");
+  constexpr int RSX = TXT + 2 * RH, RSY = TYT + 2 * RH, RA = RSX * RSY;
+  float* M = smem;  // data*mul (clamped-site load), not max(0)
   float* BV = M + RA;   // bv, later g
   float* BH = BV + RA;  // bh, later r after 4.3
   float* BP = BH + RA;  // bp, later b after 4.3
@@ -172,12 +179,12 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
   float* B43 = BP;
 
   const int tid = threadIdx.x;
-  const int gx0 = blockIdx.x * RT - RH, gy0 = blockIdx.y * RT - RH;  // global site of local (0,0)
+  const int gx0 = tile_x * TXT - RH, gy0 = tile_y * TYT - RH;  // global site of local (0,0)
   const float eps = 1e-5f;
 
   // stage 0: load with clamped coordinates
   for (int i = tid; i < RA; i += RCD_THREADS) {
-    const int ly = i / RS, lx = i - ly * RS;
+    const int ly = i / RSX, lx = i - ly * RSX;
     const int gx = clampi(gx0 + lx, 0, W - 1), gy = clampi(gy0 + ly, 0, H - 1);
     const int col = pat.at(gx, gy);
     const float v = src.load(gx, gy, col);
@@ -187,13 +194,13 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
   __syncthreads();
 
   auto C = [&](int k) { return fmaxf(M[k], 0.0f); };  // demosaic.rs:154
-  const int w1 = RS, w2 = 2 * RS, w3 = 3 * RS, w4 = 4 * RS;
+  const int w1 = RSX, w2 = 2 * RSX, w3 = 3 * RSX, w4 = 4 * RSX;
 
-  // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, RS-3)
-  for (int i = tid; i < (RS - 6) * (RS - 6); i += RCD_THREADS) {
-    const int ly = 3 + i / (RS - 6), lx = 3 + i % (RS - 6);
+  // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, edge-3) of the staged region
+  for (int i = tid; i < (RSX - 6) * (RSY - 6); i += RCD_THREADS) {
+    const int ly = 3 + i / (RSX - 6), lx = 3 + i % (RSX - 6);
     const int gx = gx0 + lx, gy = gy0 + ly;
-    const int k = ly * RS + lx;
+    const int k = ly * RSX + lx;
     float bv = 0.f, bh = 0.f, bp = 0.f, bq = 0.f, lp = 0.f;
     if (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3) {
       const float c0 = C(k);
@@ -216,11 +223,11 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
   }
   __syncthreads();
 
-  // stage 2: vh (:173-184) and pq (:261-272) on [4, RS-4)
-  for (int i = tid; i < (RS - 8) * (RS - 8); i += RCD_THREADS) {
-    const int ly = 4 + i / (RS - 8), lx = 4 + i % (RS - 8);
+  // stage 2: vh (:173-184) and pq (:261-272) on [4, edge-4)
+  for (int i = tid; i < (RSX - 8) * (RSY - 8); i += RCD_THREADS) {
+    const int ly = 4 + i / (RSX - 8), lx = 4 + i % (RSX - 8);
     const int gx = gx0 + lx, gy = gy0 + ly;
-    const int k = ly * RS + lx;
+    const int k = ly * RSX + lx;
     float vh = 0.5f, pq = 0.5f;
     if (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4) {
       const float vs = fmaxf(BV[k - w1] + BV[k] + BV[k + w1], eps);
@@ -241,7 +248,7 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
     return fabsf(0.5f - central) < fabsf(0.5f - neigh) ? neigh : central;
   };
   auto mhc_at = [&](int k, int gx, int gy, float& o0, float& o1, float& o2) {  // ring sites only
-    auto p = [&](int dx, int dy) { return M[k + dy * RS + dx]; };
+    auto p = [&](int dx, int dy) { return M[k + dy * RSX + dx]; };
     mhc_formulas(p, pat.at(gx, gy), pat.at(gx + 1, gy), o0, o1, o2);
   };
 
@@ -256,19 +263,19 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
   };
   auto inner = [&](int gx, int gy) { return gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4; };
 
-  // stage 3: green (:203-214 init, :222-245 step 3) on [5, RS-5): 42 x 21
-  // sites of each class
-  constexpr int S3 = RS - 10, S3H = S3 / 2;
-  for (int i = tid; i < S3 * S3H; i += RCD_THREADS) {  // green sites: native sample
+  // stage 3: green (:203-214 init, :222-245 step 3) on [5, edge-5): (RSY-10)
+  // rows x (RSX-10)/2 sites of each class
+  constexpr int S3Y = RSY - 10, S3H = (RSX - 10) / 2;
+  for (int i = tid; i < S3Y * S3H; i += RCD_THREADS) {  // green sites: native sample
     const int ly = 5 + i / S3H, lx = col_start(ly, 5, true) + 2 * (i % S3H);
-    if (lx >= RS - 5) continue;
-    G[ly * RS + lx] = C(ly * RS + lx);
+    if (lx >= RSX - 5) continue;
+    G[ly * RSX + lx] = C(ly * RSX + lx);
   }
-  for (int i = tid; i < S3 * S3H; i += RCD_THREADS) {  // R/B sites
+  for (int i = tid; i < S3Y * S3H; i += RCD_THREADS) {  // R/B sites
     const int ly = 5 + i / S3H, lx = col_start(ly, 5, false) + 2 * (i % S3H);
-    if (lx >= RS - 5) continue;
+    if (lx >= RSX - 5) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
-    const int k = ly * RS + lx;
+    const int k = ly * RSX + lx;
     float g;
     if (inner(gx, gy)) {
       const float vd = disc(VH, k);
@@ -297,16 +304,16 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
   }
   __syncthreads();
 
-  // stage 4: R at B and B at R (:276-308) on [7, RS-7). The pre-pass clone
+  // stage 4: R at B and B at R (:276-308) on [7, edge-7). The pre-pass clone
   // read at the diagonal +-1/+-3 sites of an R (B) site holds native B (R)
   // samples, i.e. c. Interior green sites are never read (4.4 reads R/B
   // sites only); ring green sites keep their MHC values.
-  constexpr int S4 = RS - 14, S4H = S4 / 2;
-  for (int i = tid; i < S4 * S4H; i += RCD_THREADS) {  // R/B sites
+  constexpr int S4Y = RSY - 14, S4H = (RSX - 14) / 2;
+  for (int i = tid; i < S4Y * S4H; i += RCD_THREADS) {  // R/B sites
     const int ly = 7 + i / S4H, lx = col_start(ly, 7, false) + 2 * (i % S4H);
-    if (lx >= RS - 7) continue;
+    if (lx >= RSX - 7) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
-    const int k = ly * RS + lx;
+    const int k = ly * RSX + lx;
     const int col = pat.at(gx, gy);
     float r, b;
     if (inner(gx, gy)) {
@@ -334,12 +341,12 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
     R43[k] = r;
     B43[k] = b;
   }
-  for (int i = tid; i < S4 * S4H; i += RCD_THREADS) {  // green sites of the ring
+  for (int i = tid; i < S4Y * S4H; i += RCD_THREADS) {  // green sites of the ring
     const int ly = 7 + i / S4H, lx = col_start(ly, 7, true) + 2 * (i % S4H);
-    if (lx >= RS - 7) continue;
+    if (lx >= RSX - 7) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
     if (inner(gx, gy)) continue;
-    const int k = ly * RS + lx;
+    const int k = ly * RSX + lx;
     float o0, o1, o2;
     mhc_at(k, gx, gy, o0, o1, o2);
     R43[k] = o0;
@@ -348,19 +355,19 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
   __syncthreads();
 
   // stage 5: the tile's output; R and B at green sites (:310-341)
-  constexpr int TH = RT / 2;
+  constexpr int TH = TXT / 2;
   auto clip_at = [&](int k) {
     unsigned m = 0;
     for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) m |= CL[k + dy * RS + dx];
+      for (int dx = -1; dx <= 1; dx++) m |= CL[k + dy * RSX + dx];
     return m ? 1.0f : 0.0f;
   };
-  for (int i = tid; i < RT * TH; i += RCD_THREADS) {  // green sites
+  for (int i = tid; i < TYT * TH; i += RCD_THREADS) {  // green sites
     const int ly = RH + i / TH, lx = col_start(ly, RH, true) + 2 * (i % TH);
-    if (lx >= RH + RT) continue;
+    if (lx >= RH + TXT) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
     if (gx >= W || gy >= H) continue;
-    const int k = ly * RS + lx;
+    const int k = ly * RSX + lx;
     float r = R43[k], b = B43[k];
     const float g = G[k];
     if (inner(gx, gy)) {
@@ -387,17 +394,67 @@ __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, i
     o[2] = b;
     if (out_clip) out_clip[(size_t)gy * W + gx] = clip_at(k);
   }
-  for (int i = tid; i < RT * TH; i += RCD_THREADS) {  // R/B sites: values settled by stage 4
+  for (int i = tid; i < TYT * TH; i += RCD_THREADS) {  // R/B sites: values settled by stage 4
     const int ly = RH + i / TH, lx = col_start(ly, RH, false) + 2 * (i % TH);
-    if (lx >= RH + RT) continue;
+    if (lx >= RH + TXT) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
     if (gx >= W || gy >= H) continue;
-    const int k = ly * RS + lx;
+    const int k = ly * RSX + lx;
     float* o = out_rgb + ((size_t)gy * W + gx) * 3;
     o[0] = R43[k];
     o[1] = G[k];
     o[2] = B43[k];
     if (out_clip) out_clip[(size_t)gy * W + gx] = clip_at(k);
+  }
+}
+
+template <class Src>
+__global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
+                                                               float m1, float m2, float* __restrict__ out_rgb,
+                                                               float* __restrict__ out_clip) {
+  extern __shared__ float4 smem4[];
+  rcd_tile<Src, RT, RT>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, blockIdx.x, blockIdx.y,
+                        reinterpret_cast<float*>(smem4));
+}
+
+// Tile shapes of the batched kernel (w x h); all of them fit two CTAs per SM.
+constexpr int RCD_SHAPE_W[DS_RCD_SHAPES] = {32, 64, 48, 24, 16};
+constexpr int RCD_SHAPE_H[DS_RCD_SHAPES] = {32, 16, 24, 48, 64};
+constexpr size_t smax(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t RCD_BATCH_SMEM =
+    smax(smax(smax(rcd_smem(32, 32), rcd_smem(64, 16)), smax(rcd_smem(48, 24), rcd_smem(24, 48))), rcd_smem(16, 64));
+
+// index of the frame owning global tile t: the last f with tile0(f) <= t
+template <class Get>
+__device__ __forceinline__ int find_frame(int n, int t, Get tile0) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile0(mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Persistent RCD over the tiles of all frames; each frame uses its own tile shape.
+__global__ void __launch_bounds__(RCD_THREADS, 2) rcd_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
+                                                                   int total) {
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    const int f = find_frame(n, t, [&](int i) { return frames[i].rcd_tile0; });
+    const ds_batch_frame& F = frames[f];
+    const int local = t - F.rcd_tile0;
+    const int ty = local / F.rcd_tiles_x, tx = local - ty * F.rcd_tiles_x;
+    const SrcU16 src{F.src};
+    __syncthreads();  // the previous tile is done with shared memory
+    switch (F.rcd_shape) {
+      case 0: rcd_tile<SrcU16, 32, 32>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+      case 1: rcd_tile<SrcU16, 64, 16>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+      case 2: rcd_tile<SrcU16, 48, 24>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+      case 3: rcd_tile<SrcU16, 24, 48>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+      default: rcd_tile<SrcU16, 16, 64>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    }
   }
 }
 
@@ -456,4 +513,19 @@ cudaError_t ds_launch_rcd_f32(cudaStream_t st, ds_src_f32 src, int w, int h, ds_
 cudaError_t ds_launch_rcd_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, const float mul[3],
                               float* out_rgb, float* out_clip) {
   return launch_rcd(st, SrcU16{src}, w, h, pat, mul, out_rgb, out_clip);
+}
+
+void ds_rcd_batch_shape(int s, int* tile_w, int* tile_h) {
+  s = s < 0 || s >= DS_RCD_SHAPES ? 0 : s;
+  *tile_w = RCD_SHAPE_W[s];
+  *tile_h = RCD_SHAPE_H[s];
+}
+
+cudaError_t ds_launch_rcd_batch(cudaStream_t st, const ds_batch_frame* frames, int n, int total_tiles, int grid) {
+  if (n <= 0 || total_tiles <= 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(rcd_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)RCD_BATCH_SMEM);
+  if (e != cudaSuccess) return e;
+  rcd_batch_kernel<<<grid, RCD_THREADS, RCD_BATCH_SMEM, st>>>(frames, n, total_tiles);
+  return cudaGetLastError();
 }

@@ -78,29 +78,20 @@ size_t nlm_smem_bytes(int S, int P) {
   return (plane + hb) * sizeof(float);
 }
 
+// One 64 x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
+// image; smem holds nlm_smem_bytes(S, P) bytes.
 template <int P>
-__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
-                                                                  int S, float sigma, const float* __restrict__ h_dev,
-                                                                  float norm2_log2e,
-                                                                  const unsigned char* __restrict__ tile_flags,
-                                                                  float* __restrict__ out) {
-  // tile-list mode (the learned path's fallback): only flagged tiles run
-  if (tile_flags && !tile_flags[blockIdx.y * gridDim.x + blockIdx.x]) return;
-  if (h_dev) {  // strength computed on the device (enhance.rs:40 floor included)
-    const float hh = *h_dev;
-    sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
-  }
+__device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
+                                         float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
   constexpr int TY = HRW - 2 * P;
   constexpr int DW = SEG + 2 * P;  // differences per phase-A segment
   constexpr int RB = (TY + 3) / 4; // phase-B rows per thread (a quarter of the tile)
   constexpr int PP = nlm_pitch(P);
   const NlmGeom g = nlm_geom(S, P);
-  extern __shared__ float4 smem4[];
-  float* PL = reinterpret_cast<float*>(smem4);  // scaled plane, pitch PP
-  float* HB = PL + PP * g.PHA;                  // 4 offsets x HBR rows x HP
+  float* PL = smem;             // scaled plane, pitch PP
+  float* HB = PL + PP * g.PHA;  // 4 offsets x HBR rows x HP
 
-  const int ch = blockIdx.z;
-  const int X0 = blockIdx.x * TX, Y0 = blockIdx.y * TY;
+  const int X0 = tile_x * TX, Y0 = tile_y * TY;
   const int tid = threadIdx.x;
   const int ox0 = X0 - g.R, oy0 = Y0 - g.R;  // global site of plane (0,0)
 
@@ -229,6 +220,71 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* _
 }
 
 template <int P>
+__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
+                                                                  int S, float sigma, const float* __restrict__ h_dev,
+                                                                  float norm2_log2e,
+                                                                  const unsigned char* __restrict__ tile_flags,
+                                                                  float* __restrict__ out) {
+  // tile-list mode (the learned path's fallback): only flagged tiles run
+  if (tile_flags && !tile_flags[blockIdx.y * gridDim.x + blockIdx.x]) return;
+  if (h_dev) {  // strength computed on the device (enhance.rs:40 floor included)
+    const float hh = *h_dev;
+    sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
+  }
+  extern __shared__ float4 smem4[];
+  nlm_tile<P>(in, W, H, C, S, sigma, out, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float*>(smem4));
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__global__ void stamp_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
+
+// Persistent NLM over the tiles of all frames (3 channels each). When the
+// last tile of frame f is done, stamps[f] = the device clock (ns), so the
+// host can report per-frame completion times.
+template <int P>
+__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
+                                                                   int total, int S, unsigned* __restrict__ done,
+                                                                   unsigned long long* __restrict__ stamps) {
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    int lo = 0, hi = n - 1;  // the last frame whose first tile is <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (frames[mid].nlm_tile0 <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const ds_batch_frame& F = frames[lo];
+    const int per = F.nlm_tiles_x * F.nlm_tiles_y;
+    const int local = t - F.nlm_tile0;
+    const int ch = local / per, r = local - ch * per;
+    const int ty = r / F.nlm_tiles_x, tx = r - ty * F.nlm_tiles_x;
+    __syncthreads();  // the previous tile is done with shared memory
+    nlm_tile<P>(F.rgb, F.w, F.h, 3, S, F.sigma, F.out, tx, ty, ch, smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(&done[lo], 1u) + 1u == (unsigned)(3 * per)) stamps[lo] = globaltimer_ns();
+    }
+  }
+}
+
+template <int P>
+cudaError_t launch_nlm_batch_p(cudaStream_t st, const ds_batch_frame* frames, int n, int total, int S, int grid,
+                               unsigned* done, unsigned long long* stamps) {
+  const size_t smem = nlm_smem_bytes(S, P);
+  cudaError_t e = cudaFuncSetAttribute(nlm_batch_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  nlm_batch_kernel<P><<<grid, NLM_THREADS, smem, st>>>(frames, n, total, S, done, stamps);
+  return cudaGetLastError();
+}
+
+template <int P>
 cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float sigma,
                          const float* h_dev, float norm2_log2e, const unsigned char* flags, float* out) {
   constexpr int TY = HRW - 2 * P;
@@ -302,4 +358,34 @@ cudaError_t ds_launch_nlm_dev_h(cudaStream_t st, const float* in, int w, int h, 
   if (search == 0)
     return cudaMemcpyAsync(out, in, (size_t)w * h * channels * sizeof(float), cudaMemcpyDeviceToDevice, st);
   return dispatch_nlm(st, in, w, h, channels, search, patch, 1.0f, h_dev, out);
+}
+
+// NLM pre-scale of strength h (the sigma ds_launch_nlm computes)
+float ds_nlm_sigma(float h_param, int patch) {
+  const float h2 = fmaxf(h_param * h_param, 1e-12f);
+  const float norm = patch == 0 ? 1.0f : 1.0f / (float)(2 * patch + 1);
+  const double sig2 = (double)norm * (double)norm / (double)h2 * 1.4426950408889634;
+  return (float)sqrt(sig2);
+}
+
+cudaError_t ds_launch_stamp(cudaStream_t st, unsigned long long* t) {
+  stamp_kernel<<<1, 1, 0, st>>>(t);
+  return cudaGetLastError();
+}
+
+cudaError_t ds_launch_nlm_batch(cudaStream_t st, const ds_batch_frame* frames, int n, int total_tiles, int search,
+                                int patch, int grid, unsigned* done, unsigned long long* stamps) {
+  if (n <= 0 || total_tiles <= 0) return cudaSuccess;
+  if (search <= 0 || search > DSGPU_NLM_MAX_SEARCH) return cudaErrorInvalidValue;
+  switch (patch) {
+    case 0: return launch_nlm_batch_p<0>(st, frames, n, total_tiles, search, grid, done, stamps);
+    case 1: return launch_nlm_batch_p<1>(st, frames, n, total_tiles, search, grid, done, stamps);
+    case 2: return launch_nlm_batch_p<2>(st, frames, n, total_tiles, search, grid, done, stamps);
+    case 3: return launch_nlm_batch_p<3>(st, frames, n, total_tiles, search, grid, done, stamps);
+    case 4: return launch_nlm_batch_p<4>(st, frames, n, total_tiles, search, grid, done, stamps);
+    case 5: return launch_nlm_batch_p<5>(st, frames, n, total_tiles, search, grid, done, stamps);
+    case 6: return launch_nlm_batch_p<6>(st, frames, n, total_tiles, search, grid, done, stamps);
+    case 7: return launch_nlm_batch_p<7>(st, frames, n, total_tiles, search, grid, done, stamps);
+    default: return cudaErrorInvalidValue;
+  }
 }

@@ -190,6 +190,50 @@ int dsgpu_develop_u16_noalloc(void* cuda_stream, const uint16_t* raw, int w, int
                               float h_param, int search, int patch, float* out_rgb, float* out_clip,
                               unsigned flags);
 
+/* ------------------------------------------------------------ batched develop
+ * The survey's dsgpu_rcd_nlm_batch: many frames of different sizes, CFA
+ * layouts, levels and strengths through dsgpu_develop_u16's path in one
+ * CUDA graph launch that holds one persistent RCD kernel and one persistent
+ * NLM kernel over the tiles of all frames (the reference develops one frame
+ * per call, pipeline/mod.rs:172-252). Each frame's output equals
+ * dsgpu_develop_u16's on the same frame bit for bit. */
+typedef struct dsgpu_frame {
+  const uint16_t* raw;  /* device, h rows of pitch_elems */
+  size_t pitch_elems;
+  int w, h;             /* 16 <= w, h <= DSGPU_MAX_DIM */
+  uint8_t cfa[4];
+  float black;
+  float white[3];
+  float mul[3];
+  float h_param;        /* NLM strength of this frame */
+  float* out_rgb;       /* device, w*h*3 */
+  float* out_clip;      /* device, w*h, or NULL */
+} dsgpu_frame;
+#define DSGPU_BATCH_MAX 256
+/* Device pointers only (DSGPU_HOST -> DSGPU_ERR_UNSUPPORTED); search >= 1.
+ * The demosaiced intermediates of all frames live in context scratch. The
+ * graph is captured on the first call for a batch layout (frame sizes, tile
+ * shapes, search, patch) and replayed by later calls with the same layout;
+ * frame pointers and levels may change between calls. RCD tile shapes come
+ * from the context's autotune table (dsgpu_autotune), else 32 x 32. */
+int dsgpu_rcd_nlm_batch(dsgpu_ctx* ctx, const dsgpu_frame* frames, int n, int search, int patch, unsigned flags);
+/* Completion time of each frame of the last batch, ms after the batch started
+ * on the device (measured with the device clock; waits for the batch). */
+int dsgpu_batch_frame_ms(dsgpu_ctx* ctx, double* frame_ms, int n);
+/* Autotuner: for each size class (w, h) = (sizes[2i], sizes[2i+1]), time the
+ * batched RCD kernel with every tile shape and the batched NLM kernel with 1
+ * and 2 CTAs per SM on a synthetic frame of that size, and keep the fastest
+ * in the context's table. */
+int dsgpu_autotune(dsgpu_ctx* ctx, const int* sizes, int n_sizes, int search, int patch);
+/* The table entry used for a w x h frame (the exact class, else the class
+ * nearest in pixel count, else the defaults 32 x 32 and 2 CTAs per SM);
+ * rcd_ms (may be NULL) receives the tuned RCD time per shape index (5) for
+ * an exact class, else -1. */
+int dsgpu_autotune_get(dsgpu_ctx* ctx, int w, int h, int* rcd_tile_w, int* rcd_tile_h, int* nlm_ctas_per_sm,
+                       double* rcd_ms);
+/* Set a table entry by hand (a table saved by a caller, or a test). */
+int dsgpu_autotune_set(dsgpu_ctx* ctx, int w, int h, int rcd_tile_w, int rcd_tile_h, int nlm_ctas_per_sm);
+
 /* ------------------------------------------------------------ learned path
  * A residual CNN standing in for nlm(): 8 conv3x3 layers (4 -> 48 -> ... ->
  * 48 -> 3, ReLU), input = RGB plus a constant map of the NLM strength h,
