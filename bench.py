@@ -14,6 +14,11 @@ plain NLM's, else the plain path is. The working set (48 MB raw, 288 MB
 demosaiced, 288 MB output, 2.3 GB of CNN activations) is larger than the
 126 MB L2, so no flush is needed between steps.
 
+The line also carries "batched": 64 mosaics of four camera sizes, four CFA
+layouts and two bit depths through dsgpu_rcd_nlm_batch (one CUDA graph launch
+per batch), after the tile autotuner, with aggregate Mpix/s and per-frame
+p50/p99 completion times (--no-batched skips it).
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0). Under torchrun every rank develops its own
@@ -210,6 +215,80 @@ def psnr(a, b) -> float:
     return 10.0 * float(np.log10(1.0 / max(mse, 1e-30)))
 
 
+BATCH_SIZES = [(4000, 3000), (6000, 4000), (8256, 5504), (9504, 6336)]
+BATCH_FRAMES = 64
+
+
+def run_batched(ctx, dev, steps: int, warmup: int, seed: int = 4) -> dict:
+    """The batched workload: 64 mosaics with sizes drawn from the seed among
+    4000x3000, 6000x4000, 8256x5504 and 9504x6336, CFA among the four Bayer
+    layouts, 12 or 14 bits, read noise U(2, 12) DN, gain U(0.25, 1) e/DN;
+    per-frame h = 1.5 x its noise sigma at mid grey; patch 7x7, search 21x21.
+    The tile autotuner runs first on the four size classes; each step is one
+    dsgpu_rcd_nlm_batch call (one CUDA graph launch: a persistent RCD and a
+    persistent NLM kernel over all frames), inputs resident in HBM."""
+    import torch
+
+    import darkslide_b200 as ds
+
+    rng = np.random.default_rng(seed)
+    pats = [ds.RGGB, ds.BGGR, ds.GRBG, ds.GBRG]
+    stream = torch.cuda.Stream(dev)
+    frames = []
+    with torch.cuda.stream(stream):
+        for k in range(BATCH_FRAMES):
+            w, h = BATCH_SIZES[int(rng.integers(len(BATCH_SIZES)))]
+            pat = pats[int(rng.integers(4))]
+            bits = 12 if rng.random() < 0.5 else 14
+            black, white = (256, 4095) if bits == 12 else (512, 16383)
+            sc = ds.Scene(seed=1000 + k, w=w, h=h, pattern=pat, black=black, white=white,
+                          gain=float(rng.uniform(0.25, 1.0)), read_sigma=float(rng.uniform(2.0, 12.0)))
+            raw = sc.render(dev, ctx=ctx)
+            frames.append(ds.BatchFrame(raw=raw, pattern=pat, black=black, white=[white] * 3,
+                                        mul=[2.0, 1.0, 1.0 / 0.7], h_param=1.5 * sc.sigma_norm(),
+                                        out=torch.empty((h, w, 3), dtype=torch.float32, device=dev)))
+    stream.synchronize()
+    px = sum(f.raw.shape[0] * f.raw.shape[1] for f in frames)
+    t0 = time.perf_counter()
+    ds.autotune(BATCH_SIZES, SEARCH, PATCH, ctx=ctx)
+    tune_s = time.perf_counter() - t0
+    n0 = ctx.launch_count()
+    lat = []
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, warmup)):
+            ds.develop_batch(frames, SEARCH, PATCH, ctx=ctx)
+        stream.synchronize()
+        n0 = ctx.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms_total = 0.0
+        for _ in range(steps):
+            e0.record(stream)
+            ds.develop_batch(frames, SEARCH, PATCH, ctx=ctx, sync=False)
+            e1.record(stream)
+            e1.synchronize()
+            ms_total += e0.elapsed_time(e1)
+            lat.extend(ds.batch_frame_ms(len(frames), ctx=ctx).tolist())
+    launches = ctx.launch_count() - n0
+    table = {f"{w}x{h}": ds.autotune_get(w, h, ctx=ctx) for w, h in BATCH_SIZES}
+    counts = {f"{w}x{h}": sum(1 for f in frames if f.raw.shape == (h, w)) for w, h in BATCH_SIZES}
+    del frames
+    torch.cuda.empty_cache()
+    ms = ms_total / steps
+    return {
+        "workload": "64 mosaics, sizes from {4000x3000, 6000x4000, 8256x5504, 9504x6336}, CFA from the 4 Bayer "
+                    "layouts, 12/14-bit, read noise U(2,12) DN, gain U(0.25,1); RCD + NLM 7x7/21x21 per frame",
+        "frames": BATCH_FRAMES, "frames_per_size": counts, "mpix_per_batch": px / 1e6,
+        "value": px / (ms * 1e-3) / 1e6, "unit": "Mpix/s", "ms_per_batch": ms, "steps": steps,
+        "frame_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                             "max": float(np.max(lat)),
+                             "definition": "device clock from the batch's start to the end of the frame's last "
+                                           "NLM tile, over all frames of the timed batches"},
+        "launch": "one CUDA graph per batch: descriptor upload, start stamp, persistent RCD kernel, persistent "
+                  "NLM kernel over all frames' tiles",
+        "gpu_launches_per_batch": launches / steps, "autotune_s": tune_s, "autotune": table,
+    }
+
+
 def run_ours(args):
     import ctypes
 
@@ -361,6 +440,15 @@ def run_ours(args):
     meets = loss_db <= QUALITY_BOUND_DB
     tiles = -(-W // 64) * -(-H // (64 - 2 * PATCH))
 
+    del rgb
+    batched = None
+    if not args.no_batched:
+        out = None
+        torch.cuda.empty_cache()
+        batched = run_batched(ctx, dev, steps=max(2, min(args.steps, 3)), warmup=1)
+        if ws > 1:  # the whole job: every rank developed its own batch
+            batched["value"] = max_over_ranks(-batched["value"]) * -ws
+
     if rank == 0:
         peaks = {}
         try:
@@ -449,6 +537,8 @@ def run_ours(args):
         }
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -465,6 +555,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-frame batched workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
