@@ -236,15 +236,16 @@ def box_blur(p: Plane, r: int, ctx: Context | None = None) -> Plane:
     return Plane(p.w, p.h, out)
 
 
-def nlm(p, h_param: float, search: int, patch: int, ctx: Context | None = None):
-    """enhance.rs:36-72. ``p`` is a Plane, or an Image3 denoised per channel."""
+def nlm(p, h_param: float, search: int, patch: int, ctx: Context | None = None, fp16_staging: bool = False):
+    """enhance.rs:36-72. ``p`` is a Plane, or an Image3 denoised per channel.
+    ``fp16_staging``: the precision variant (DSGPU_FP16_STAGING)."""
     chans = 3 if isinstance(p, Image3) else 1
     c = _Call(p.data, ctx)
     src, pi = c.inp(p.data, np.float32)
     shape = (p.h, p.w, 3) if chans == 3 else (p.h, p.w)
     out, po = c.out(shape)
     c.ctx.check(lib().dsgpu_nlm(c.ctx.handle, pi, p.w, p.h, chans, float(h_param), int(search), int(patch), po,
-                                c.flags), "dsgpu_nlm")
+                                c.flags | (_lib.DSGPU_FP16_STAGING if fp16_staging else 0)), "dsgpu_nlm")
     return Image3(p.w, p.h, out) if chans == 3 else Plane(p.w, p.h, out)
 
 
@@ -327,9 +328,10 @@ def autotune_set(w: int, h: int, rcd_tile, nlm_ctas_per_sm: int, ctx: Context | 
 
 
 def develop_u16(raw, pattern: CfaPattern, black: float, white, mul, h_param: float, search: int, patch: int,
-                with_clip: bool = False, ctx: Context | None = None):
+                with_clip: bool = False, ctx: Context | None = None, fp16_staging: bool = False):
     """u16 raw -> normalise -> RCD -> per-channel NLM in one device pass.
-    Returns the denoised Image3 (and the clip Plane when ``with_clip``)."""
+    Returns the denoised Image3 (and the clip Plane when ``with_clip``).
+    ``fp16_staging``: NLM's precision variant (DSGPU_FP16_STAGING)."""
     c = _Call(raw, ctx)
     h, w = raw.shape
     src, p = c.inp(raw, np.uint16)
@@ -337,7 +339,8 @@ def develop_u16(raw, pattern: CfaPattern, black: float, white, mul, h_param: flo
     clip, pc = c.out((h, w)) if with_clip else (None, ctypes.c_void_p(0))
     pat, wh, m = pattern.codes(), _f3(white), _f3(mul)
     c.ctx.check(lib().dsgpu_develop_u16(c.ctx.handle, p, w, h, w, _vp(pat), float(black), _vp(wh), _vp(m),
-                                        float(h_param), int(search), int(patch), pr, pc, c.flags),
+                                        float(h_param), int(search), int(patch), pr, pc,
+                                        c.flags | (_lib.DSGPU_FP16_STAGING if fp16_staging else 0)),
                 "dsgpu_develop_u16")
     img = Image3(w, h, rgb)
     return (img, Plane(w, h, clip)) if with_clip else img

@@ -23,6 +23,7 @@ DSGPU_ERR_TIMEOUT = -7
 DSGPU_ERR_UNSUPPORTED = -8
 DSGPU_HOST = 1
 DSGPU_ASYNC = 2
+DSGPU_FP16_STAGING = 4
 DSGPU_QUALITY_DRAFT = 0
 DSGPU_QUALITY_FULL = 1
 DSGPU_STAGE_DEMOSAIC = 0

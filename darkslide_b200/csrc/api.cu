@@ -171,7 +171,7 @@ int nlm_args_ok(int channels, int search, int patch) {
 // NLM on device buffers; a negative search radius yields an empty offset set
 // and therefore 0 / max(0, 1e-12) = 0 (enhance.rs:41, :71).
 int run_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h_param, int search, int patch,
-            float* out) {
+            float* out, unsigned flags = 0) {
   const size_t n = (size_t)w * h * channels;
   if (n == 0) return DSGPU_OK;
   StageMark mark(ctx, DSGPU_STAGE_NLM);
@@ -179,7 +179,8 @@ int run_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h
     DS_TRY(cudaMemsetAsync(out, 0, n * sizeof(float), ctx->stream));
     return DSGPU_OK;
   }
-  DS_TRY(ds_launch_nlm(ctx->stream, in, w, h, channels, h_param, search, patch, out));
+  DS_TRY(ds_launch_nlm(ctx->stream, in, w, h, channels, h_param, search, patch, out,
+                       (flags & DSGPU_FP16_STAGING) != 0));
   ctx->launches += 1;
   return DSGPU_OK;
 }
@@ -478,7 +479,7 @@ int dsgpu_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float
   void* dout;
   DS_CHECK(stage_in(ctx, flags, S_IN, in, n * sizeof(float), &din));
   DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, n * sizeof(float), &dout));
-  DS_CHECK(run_nlm(ctx, (const float*)din, w, h, channels, h_param, search, patch, (float*)dout));
+  DS_CHECK(run_nlm(ctx, (const float*)din, w, h, channels, h_param, search, patch, (float*)dout, flags));
   return finish(ctx, flags, out, dout, n * sizeof(float));
 }
 
@@ -512,7 +513,7 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
     DS_TRY(ds_launch_rcd_u16(ctx->stream, src, w, h, pat, mul, (float*)mid, (float*)dclip));
     ctx->launches += 1;
   }
-  DS_CHECK(run_nlm(ctx, (const float*)mid, w, h, 3, h_param, search, patch, (float*)drgb));
+  DS_CHECK(run_nlm(ctx, (const float*)mid, w, h, 3, h_param, search, patch, (float*)drgb, flags));
   return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));
 }
 

@@ -70,8 +70,10 @@ cudaError_t ds_launch_rcd_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_
 cudaError_t ds_launch_superpixel(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, const float mul[3],
                                  float* out_rgb, float* out_clip);
 cudaError_t ds_launch_box_blur(cudaStream_t st, const float* in, int w, int h, int r, float* tmp, float* out);
+// fp16_staging: the precision variant (plane staged in half precision,
+// sums in FP32 with a compensated weight sum); see k_nlm.cu
 cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int channels, float h_param, int search,
-                          int patch, float* out);
+                          int patch, float* out, bool fp16_staging = false);
 cudaError_t ds_launch_nlm_dev_h(cudaStream_t st, const float* in, int w, int h, int channels, const float* h_dev,
                                 int search, int patch, float* out);
 void ds_nlm_tile_grid(int w, int h, int patch, int* tiles_x, int* tiles_y, int* tile_w, int* tile_h);

@@ -31,6 +31,8 @@
 // shifted sample p_clamped(x+o) is a plain shared read; the reference's box
 // filter clamps the DIFFERENCE plane, so H rows are clamped per row and, in
 // tiles whose patch window leaves the image, columns per element.
+#include <cuda_fp16.h>
+
 #include <type_traits>
 
 #include "internal.cuh"
@@ -71,36 +73,55 @@ __host__ __device__ inline NlmGeom nlm_geom(int S, int P) {
   return g;
 }
 
-size_t nlm_smem_bytes(int S, int P) {
+// plane bytes (f32, or f16 when staged in half precision), rounded to 16
+size_t nlm_plane_bytes(int S, int P, bool f16) {
   const NlmGeom g = nlm_geom(S, P);
-  size_t plane = (size_t)nlm_pitch(P) * g.PHA;
-  size_t hb = (size_t)4 * HBR * HP;
-  return (plane + hb) * sizeof(float);
+  return ((size_t)nlm_pitch(P) * g.PHA * (f16 ? 2 : 4) + 15) / 16 * 16;
 }
 
+size_t nlm_smem_bytes(int S, int P, bool f16 = false) {
+  return nlm_plane_bytes(S, P, f16) + (size_t)4 * HBR * HP * sizeof(float);
+}
+
+__device__ __forceinline__ float ldp(const float* p) { return *p; }
+__device__ __forceinline__ float ldp(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ void stp(float* p, float v) { *p = v; }
+__device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v); }
+
 // One 64 x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
-// image; smem holds nlm_smem_bytes(S, P) bytes.
-template <int P>
+// image; smem holds nlm_smem_bytes(S, P, F16) bytes.
+// F16 (the precision variant): the pre-scaled plane is staged in half
+// precision, centred on the tile's centre sample (NLM weights depend only on
+// differences, so the offset costs nothing there and keeps the half-precision
+// error of the staged values small; it is added back to the result), while
+// distances, weights and sums stay in FP32 and the weight sum (the
+// normalisation) is accumulated with Kahan compensation.
+template <int P, bool F16 = false>
 __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
                                          float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
+  using T = typename std::conditional<F16, __half, float>::type;
   constexpr int TY = HRW - 2 * P;
   constexpr int DW = SEG + 2 * P;  // differences per phase-A segment
   constexpr int RB = (TY + 3) / 4; // phase-B rows per thread (a quarter of the tile)
   constexpr int PP = nlm_pitch(P);
   const NlmGeom g = nlm_geom(S, P);
-  float* PL = smem;             // scaled plane, pitch PP
-  float* HB = PL + PP * g.PHA;  // 4 offsets x HBR rows x HP
+  T* PL = reinterpret_cast<T*>(smem);  // scaled plane, pitch PP
+  float* HB = reinterpret_cast<float*>(reinterpret_cast<char*>(smem) +
+                                       ((size_t)PP * g.PHA * sizeof(T) + 15) / 16 * 16);  // 4 offsets x HBR rows x HP
 
   const int X0 = tile_x * TX, Y0 = tile_y * TY;
   const int tid = threadIdx.x;
   const int ox0 = X0 - g.R, oy0 = Y0 - g.R;  // global site of plane (0,0)
 
+  float off = 0.f;  // F16: the tile's centre sample
+  if (F16) off = in[((size_t)clampi(Y0 + TY / 2, 0, H - 1) * W + clampi(X0 + TX / 2, 0, W - 1)) * C + ch];
   for (int i = tid; i < g.PW * g.PH; i += NLM_THREADS) {
     const int ly = i / g.PW, lx = i - ly * g.PW;
     const int gx = clampi(ox0 + lx, 0, W - 1), gy = clampi(oy0 + ly, 0, H - 1);
-    PL[ly * PP + lx] = in[((size_t)gy * W + gx) * C + ch] * sigma;
+    const float v = in[((size_t)gy * W + gx) * C + ch];
+    stp(&PL[ly * PP + lx], F16 ? (v - off) * sigma : v * sigma);
   }
-  for (int i = tid; i < (g.PHA - g.PH) * PP; i += NLM_THREADS) PL[g.PH * PP + i] = 0.f;
+  for (int i = tid; i < (g.PHA - g.PH) * PP; i += NLM_THREADS) stp(&PL[g.PH * PP + i], 0.f);
 
   // ---- phase-A role: H row `arow` (tile row arow - P), segment at ax0
   const int arow = tid & (HRW - 1);
@@ -117,13 +138,14 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
 #pragma unroll
   for (int k = 0; k < DW; k++) {
     const int col = xin ? acol0 + k : clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
-    pv[k] = PL[aprow * PP + col];
+    pv[k] = ldp(&PL[aprow * PP + col]);
   }
-  float a[RB], s[RB];
+  float a[RB], s[RB], cs[F16 ? RB : 1];  // cs: Kahan compensation of s (F16)
 #pragma unroll
   for (int r = 0; r < RB; r++) {
     a[r] = 0.f;
     s[r] = 0.f;
+    if (F16) cs[r] = 0.f;
   }
 
   // One 2x2 block of offsets {dx0, dx0+1} x {dy0, dy0+NJ-1}.
@@ -133,12 +155,12 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
     // vertical sum is the ex2 argument itself
 #pragma unroll
     for (int j = 0; j < NJ; j++) {
-      const float* qrow = PL + (aprow + dy0 + j) * PP + dx0;
+      const T* qrow = PL + (aprow + dy0 + j) * PP + dx0;
       float d0[DW], d1[DW];
       if (xin) {
         float q[DW + 1];
 #pragma unroll
-        for (int k = 0; k <= DW; k++) q[k] = qrow[acol0 + k];
+        for (int k = 0; k <= DW; k++) q[k] = ldp(&qrow[acol0 + k]);
 #pragma unroll
         for (int k = 0; k < DW; k++) {
           d0[k] = pv[k] - q[k];
@@ -148,8 +170,8 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
 #pragma unroll
         for (int k = 0; k < DW; k++) {
           const int col = clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
-          d0[k] = pv[k] - qrow[col];
-          d1[k] = pv[k] - qrow[col + 1];
+          d0[k] = pv[k] - ldp(&qrow[col]);
+          d1[k] = pv[k] - ldp(&qrow[col + 1]);
         }
       }
       float h0 = 0.f, h1 = 0.f;
@@ -177,10 +199,10 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
 #pragma unroll
     for (int i = 0; i < 2; i++) {
       if (dx0 + i <= S) {  // false only for the dx tail of an odd search width
-        const float* qc = PL + (brow0 + g.R + dy0) * PP + bcol + g.R + dx0 + i;
+        const T* qc = PL + (brow0 + g.R + dy0) * PP + bcol + g.R + dx0 + i;
         float qv[RB + NJ - 1];
 #pragma unroll
-        for (int r = 0; r < RB + NJ - 1; r++) qv[r] = qc[r * PP];
+        for (int r = 0; r < RB + NJ - 1; r++) qv[r] = ldp(&qc[r * PP]);
 #pragma unroll
         for (int j = 0; j < NJ; j++) {
           const float* hc = HB + (j * 2 + i) * (HBR * HP) + brow0 * HP + bcol;
@@ -195,7 +217,14 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
             if (r > 0) v = v + hv[r + 2 * P] - hv[r - 1];
             const float wgt = ex2(v);
             a[r] = fmaf(wgt, qv[r + j], a[r]);
-            s[r] += wgt;
+            if (F16) {  // Kahan: s[r] + cs[r] carries the sum of weights
+              const float y = wgt - cs[r];
+              const float t = s[r] + y;
+              cs[r] = (t - s[r]) - y;
+              s[r] = t;
+            } else {
+              s[r] += wgt;
+            }
           }
         }
       }
@@ -214,12 +243,14 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
   for (int r = 0; r < RB; r++) {
     const int y = brow0 + r;
     const int gx = X0 + bcol, gy = Y0 + y;
-    if (y < TY && gx < W && gy < H)
-      out[((size_t)gy * W + gx) * C + ch] = __fdiv_rn(a[r] * inv_sigma, fmaxf(s[r], 1e-12f));
+    if (y < TY && gx < W && gy < H) {
+      const float o = __fdiv_rn(a[r] * inv_sigma, fmaxf(F16 ? s[r] - cs[r] : s[r], 1e-12f));
+      out[((size_t)gy * W + gx) * C + ch] = F16 ? o + off : o;
+    }
   }
 }
 
-template <int P>
+template <int P, bool F16>
 __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
                                                                   int S, float sigma, const float* __restrict__ h_dev,
                                                                   float norm2_log2e,
@@ -232,7 +263,7 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* _
     sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
   }
   extern __shared__ float4 smem4[];
-  nlm_tile<P>(in, W, H, C, S, sigma, out, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float*>(smem4));
+  nlm_tile<P, F16>(in, W, H, C, S, sigma, out, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float*>(smem4));
 }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -284,15 +315,16 @@ cudaError_t launch_nlm_batch_p(cudaStream_t st, const ds_batch_frame* frames, in
   return cudaGetLastError();
 }
 
-template <int P>
+template <int P, bool F16>
 cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float sigma,
                          const float* h_dev, float norm2_log2e, const unsigned char* flags, float* out) {
   constexpr int TY = HRW - 2 * P;
-  const size_t smem = nlm_smem_bytes(S, P);
-  cudaError_t e = cudaFuncSetAttribute(nlm_tile_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = nlm_smem_bytes(S, P, F16);
+  cudaError_t e =
+      cudaFuncSetAttribute(nlm_tile_kernel<P, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY, C);
-  nlm_tile_kernel<P><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags, out);
+  nlm_tile_kernel<P, F16><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags, out);
   return cudaGetLastError();
 }
 
@@ -300,27 +332,34 @@ cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, 
 
 namespace {
 
-cudaError_t dispatch_nlm(cudaStream_t st, const float* in, int w, int h, int C, int S, int P, float sigma,
-                         const float* h_dev, float* out, const unsigned char* flags = nullptr) {
+template <bool F16>
+cudaError_t dispatch_nlm_t(cudaStream_t st, const float* in, int w, int h, int C, int S, int P, float sigma,
+                           const float* h_dev, float* out, const unsigned char* flags) {
   const float norm = P == 0 ? 1.0f : 1.0f / (float)(2 * P + 1);
   const float n2l = norm * norm * 1.4426950408889634f;
   switch (P) {
-    case 0: return launch_nlm_p<0>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 1: return launch_nlm_p<1>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 2: return launch_nlm_p<2>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 3: return launch_nlm_p<3>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 4: return launch_nlm_p<4>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 5: return launch_nlm_p<5>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 6: return launch_nlm_p<6>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 7: return launch_nlm_p<7>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 0: return launch_nlm_p<0, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 1: return launch_nlm_p<1, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 2: return launch_nlm_p<2, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 3: return launch_nlm_p<3, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 4: return launch_nlm_p<4, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 5: return launch_nlm_p<5, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 6: return launch_nlm_p<6, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 7: return launch_nlm_p<7, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t dispatch_nlm(cudaStream_t st, const float* in, int w, int h, int C, int S, int P, float sigma,
+                         const float* h_dev, float* out, const unsigned char* flags = nullptr, bool f16 = false) {
+  return f16 ? dispatch_nlm_t<true>(st, in, w, h, C, S, P, sigma, h_dev, out, flags)
+             : dispatch_nlm_t<false>(st, in, w, h, C, S, P, sigma, h_dev, out, flags);
 }
 
 }  // namespace
 
 cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int channels, float h_param, int search,
-                          int patch, float* out) {
+                          int patch, float* out, bool fp16_staging) {
   if (search == 0) {  // only the centre offset: weight 1, out = p exactly (enhance.rs:41-71)
     return cudaMemcpyAsync(out, in, (size_t)w * h * channels * sizeof(float), cudaMemcpyDeviceToDevice, st);
   }
@@ -330,7 +369,7 @@ cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int ch
   const float h2 = fmaxf(h_param * h_param, 1e-12f);
   const float norm = patch == 0 ? 1.0f : 1.0f / (float)(2 * patch + 1);
   const double sig2 = (double)norm * (double)norm / (double)h2 * 1.4426950408889634;
-  return dispatch_nlm(st, in, w, h, channels, search, patch, (float)sqrt(sig2), nullptr, out);
+  return dispatch_nlm(st, in, w, h, channels, search, patch, (float)sqrt(sig2), nullptr, out, nullptr, fp16_staging);
 }
 
 // NLM tile geometry (the fallback's flag grid): tiles_x x tiles_y of 64 x (64 - 2P)

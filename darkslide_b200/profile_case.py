@@ -29,7 +29,9 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--search", type=int, default=10)
     ap.add_argument("--patch", type=int, default=3)
+    ap.add_argument("--fp16", action="store_true", help="NLM's FP16-staging precision variant")
     a = ap.parse_args()
+    xflags = _lib.DSGPU_FP16_STAGING if a.fp16 else 0
     dev = torch.device("cuda", 0)
     ctx = ds.Context(0)
     st = torch.cuda.Stream(dev)
@@ -56,7 +58,7 @@ def main():
     def call():
         if a.case == "nlm":
             r = L.dsgpu_nlm(ctx.handle, vp(rgb.data_ptr()), w, h, 3, float(hp), a.search, a.patch, vp(out.data_ptr()),
-                            _lib.DSGPU_ASYNC)
+                            _lib.DSGPU_ASYNC | xflags)
         elif a.case == "rcd":
             r = L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(mul.ctypes.data),
                                  _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(clip.data_ptr()), _lib.DSGPU_ASYNC)
@@ -68,7 +70,7 @@ def main():
         else:
             r = L.dsgpu_develop_u16(ctx.handle, vp(raw.data_ptr()), w, h, w, vp(pat.ctypes.data), 512.0,
                                     vp(white.ctypes.data), vp(mul.ctypes.data), float(hp), a.search, a.patch,
-                                    vp(out.data_ptr()), vp(0), _lib.DSGPU_ASYNC)
+                                    vp(out.data_ptr()), vp(0), _lib.DSGPU_ASYNC | xflags)
         ctx.check(r, a.case)
 
     net = None

@@ -50,6 +50,12 @@ extern "C" {
 /* flags */
 #define DSGPU_HOST 1u  /* buffers are host memory */
 #define DSGPU_ASYNC 2u /* device buffers: do not synchronise before returning */
+/* dsgpu_nlm / dsgpu_develop_u16: the precision variant of NLM. The tile is
+ * staged in shared memory in FP16 (centred on the tile's centre sample);
+ * patch distances, weights and sums stay in FP32 and the weight sum is
+ * accumulated with Kahan compensation. Not bit-equal to the FP32 path; its
+ * error against the FP64 oracle is measured by the tests and the profiles. */
+#define DSGPU_FP16_STAGING 4u
 
 /* demosaic quality (demosaic.rs:9-15) */
 #define DSGPU_QUALITY_DRAFT 0
