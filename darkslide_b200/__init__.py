@@ -36,7 +36,7 @@ from ._lib import Context, DsgpuError, SceneDesc, default_context, lib
 
 __all__ = [
     "CfaPattern", "CfaImage", "Plane", "Image3", "Quality", "demosaic", "rcd_bayer", "mhc_bayer", "clip_plane",
-    "box_blur", "nlm", "normalize_u16", "develop_u16", "BatchFrame", "develop_batch", "batch_frame_ms",
+    "box_blur", "nlm", "normalize_u16", "develop_u16", "cfa_clip_levels", "reconstruct_highlights", "BatchFrame", "develop_batch", "batch_frame_ms",
     "autotune", "autotune_get", "autotune_set", "estimate_noise", "guided_filter", "denoise", "Oklab", "Context", "DsgpuError", "default_context", "Scene",
     "RGGB", "BGGR", "GRBG", "GBRG",
 ]
@@ -249,6 +249,37 @@ def nlm(p, h_param: float, search: int, patch: int, ctx: Context | None = None, 
     return Image3(p.w, p.h, out) if chans == 3 else Plane(p.w, p.h, out)
 
 
+def cfa_clip_levels(cfa: "CfaImage", ctx: Context | None = None) -> np.ndarray:
+    """demosaic.rs:419-430: per-colour clip level of a normalised mosaic
+    (float32 max where the maximum stays below 0.95)."""
+    c = _Call(cfa.data, ctx)
+    _, p = c.inp(cfa.data, np.float32)
+    out = np.empty(3, np.float32)
+    pat = cfa.pattern.codes()
+    c.ctx.check(lib().dsgpu_cfa_clip_levels(c.ctx.handle, p, cfa.w, cfa.h, _vp(pat),
+                                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), c.flags),
+                "dsgpu_cfa_clip_levels")
+    return out
+
+
+def reconstruct_highlights(img: "Image3", clip: "Plane", mul, raw_clip, ctx: Context | None = None) -> "Image3":
+    """demosaic.rs:435-502 on a copy of img (Image3); clip is the demosaic's
+    clip Plane, raw_clip the levels of cfa_clip_levels."""
+    c = _Call(img.data, ctx)
+    if c.torch:
+        data = img.data.contiguous().clone()
+        pi = ctypes.c_void_p(data.data_ptr())
+        _, pc = c.inp(clip.data, np.float32)
+    else:
+        data = np.array(img.data, dtype=np.float32, order="C", copy=True)
+        pi = data.ctypes.data_as(ctypes.c_void_p)
+        _, pc = c.inp(clip.data, np.float32)
+    m, rc = _f3(mul), np.ascontiguousarray(raw_clip, np.float32)
+    c.ctx.check(lib().dsgpu_reconstruct_highlights(c.ctx.handle, pi, pc, img.w, img.h, _vp(m), _vp(rc), c.flags),
+                "dsgpu_reconstruct_highlights")
+    return Image3(img.w, img.h, data)
+
+
 @dataclass
 class BatchFrame:
     """One frame of develop_batch: a CUDA uint16 tensor (h, w), its CFA
@@ -328,10 +359,12 @@ def autotune_set(w: int, h: int, rcd_tile, nlm_ctas_per_sm: int, ctx: Context | 
 
 
 def develop_u16(raw, pattern: CfaPattern, black: float, white, mul, h_param: float, search: int, patch: int,
-                with_clip: bool = False, ctx: Context | None = None, fp16_staging: bool = False):
+                with_clip: bool = False, ctx: Context | None = None, fp16_staging: bool = False,
+                highlights: bool = False):
     """u16 raw -> normalise -> RCD -> per-channel NLM in one device pass.
     Returns the denoised Image3 (and the clip Plane when ``with_clip``).
-    ``fp16_staging``: NLM's precision variant (DSGPU_FP16_STAGING)."""
+    ``fp16_staging``: NLM's precision variant (DSGPU_FP16_STAGING);
+    ``highlights``: reconstruct highlights between RCD and NLM (DSGPU_HIGHLIGHTS)."""
     c = _Call(raw, ctx)
     h, w = raw.shape
     src, p = c.inp(raw, np.uint16)
@@ -340,7 +373,8 @@ def develop_u16(raw, pattern: CfaPattern, black: float, white, mul, h_param: flo
     pat, wh, m = pattern.codes(), _f3(white), _f3(mul)
     c.ctx.check(lib().dsgpu_develop_u16(c.ctx.handle, p, w, h, w, _vp(pat), float(black), _vp(wh), _vp(m),
                                         float(h_param), int(search), int(patch), pr, pc,
-                                        c.flags | (_lib.DSGPU_FP16_STAGING if fp16_staging else 0)),
+                                        c.flags | (_lib.DSGPU_FP16_STAGING if fp16_staging else 0)
+                                        | (_lib.DSGPU_HIGHLIGHTS if highlights else 0)),
                 "dsgpu_develop_u16")
     img = Image3(w, h, rgb)
     return (img, Plane(w, h, clip)) if with_clip else img

@@ -1,5 +1,6 @@
 // C ABI of libdsgpu: argument checks, context, scratch and host staging,
 // and dispatch to the kernels. See include/dsgpu.h for the contract.
+#include <cfloat>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -501,20 +502,86 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
   DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out_rgb, n * 3 * sizeof(float), &drgb));
   if (out_clip) DS_CHECK(stage_out_ptr(ctx, flags, S_OUT2, out_clip, n * sizeof(float), &dclip));
   DS_CHECK(scratch(ctx, S_RGB, n * 3 * sizeof(float), &mid));
+  const bool hl = (flags & DSGPU_HIGHLIGHTS) != 0;
+  void* hl_work = nullptr;
+  float* hl_clip = (float*)dclip;  // highlights need the clip plane even when the caller does not
+  if (hl) {
+    const size_t hb = ds_highlights_scratch_bytes(w, h);
+    DS_CHECK(scratch(ctx, S_WORK, hb + 64 + (dclip ? 0 : n * sizeof(float)), &hl_work));
+    if (!hl_clip) hl_clip = reinterpret_cast<float*>(static_cast<char*>(hl_work) + hb + 64);
+  }
+  unsigned* hl_bits = hl ? reinterpret_cast<unsigned*>(static_cast<char*>(hl_work) + ds_highlights_scratch_bytes(w, h))
+                         : nullptr;
+  float* hl_rc = hl ? reinterpret_cast<float*>(hl_bits + 8) : nullptr;
+  ds_src_u16 src{(const uint16_t*)din, pitch, black, {white[0], white[1], white[2]}};
   if (w < 16 || h < 16) {
     void* cfa_f;
     DS_CHECK(scratch(ctx, S_CFA, n * sizeof(float), &cfa_f));
     DS_TRY(ds_launch_normalize_u16(ctx->stream, (const uint16_t*)din, w, h, pitch, pat, black, white, (float*)cfa_f));
     ctx->launches += 1;
-    DS_CHECK(rcd_dev(ctx, (const float*)cfa_f, w, h, pat, mul, (float*)mid, (float*)dclip));
+    DS_CHECK(rcd_dev(ctx, (const float*)cfa_f, w, h, pat, mul, (float*)mid, hl_clip));
   } else {
     StageMark mark(ctx, DSGPU_STAGE_DEMOSAIC);
-    ds_src_u16 src{(const uint16_t*)din, pitch, black, {white[0], white[1], white[2]}};
-    DS_TRY(ds_launch_rcd_u16(ctx->stream, src, w, h, pat, mul, (float*)mid, (float*)dclip));
+    DS_TRY(ds_launch_rcd_u16(ctx->stream, src, w, h, pat, mul, (float*)mid, hl_clip));
     ctx->launches += 1;
+  }
+  if (hl) {  // Engine::base: reconstruct_highlights(img, clip, mul, cfa_clip_levels(cfa)) (pipeline/mod.rs:186-187)
+    unsigned launches = 0;
+    DS_TRY(ds_launch_clip_levels_u16(ctx->stream, src, w, h, pat, hl_bits, hl_rc));
+    DS_TRY(ds_launch_highlights(ctx->stream, (float*)mid, hl_clip, w, h, mul, hl_rc, hl_work, &launches));
+    ctx->launches += 2 + launches;
   }
   DS_CHECK(run_nlm(ctx, (const float*)mid, w, h, 3, h_param, search, patch, (float*)drgb, flags));
   return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));
+}
+
+// -------------------------------------------------------------- highlights
+
+int dsgpu_cfa_clip_levels(dsgpu_ctx* ctx, const float* cfa, int w, int h, const uint8_t pat_codes[4], float* out3,
+                          unsigned flags) {
+  if (!ctx || !out3) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  ds_pat pat;
+  DS_CHECK(check_pat(pat_codes, &pat));
+  const size_t n = (size_t)w * h;
+  if (n == 0) {  // no samples: every maximum stays 0, below the 0.95 trust level
+    out3[0] = out3[1] = out3[2] = FLT_MAX;
+    return DSGPU_OK;
+  }
+  if (!cfa) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* work;
+  DS_CHECK(stage_in(ctx, flags, S_IN, cfa, n * sizeof(float), &din));
+  DS_CHECK(scratch(ctx, S_TMP, 64, &work));
+  float* raw_clip = reinterpret_cast<float*>(static_cast<char*>(work) + 32);
+  DS_TRY(ds_launch_clip_levels_f32(ctx->stream, (const float*)din, w, h, pat, (unsigned*)work, raw_clip));
+  ctx->launches += 2;
+  DS_TRY(cudaMemcpyAsync(out3, raw_clip, 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  DS_TRY(cudaStreamSynchronize(ctx->stream));
+  return DSGPU_OK;
+}
+
+int dsgpu_reconstruct_highlights(dsgpu_ctx* ctx, float* rgb, const float* clip, int w, int h, const float mul[3],
+                                 const float raw_clip[3], unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  const size_t n = (size_t)w * h;
+  if (n == 0) return DSGPU_OK;
+  if (!rgb || !clip || !mul || !raw_clip) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void *dimg, *dclip;
+  void* work;
+  DS_CHECK(stage_in(ctx, flags, S_OUT, rgb, n * 3 * sizeof(float), &dimg));
+  DS_CHECK(stage_in(ctx, flags, S_IN, clip, n * sizeof(float), &dclip));
+  const size_t hb = ds_highlights_scratch_bytes(w, h);
+  DS_CHECK(scratch(ctx, S_WORK, hb + 64, &work));
+  float* rc = reinterpret_cast<float*>(static_cast<char*>(work) + hb);
+  DS_TRY(cudaMemcpyAsync(rc, raw_clip, 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  unsigned launches = 0;
+  DS_TRY(ds_launch_highlights(ctx->stream, (float*)dimg, (const float*)dclip, w, h, mul, rc, work, &launches));
+  ctx->launches += launches;
+  return finish(ctx, flags, rgb, dimg, n * 3 * sizeof(float));
 }
 
 // ----------------------------------------------------------------- denoise

@@ -70,6 +70,15 @@ cudaError_t ds_launch_rcd_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_
 cudaError_t ds_launch_superpixel(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, const float mul[3],
                                  float* out_rgb, float* out_clip);
 cudaError_t ds_launch_box_blur(cudaStream_t st, const float* in, int w, int h, int r, float* tmp, float* out);
+// highlight reconstruction (demosaic.rs:419-502)
+void ds_box_radii_for_gauss(float sigma, int n, int* radii);
+cudaError_t ds_launch_clip_levels_f32(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, unsigned* bits,
+                                      float* raw_clip);
+cudaError_t ds_launch_clip_levels_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, unsigned* bits,
+                                      float* raw_clip);
+size_t ds_highlights_scratch_bytes(int w, int h);
+cudaError_t ds_launch_highlights(cudaStream_t st, float* img, const float* clip, int w, int h, const float mul[3],
+                                 const float* raw_clip, void* scratch, unsigned* launches);
 // fp16_staging: the precision variant (plane staged in half precision,
 // sums in FP32 with a compensated weight sum); see k_nlm.cu
 cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int channels, float h_param, int search,

@@ -4,6 +4,8 @@
 // This file is compiled with -fmad=false: the reference (Rust) rounds every
 // product before adding it, so the GPU must not contract a*b+c into FMAs for
 // these kernels to reproduce it bit for bit. Divisions are IEEE (__fdiv_rn).
+#include <cfloat>
+
 #include "internal.cuh"
 
 namespace {
@@ -458,6 +460,114 @@ __global__ void __launch_bounds__(RCD_THREADS, 2) rcd_batch_kernel(const ds_batc
   }
 }
 
+// ------------------------------------------------------------------ highlights
+// cfa_clip_levels (demosaic.rs:419-430): per-colour maximum of every third
+// row. Values are clamped at 0 (the reference starts its maxima at 0), so the
+// float bit patterns order like the values and atomicMax on them is exact.
+template <class Src>
+__global__ void clip_levels_kernel(Src src, int w, int h, ds_pat pat, unsigned* __restrict__ mx_bits) {
+  __shared__ unsigned smx[3];
+  if (threadIdx.x < 3) smx[threadIdx.x] = 0u;
+  __syncthreads();
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = 3 * blockIdx.y;
+  if (x < w) {
+    const int c = pat.at(x, y);
+    const float v = src.load(x, y, c);
+    if (v > 0.f) atomicMax(&smx[c], __float_as_uint(v));
+  }
+  __syncthreads();
+  if (threadIdx.x < 3 && smx[threadIdx.x]) atomicMax(&mx_bits[threadIdx.x], smx[threadIdx.x]);
+}
+
+// levels >= 0.95 are trusted, others become FLT_MAX (demosaic.rs:429)
+__global__ void clip_levels_final_kernel(const unsigned* __restrict__ mx_bits, float* __restrict__ raw_clip) {
+  const int c = threadIdx.x;
+  if (c < 3) {
+    const float m = __uint_as_float(mx_bits[c]);
+    raw_clip[c] = m >= 0.95f ? m : FLT_MAX;
+  }
+}
+
+struct HlLevels {
+  float lvl[3];
+  __device__ __forceinline__ HlLevels(const float* raw_clip, float m0, float m1, float m2) {
+    const float mul[3] = {m0, m1, m2};
+#pragma unroll
+    for (int c = 0; c < 3; c++) lvl[c] = raw_clip[c] == FLT_MAX ? FLT_MAX : raw_clip[c] * mul[c] * 0.97f;
+  }
+  __device__ __forceinline__ bool clipped(float v, int c, float clip) const {
+    return v >= lvl[c] || (clip > 0.f && v >= lvl[c] * 0.8f);
+  }
+};
+
+// demosaic.rs:445-462: the weight and colour-ratio planes of bright unclipped
+// pixels away from clipped ones; also raises *any when the clip plane has a
+// set pixel (the reference returns early otherwise, :436-438).
+__global__ void hl_weights_kernel(const float* __restrict__ img, const float* __restrict__ clip,
+                                  const float* __restrict__ near_clip, const float* __restrict__ raw_clip, float m0,
+                                  float m1, float m2, size_t n, float* __restrict__ wgt, float* __restrict__ rr,
+                                  float* __restrict__ br, int* __restrict__ any) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const HlLevels L(raw_clip, m0, m1, m2);
+  const float cl = clip[i];
+  if (cl > 0.f) *any = 1;
+  const float p0 = img[3 * i], p1 = img[3 * i + 1], p2 = img[3 * i + 2];
+  float k = 0.f, r = 0.f, b = 0.f;
+  if (!(near_clip[i] > 0.f || L.clipped(p0, 0, cl) || L.clipped(p1, 1, cl) || L.clipped(p2, 2, cl) || p1 <= 1e-4f)) {
+    const float lmin = fminf(fminf(fminf(L.lvl[0], L.lvl[1]), L.lvl[2]), 4.0f);
+    const float y = __fdiv_rn(__fdiv_rn(p0 + p1 + p2, 3.0f), lmin);
+    k = fminf(y * y, 1.0f);
+    r = fminf(fmaxf(__fdiv_rn(p0, p1), 0.1f), 10.0f) * k;
+    b = fminf(fmaxf(__fdiv_rn(p2, p1), 0.1f), 10.0f) * k;
+  }
+  wgt[i] = k;
+  rr[i] = r;
+  br[i] = b;
+}
+
+// demosaic.rs:466-500: rebuild clipped channels from the blurred ratios
+__global__ void hl_apply_kernel(float* __restrict__ img, const float* __restrict__ clip,
+                                const float* __restrict__ raw_clip, float m0, float m1, float m2, size_t n,
+                                const float* __restrict__ wb, const float* __restrict__ rrb,
+                                const float* __restrict__ brb, const int* __restrict__ any) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !*any) return;
+  const HlLevels L(raw_clip, m0, m1, m2);
+  float p[3] = {img[3 * i], img[3 * i + 1], img[3 * i + 2]};
+  const float cv = clip[i];
+  const bool cl[3] = {L.clipped(p[0], 0, cv), L.clipped(p[1], 1, cv), L.clipped(p[2], 2, cv)};
+  const int nc = (int)cl[0] + (int)cl[1] + (int)cl[2];
+  if (nc == 0) return;
+  if (nc == 3) {
+    const float m = fmaxf(fmaxf(p[0], p[1]), p[2]);
+    img[3 * i] = img[3 * i + 1] = img[3 * i + 2] = m;
+    return;
+  }
+  const float wv = wb[i];
+  float r = 1.0f, b = 1.0f;
+  if (wv > 1e-4f) {
+    r = __fdiv_rn(rrb[i], wv);
+    b = __fdiv_rn(brb[i], wv);
+  }
+  const float trust = fminf(wv * 3.0f, 1.0f);
+  r = 1.0f + (r - 1.0f) * trust;
+  b = 1.0f + (b - 1.0f) * trust;
+  const float ratio[3] = {r, 1.0f, b};
+  float g = p[1];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    if (!cl[c]) g = fmaxf(g, __fdiv_rn(p[c], ratio[c]));
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    if (cl[c]) p[c] = fmaxf(p[c], g * ratio[c]);
+  const float top = fmaxf(fmaxf(p[0], p[1]), p[2]);
+  const float t3 = __fdiv_rn((float)nc, 3.0f);
+  const float t = t3 * t3;
+#pragma unroll
+  for (int c = 0; c < 3; c++) img[3 * i + c] = p[c] + (top - p[c]) * t * 0.5f;
+}
+
 template <class Src>
 cudaError_t launch_rcd(cudaStream_t st, Src src, int w, int h, ds_pat pat, const float mul[3], float* out_rgb,
                        float* out_clip) {
@@ -528,4 +638,84 @@ cudaError_t ds_launch_rcd_batch(cudaStream_t st, const ds_batch_frame* frames, i
   if (e != cudaSuccess) return e;
   rcd_batch_kernel<<<grid, RCD_THREADS, RCD_BATCH_SMEM, st>>>(frames, n, total_tiles);
   return cudaGetLastError();
+}
+
+// ---- highlights (host side)
+
+// image.rs:363-373 box_radii_for_gauss, in f32 as written there
+void ds_box_radii_for_gauss(float sigma, int n, int* radii) {
+  const float w_ideal = sqrtf(12.0f * sigma * sigma / (float)n + 1.0f);
+  int wl = (int)floorf(w_ideal);
+  if (wl % 2 == 0) wl -= 1;
+  const int wu = wl + 2;
+  const float m_ideal = (12.0f * sigma * sigma - (float)(n * wl * wl) - 4.0f * (float)n * (float)wl - 3.0f * (float)n) /
+                        (-4.0f * (float)wl - 4.0f);
+  const int m = (int)roundf(m_ideal);
+  for (int i = 0; i < n; i++) {
+    const int r = ((i < m ? wl : wu) - 1) / 2;
+    radii[i] = r > 0 ? r : 0;
+  }
+}
+
+template <class Src>
+static cudaError_t launch_clip_levels(cudaStream_t st, Src src, int w, int h, ds_pat pat, unsigned* bits,
+                                      float* raw_clip) {
+  cudaError_t e = cudaMemsetAsync(bits, 0, 3 * sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  if (w > 0 && h > 0) {
+    dim3 grid((w + 255) / 256, (h + 2) / 3);
+    clip_levels_kernel<Src><<<grid, 256, 0, st>>>(src, w, h, pat, bits);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  clip_levels_final_kernel<<<1, 32, 0, st>>>(bits, raw_clip);
+  return cudaGetLastError();
+}
+
+cudaError_t ds_launch_clip_levels_f32(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, unsigned* bits,
+                                      float* raw_clip) {
+  return launch_clip_levels(st, SrcF32{ds_src_f32{cfa, w}}, w, h, pat, bits, raw_clip);
+}
+
+cudaError_t ds_launch_clip_levels_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, unsigned* bits,
+                                      float* raw_clip) {
+  return launch_clip_levels(st, SrcU16{src}, w, h, pat, bits, raw_clip);
+}
+
+size_t ds_highlights_scratch_bytes(int w, int h) { return (size_t)w * h * sizeof(float) * 10 + 256; }
+
+// reconstruct_highlights (demosaic.rs:435-502) in place on img; raw_clip is a
+// device array of 3 (from ds_launch_clip_levels_*); scratch holds
+// ds_highlights_scratch_bytes(w, h).
+cudaError_t ds_launch_highlights(cudaStream_t st, float* img, const float* clip, int w, int h, const float mul[3],
+                                 const float* raw_clip, void* scratch, unsigned* launches) {
+  const size_t n = (size_t)w * h;
+  if (n == 0) return cudaSuccess;
+  float* f = static_cast<float*>(scratch);
+  float *near_clip = f, *wgt = f + n, *rr = f + 2 * n, *br = f + 3 * n, *wb = f + 4 * n, *rrb = f + 5 * n,
+        *brb = f + 6 * n, *ta = f + 7 * n, *tb = f + 8 * n, *tmp = f + 9 * n;
+  int* any = reinterpret_cast<int*>(f + 10 * n);
+  cudaError_t e = cudaMemsetAsync(any, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = ds_launch_box_blur(st, clip, w, h, 3, tmp, near_clip);
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (e == cudaSuccess) {
+    hl_weights_kernel<<<blocks, 256, 0, st>>>(img, clip, near_clip, raw_clip, mul[0], mul[1], mul[2], n, wgt, rr, br,
+                                              any);
+    e = cudaGetLastError();
+  }
+  const float sigma = fmaxf((float)(w > h ? w : h) / 120.0f, 2.0f);  // demosaic.rs:442
+  int r[3];
+  ds_box_radii_for_gauss(sigma, 3, r);
+  const float* src[3] = {wgt, rr, br};
+  float* dst[3] = {wb, rrb, brb};
+  for (int k = 0; k < 3 && e == cudaSuccess; k++) {  // gaussian_blur (image.rs:327-338), sigma >= 2
+    e = ds_launch_box_blur(st, src[k], w, h, r[0], tmp, ta);
+    if (e == cudaSuccess) e = ds_launch_box_blur(st, ta, w, h, r[1], tmp, tb);
+    if (e == cudaSuccess) e = ds_launch_box_blur(st, tb, w, h, r[2], tmp, dst[k]);
+  }
+  if (e == cudaSuccess) {
+    hl_apply_kernel<<<blocks, 256, 0, st>>>(img, clip, raw_clip, mul[0], mul[1], mul[2], n, wb, rrb, brb, any);
+    e = cudaGetLastError();
+  }
+  if (launches) *launches += 3 + 2 * 10;
+  return e;
 }

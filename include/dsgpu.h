@@ -56,6 +56,10 @@ extern "C" {
  * accumulated with Kahan compensation. Not bit-equal to the FP32 path; its
  * error against the FP64 oracle is measured by the tests and the profiles. */
 #define DSGPU_FP16_STAGING 4u
+/* dsgpu_develop_u16: reconstruct highlights between RCD and NLM, as
+ * Engine::base does (pipeline/mod.rs:186-187): cfa_clip_levels of the
+ * normalised mosaic, then reconstruct_highlights with the clip plane. */
+#define DSGPU_HIGHLIGHTS 8u
 
 /* demosaic quality (demosaic.rs:9-15) */
 #define DSGPU_QUALITY_DRAFT 0
@@ -154,6 +158,20 @@ int dsgpu_guided_filter(dsgpu_ctx* ctx, const float* I, const float* p, int w, i
 /* Oklab matrices of Oklab::new() (color.rs:394-399): to_lms, from_lms and
  * inverse M2, row-major, 27 floats. Host only. */
 int dsgpu_oklab_matrices(float* out27);
+
+/* Per-colour clip level actually reached in a normalised mosaic: the maximum
+ * over every third row, kept when >= 0.95, else FLT_MAX. out3 is host
+ * memory (the call waits). Replaces cfa_clip_levels, demosaic.rs:419-430. */
+int dsgpu_cfa_clip_levels(dsgpu_ctx* ctx, const float* cfa, int w, int h, const uint8_t pattern[4], float* out3,
+                          unsigned flags);
+/* Highlight reconstruction in place on interleaved RGB (w*h*3): channels at
+ * their clip level are rebuilt from colour ratios of nearby bright unclipped
+ * pixels, fully clipped pixels become neutral. clip: the clip plane of
+ * dsgpu_demosaic; raw_clip: host array of 3 (dsgpu_cfa_clip_levels). A no-op
+ * when no clip-plane pixel is set. Replaces reconstruct_highlights,
+ * demosaic.rs:435-502 (bit-exact). */
+int dsgpu_reconstruct_highlights(dsgpu_ctx* ctx, float* rgb, const float* clip, int w, int h, const float mul[3],
+                                 const float raw_clip[3], unsigned flags);
 
 /* Strong denoise of an interleaved linear RGB image, amount 0..100: Oklab L
  * through NLM (search 3, patch 1, h = sigma (0.6 + 1.6 amount/100)), chroma

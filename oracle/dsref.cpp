@@ -20,6 +20,8 @@
 //   enhance.rs:36-72    nlm (offset chunks reduced in chunk order)
 //   enhance.rs:75-92    denoise (Oklab L NLM + guided chroma)
 //   image.rs:385-405    guided_filter
+//   demosaic.rs:419-502 cfa_clip_levels, reconstruct_highlights
+//   image.rs:327-338, 363-373  gaussian_blur (sigma >= 2), box_radii_for_gauss
 //   color.rs:6-98, 380-419  matrix helpers, Bradford, ProPhoto, Oklab
 // Every kernel is a template on the arithmetic type; the double instantiation
 // is the FP64 oracle.
@@ -34,6 +36,7 @@
 // Build with -ffp-contract=off: Rust never fuses a*b+c, so neither may we.
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -560,6 +563,102 @@ void guided_filter(const float* I, const float* p, size_t w, size_t h, size_t r,
   for (size_t k = 0; k < n; k++) out[k] = ma[k] * I[k] + mb[k];
 }
 
+// ---------------------------------------------------------------- highlights
+// demosaic.rs:419-430 cfa_clip_levels: per-colour maximum over every third
+// row, trusted as a clip level only when >= 0.95.
+void cfa_clip_levels(const float* cfa, long w, long h, const Pat& pat, float out[3]) {
+  float mx[3] = {0.f, 0.f, 0.f};
+  for (long y = 0; y < h; y += 3)
+    for (long x = 0; x < w; x++) {
+      const int c = pat.at(x, y);
+      mx[c] = std::fmax(mx[c], cfa[y * w + x]);
+    }
+  for (int c = 0; c < 3; c++) out[c] = mx[c] >= 0.95f ? mx[c] : FLT_MAX;
+}
+
+// image.rs:363-373 box_radii_for_gauss, f32 as written there.
+void box_radii_for_gauss(float sigma, int n, int* radii) {
+  const float w_ideal = std::sqrt(12.0f * sigma * sigma / (float)n + 1.0f);
+  int wl = (int)std::floor(w_ideal);
+  if (wl % 2 == 0) wl -= 1;
+  const int wu = wl + 2;
+  const float m_ideal = (12.0f * sigma * sigma - (float)(n * wl * wl) - 4.0f * (float)n * (float)wl - 3.0f * (float)n) /
+                        (-4.0f * (float)wl - 4.0f);
+  const int m = (int)std::round(m_ideal);
+  for (int i = 0; i < n; i++) radii[i] = std::max(((i < m ? wl : wu) - 1) / 2, 0);
+}
+
+// image.rs:327-338 gaussian_blur for sigma >= 2 (three box blurs); the
+// highlight code only calls it with sigma >= 2.
+void gaussian_blur_boxes(const float* p, long w, long h, float sigma, float* out) {
+  int r[3];
+  box_radii_for_gauss(sigma, 3, r);
+  std::vector<float> a((size_t)w * h), b((size_t)w * h);
+  box_blur<float>(p, w, h, r[0], a.data());
+  box_blur<float>(a.data(), w, h, r[1], b.data());
+  box_blur<float>(b.data(), w, h, r[2], out);
+}
+
+// demosaic.rs:435-502 reconstruct_highlights, in place on interleaved RGB.
+void reconstruct_highlights(float* img, const float* clip, long w, long h, const float mul[3], const float raw_clip[3]) {
+  const size_t n = (size_t)w * h;
+  bool any = false;
+  for (size_t i = 0; i < n && !any; i++) any = clip[i] > 0.0f;
+  if (!any) return;
+  float lvl[3];
+  for (int c = 0; c < 3; c++) lvl[c] = raw_clip[c] == FLT_MAX ? FLT_MAX : raw_clip[c] * mul[c] * 0.97f;
+  auto is_clipped = [&](const float* p, int c, size_t i) {
+    return p[c] >= lvl[c] || (clip[i] > 0.0f && p[c] >= lvl[c] * 0.8f);
+  };
+  const float sigma = std::fmax((float)std::max(w, h) / 120.0f, 2.0f);
+  const float lmin = std::fmin(std::fmin(std::fmin(lvl[0], lvl[1]), lvl[2]), 4.0f);
+  std::vector<float> near_clip(n), wgt(n, 0.f), rr(n, 0.f), br(n, 0.f);
+  box_blur<float>(clip, w, h, 3, near_clip.data());
+  for (size_t i = 0; i < n; i++) {
+    const float* p = img + 3 * i;
+    if (near_clip[i] > 0.0f || is_clipped(p, 0, i) || is_clipped(p, 1, i) || is_clipped(p, 2, i) || p[1] <= 1e-4f)
+      continue;
+    const float y = (p[0] + p[1] + p[2]) / 3.0f / lmin;
+    const float k = std::fmin(y * y, 1.0f);
+    wgt[i] = k;
+    rr[i] = std::clamp(p[0] / p[1], 0.1f, 10.0f) * k;
+    br[i] = std::clamp(p[2] / p[1], 0.1f, 10.0f) * k;
+  }
+  std::vector<float> wb(n), rrb(n), brb(n);
+  gaussian_blur_boxes(wgt.data(), w, h, sigma, wb.data());
+  gaussian_blur_boxes(rr.data(), w, h, sigma, rrb.data());
+  gaussian_blur_boxes(br.data(), w, h, sigma, brb.data());
+  for (size_t i = 0; i < n; i++) {
+    float* p = img + 3 * i;
+    const bool cl[3] = {is_clipped(p, 0, i), is_clipped(p, 1, i), is_clipped(p, 2, i)};
+    const int nc = (int)cl[0] + (int)cl[1] + (int)cl[2];
+    if (nc == 0) continue;
+    const float m = std::fmax(std::fmax(p[0], p[1]), p[2]);
+    if (nc == 3) {
+      p[0] = p[1] = p[2] = m;
+      continue;
+    }
+    const float wv = wb[i];
+    float r = 1.0f, b = 1.0f;
+    if (wv > 1e-4f) {
+      r = rrb[i] / wv;
+      b = brb[i] / wv;
+    }
+    const float trust = std::fmin(wv * 3.0f, 1.0f);
+    r = 1.0f + (r - 1.0f) * trust;
+    b = 1.0f + (b - 1.0f) * trust;
+    const float ratio[3] = {r, 1.0f, b};
+    float g = p[1];
+    for (int c = 0; c < 3; c++)
+      if (!cl[c]) g = std::fmax(g, p[c] / ratio[c]);
+    for (int c = 0; c < 3; c++)
+      if (cl[c]) p[c] = std::fmax(p[c], g * ratio[c]);
+    const float top = std::fmax(std::fmax(p[0], p[1]), p[2]);
+    const float t = ((float)nc / 3.0f) * ((float)nc / 3.0f);  // powi(2)
+    for (int c = 0; c < 3; c++) p[c] += (top - p[c]) * t * 0.5f;
+  }
+}
+
 // ------------------------------------------------------------------ denoise
 // enhance.rs:75-92
 void denoise(const float* img, size_t w, size_t h, float amount, int nthreads, float* out, float* sigma_out) {
@@ -685,6 +784,19 @@ void dsref_oklab_to_prophoto(const float* lab, int n, float* rgb) {
 
 void dsref_guided_filter_f32(const float* I, const float* p, int w, int h, int r, float eps, float* out) {
   guided_filter(I, p, w, h, r, eps, out);
+}
+
+void dsref_cfa_clip_levels(const float* cfa, int w, int h, const uint8_t pat[4], float* out3) {
+  Pat p;
+  std::memcpy(p.c, pat, 4);
+  cfa_clip_levels(cfa, w, h, p, out3);
+}
+
+void dsref_box_radii_for_gauss(float sigma, int n, int* radii) { box_radii_for_gauss(sigma, n, radii); }
+
+void dsref_reconstruct_highlights(float* img, const float* clip, int w, int h, const float mul[3],
+                                  const float raw_clip[3]) {
+  reconstruct_highlights(img, clip, w, h, mul, raw_clip);
 }
 
 void dsref_denoise_f32(const float* img, int w, int h, float amount, int nthreads, float* out, float* sigma) {

@@ -52,6 +52,9 @@ def lib():
         L.dsref_box_blur_f64.argtypes = [_f64p, i, i, i, _f64p]
         L.dsref_nlm_f32.argtypes = [_f32p, i, i, f, i, i, i, _f32p]
         L.dsref_nlm_f64.argtypes = [_f64p, i, i, d, i, i, i, _f64p]
+        L.dsref_cfa_clip_levels.argtypes = [_f32p, i, i, _u8p, _f32p]
+        L.dsref_box_radii_for_gauss.argtypes = [f, i, np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")]
+        L.dsref_reconstruct_highlights.argtypes = [_f32p, _f32p, i, i, _f32p, _f32p]
         L.dsref_estimate_noise_f32.argtypes = [_f32p, i, i]
         L.dsref_estimate_noise_f32.restype = f
         L.dsref_oklab_matrices.argtypes = [_f32p]
@@ -215,3 +218,27 @@ def denoise(img: np.ndarray, amount: float, nthreads: int | None = None):
     nt = threads() if nthreads is None else int(nthreads)
     lib().dsref_denoise_f32(a, w, h, float(amount), nt, out, sig)
     return out, float(sig[0])
+
+
+def cfa_clip_levels(cfa_data: np.ndarray, cfa) -> np.ndarray:
+    """demosaic.rs:419-430: per-colour clip level (FLT_MAX where untrusted)."""
+    a = np.ascontiguousarray(cfa_data, dtype=np.float32)
+    out = np.empty(3, np.float32)
+    lib().dsref_cfa_clip_levels(a, a.shape[1], a.shape[0], _pat(cfa), out)
+    return out
+
+
+def box_radii_for_gauss(sigma: float, n: int = 3) -> list:
+    """image.rs:363-373."""
+    out = np.empty(n, np.int32)
+    lib().dsref_box_radii_for_gauss(float(sigma), int(n), out)
+    return [int(v) for v in out]
+
+
+def reconstruct_highlights(img: np.ndarray, clip: np.ndarray, mul, raw_clip) -> np.ndarray:
+    """demosaic.rs:435-502 on a copy of an interleaved (h, w, 3) image."""
+    out = np.array(img, dtype=np.float32, order="C", copy=True)
+    c = np.ascontiguousarray(clip, dtype=np.float32)
+    lib().dsref_reconstruct_highlights(out, c, out.shape[1], out.shape[0], np.ascontiguousarray(mul, np.float32),
+                                       np.ascontiguousarray(raw_clip, np.float32))
+    return out

@@ -10,6 +10,8 @@ agree with the oracle bit for bit (NLM up to the last ulp of ``exp``).
   demosaic.rs:31-42    clip_plane
   image.rs:269-313     box_blur
   enhance.rs:36-72     nlm
+  demosaic.rs:419-502  cfa_clip_levels, reconstruct_highlights
+  image.rs:327-373     gaussian_blur (sigma >= 2), box_radii_for_gauss
 """
 from __future__ import annotations
 
@@ -235,3 +237,83 @@ def nlm(p, h_param, search, patch, nthreads=1):
         acc = acc + a
         wsum = wsum + s
     return acc / np.fmax(wsum, dt(1e-12))
+
+
+FMAX = F(np.finfo(F).max)
+
+
+def cfa_clip_levels(cfa, pat):
+    h, w = cfa.shape
+    cm = _color_map(pat, h, w)[::3]
+    rows = cfa[::3]
+    mx = np.zeros(3, F)
+    for c in range(3):
+        v = rows[cm == c]
+        if v.size:
+            mx[c] = np.fmax(F(0), v.max())
+    return np.where(mx >= F(0.95), mx, FMAX).astype(F)
+
+
+def _round_half_away(x):
+    return int(np.sign(x) * np.floor(abs(float(x)) + 0.5))
+
+
+def box_radii_for_gauss(sigma, n=3):
+    sigma, nf = F(sigma), F(n)
+    w_ideal = np.sqrt(F(12) * sigma * sigma / nf + F(1))
+    wl = int(np.floor(w_ideal))
+    if wl % 2 == 0:
+        wl -= 1
+    wu = wl + 2
+    m_ideal = (F(12) * sigma * sigma - F(n * wl * wl) - F(4) * nf * F(wl) - F(3) * nf) / (F(-4) * F(wl) - F(4))
+    m = _round_half_away(m_ideal)
+    return [max(((wl if i < m else wu) - 1) // 2, 0) for i in range(n)]
+
+
+def gaussian_blur(p, sigma):
+    r = box_radii_for_gauss(sigma, 3)
+    return box_blur(box_blur(box_blur(p, r[0]), r[1]), r[2])
+
+
+def reconstruct_highlights(img, clip, mul, raw_clip):
+    img = np.asarray(img, F)
+    if not (clip > 0).any():
+        return img.copy()
+    lvl = [FMAX if F(raw_clip[c]) == FMAX else F(raw_clip[c]) * F(mul[c]) * F(0.97) for c in range(3)]
+    P = [img[..., c] for c in range(3)]
+    cl = [(P[c] >= lvl[c]) | ((clip > 0) & (P[c] >= lvl[c] * F(0.8))) for c in range(3)]
+    h, w = clip.shape
+    sigma = max(F(max(w, h)) / F(120), F(2))
+    lmin = min(min(min(lvl[0], lvl[1]), lvl[2]), F(4))
+    near = box_blur(clip.astype(F), 3)
+    valid = ~((near > 0) | cl[0] | cl[1] | cl[2] | (P[1] <= F(1e-4)))
+    with np.errstate(all="ignore"):
+        y = (P[0] + P[1] + P[2]) / F(3) / lmin
+        k = np.minimum(y * y, F(1))
+        rr = np.clip(P[0] / P[1], F(0.1), F(10)) * k
+        br = np.clip(P[2] / P[1], F(0.1), F(10)) * k
+    z = F(0)
+    wgt, rr, br = (np.where(valid, a, z).astype(F) for a in (k, rr, br))
+    wb, rrb, brb = (gaussian_blur(a, sigma) for a in (wgt, rr, br))
+    nc = cl[0].astype(np.int32) + cl[1] + cl[2]
+    m = np.fmax(np.fmax(P[0], P[1]), P[2])
+    with np.errstate(all="ignore"):
+        big = wb > F(1e-4)
+        r = np.where(big, rrb / wb, F(1)).astype(F)
+        b = np.where(big, brb / wb, F(1)).astype(F)
+    trust = np.minimum(wb * F(3), F(1))
+    r = F(1) + (r - F(1)) * trust
+    b = F(1) + (b - F(1)) * trust
+    ratio = [r, np.ones_like(r), b]
+    g = P[1].copy()
+    with np.errstate(all="ignore"):
+        for c in range(3):
+            g = np.where(~cl[c], np.fmax(g, P[c] / ratio[c]), g)
+    q = [np.where(cl[c], np.fmax(P[c], g * ratio[c]), P[c]) for c in range(3)]
+    top = np.fmax(np.fmax(q[0], q[1]), q[2])
+    t = (nc.astype(F) / F(3)) * (nc.astype(F) / F(3))
+    q = [q[c] + (top - q[c]) * t * F(0.5) for c in range(3)]
+    out = np.stack(q, axis=-1)
+    out = np.where((nc == 3)[..., None], m[..., None], out)
+    out = np.where((nc == 0)[..., None], img, out)
+    return out.astype(F)

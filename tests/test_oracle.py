@@ -164,3 +164,39 @@ def test_cnn_reference_gradients_match_finite_differences():
         e[idx] = 1e-6
         fd = (loss(p + e) - loss(p - e)) / 2e-6
         assert abs(g[idx] - fd) <= 1e-6 + 1e-5 * abs(fd), (idx, g[idx], fd)
+
+
+def _clipped_frame(seed, h, w, pat):
+    """A mosaic with saturated regions: a bright gradient pushed past white."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:h, 0:w]
+    base = 0.5 + 0.7 * np.sin(xx / 7.0) * np.cos(yy / 11.0) + rng.normal(0, 0.01, (h, w))
+    gains = np.array([0.8, 1.0, 0.6], np.float32)
+    cm = R._color_map(pat, h, w)
+    return np.minimum(base * gains[cm], 1.0).astype(np.float32)
+
+
+@pytest.mark.parametrize("pat", PATTERNS)
+@pytest.mark.parametrize("hw", [(40, 52), (97, 61)])
+def test_oracle_matches_numpy_restatement_highlights(oracle, pat, hw):
+    cfa = _clipped_frame(hash((tuple(pat), hw)) & 0xFFFF, *hw, pat)
+    mul = np.array([2.0, 1.0, 1.4285714], np.float32)
+    lv = oracle.cfa_clip_levels(cfa, pat)
+    np.testing.assert_array_equal(lv, R.cfa_clip_levels(cfa, pat))
+    img = oracle.rcd(cfa, pat, mul)
+    clip = oracle.clip_plane(cfa)
+    assert clip.any() and lv[1] < np.finfo(np.float32).max
+    a = oracle.reconstruct_highlights(img, clip, mul, lv)
+    np.testing.assert_array_equal(a, R.reconstruct_highlights(img, clip, mul, lv))
+    assert not np.array_equal(a, img)  # something was rebuilt
+
+
+@pytest.mark.parametrize("sigma", [2.0, 2.5, 8.3, 50.0, 79.2])
+def test_box_radii_match(oracle, sigma):
+    assert oracle.box_radii_for_gauss(sigma) == R.box_radii_for_gauss(sigma)
+
+
+def test_highlights_untouched_without_clipping(oracle):
+    img = np.random.default_rng(3).uniform(0, 0.8, (20, 30, 3)).astype(np.float32)
+    out = oracle.reconstruct_highlights(img, np.zeros((20, 30), np.float32), [2, 1, 1.4], [1.0, 1.0, 1.0])
+    np.testing.assert_array_equal(out, img)
