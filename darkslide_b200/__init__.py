@@ -36,7 +36,7 @@ from ._lib import Context, DsgpuError, SceneDesc, default_context, lib
 
 __all__ = [
     "CfaPattern", "CfaImage", "Plane", "Image3", "Quality", "demosaic", "rcd_bayer", "mhc_bayer", "clip_plane",
-    "box_blur", "nlm", "normalize_u16", "develop_u16", "cfa_clip_levels", "reconstruct_highlights", "BatchFrame", "develop_batch", "batch_frame_ms",
+    "box_blur", "nlm", "normalize_u16", "develop_u16", "cfa_clip_levels", "reconstruct_highlights", "apply_orientation", "BatchFrame", "develop_batch", "batch_frame_ms",
     "autotune", "autotune_get", "autotune_set", "estimate_noise", "guided_filter", "denoise", "Oklab", "Context", "DsgpuError", "default_context", "Scene",
     "RGGB", "BGGR", "GRBG", "GBRG",
 ]
@@ -278,6 +278,18 @@ def reconstruct_highlights(img: "Image3", clip: "Plane", mul, raw_clip, ctx: Con
     c.ctx.check(lib().dsgpu_reconstruct_highlights(c.ctx.handle, pi, pc, img.w, img.h, _vp(m), _vp(rc), c.flags),
                 "dsgpu_reconstruct_highlights")
     return Image3(img.w, img.h, data)
+
+
+def apply_orientation(img: "Image3", orientation: int, ctx: Context | None = None) -> "Image3":
+    """decode.rs:414-426: the image in EXIF orientation 1-8 (5-8 swap w and h)."""
+    c = _Call(img.data, ctx)
+    _, pi = c.inp(img.data, np.float32)
+    swap = 5 <= int(orientation) <= 8
+    ow, oh = (img.h, img.w) if swap else (img.w, img.h)
+    out, po = c.out((oh, ow, 3))
+    c.ctx.check(lib().dsgpu_apply_orientation(c.ctx.handle, pi, img.w, img.h, int(orientation), po, c.flags),
+                "dsgpu_apply_orientation")
+    return Image3(ow, oh, out)
 
 
 @dataclass

@@ -44,7 +44,7 @@ EXPORTS = [
     "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_cnn_set_loss", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
     "dsgpu_measure_mma_sync",
     "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render", "dsgpu_scene_render_window",
-    "dsgpu_cfa_clip_levels", "dsgpu_reconstruct_highlights", "dsgpu_rcd_nlm_batch", "dsgpu_batch_frame_ms", "dsgpu_autotune", "dsgpu_autotune_get", "dsgpu_autotune_set",
+    "dsgpu_cfa_clip_levels", "dsgpu_reconstruct_highlights", "dsgpu_apply_orientation", "dsgpu_rcd_nlm_batch", "dsgpu_batch_frame_ms", "dsgpu_autotune", "dsgpu_autotune_get", "dsgpu_autotune_set",
 ]
 
 
@@ -147,6 +147,7 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_scene_truth_host.argtypes = [ctypes.POINTER(SceneDesc), i, i, i, i, vp]
             L.dsgpu_scene_render.argtypes = [vp, ctypes.POINTER(SceneDesc), vp, u]
             L.dsgpu_scene_render_window.argtypes = [vp, ctypes.POINTER(SceneDesc), i, i, i, i, vp, u]
+            L.dsgpu_apply_orientation.argtypes = [vp, vp, i, i, i, vp, u]
             L.dsgpu_cfa_clip_levels.argtypes = [vp, vp, i, i, vp, ctypes.POINTER(f), u]
             L.dsgpu_reconstruct_highlights.argtypes = [vp, vp, vp, i, i, vp, vp, u]
             L.dsgpu_rcd_nlm_batch.argtypes = [vp, ctypes.POINTER(Frame), i, i, i, u]

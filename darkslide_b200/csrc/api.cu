@@ -584,6 +584,25 @@ int dsgpu_reconstruct_highlights(dsgpu_ctx* ctx, float* rgb, const float* clip, 
   return finish(ctx, flags, rgb, dimg, n * 3 * sizeof(float));
 }
 
+// ------------------------------------------------------------- orientation
+
+int dsgpu_apply_orientation(dsgpu_ctx* ctx, const float* in, int w, int h, int orientation, float* out,
+                            unsigned flags) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DS_CHECK(check_dims(w, h));
+  const size_t bytes = (size_t)w * h * 3 * sizeof(float);
+  if (bytes == 0) return DSGPU_OK;
+  if (!in || !out || in == out) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  const void* din;
+  void* dout;
+  DS_CHECK(stage_in(ctx, flags, S_IN, in, bytes, &din));
+  DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, bytes, &dout));
+  DS_TRY(ds_launch_orientation(ctx->stream, (const float*)din, w, h, orientation, (float*)dout));
+  ctx->launches += 1;
+  return finish(ctx, flags, out, dout, bytes);
+}
+
 // ----------------------------------------------------------------- denoise
 
 int dsgpu_oklab_matrices(float* out27) {

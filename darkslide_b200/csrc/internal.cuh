@@ -77,6 +77,7 @@ cudaError_t ds_launch_clip_levels_f32(cudaStream_t st, const float* cfa, int w, 
 cudaError_t ds_launch_clip_levels_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, unsigned* bits,
                                       float* raw_clip);
 size_t ds_highlights_scratch_bytes(int w, int h);
+cudaError_t ds_launch_orientation(cudaStream_t st, const float* in, int w, int h, int orientation, float* out);
 cudaError_t ds_launch_highlights(cudaStream_t st, float* img, const float* clip, int w, int h, const float mul[3],
                                  const float* raw_clip, void* scratch, unsigned* launches);
 // fp16_staging: the precision variant (plane staged in half precision,

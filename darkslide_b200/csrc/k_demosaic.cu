@@ -719,3 +719,64 @@ cudaError_t ds_launch_highlights(cudaStream_t st, float* img, const float* clip,
   if (launches) *launches += 3 + 2 * 10;
   return e;
 }
+
+// ---- orientation (decode.rs:414-426)
+
+// Source pixel of output (x, y) for EXIF orientation o of a w x h image.
+__device__ __forceinline__ void orient_src(int o, int w, int h, int x, int y, int& sx, int& sy) {
+  switch (o) {
+    case 2: sx = w - 1 - x; sy = y; break;
+    case 3: sx = w - 1 - x; sy = h - 1 - y; break;
+    case 4: sx = x; sy = h - 1 - y; break;
+    case 5: sx = y; sy = x; break;
+    case 6: sx = y; sy = h - 1 - x; break;
+    case 7: sx = w - 1 - y; sy = h - 1 - x; break;
+    case 8: sx = w - 1 - y; sy = x; break;
+    default: sx = x; sy = y; break;
+  }
+}
+
+// One 32 x 32 output tile: its source block is read row by row (coalesced)
+// into shared memory, then written out row by row (coalesced); the mapping
+// is affine with unit coefficients, so the block is 32 x 32 as well.
+__global__ void orient_kernel(const float* __restrict__ in, int w, int h, int o, int ow, int oh,
+                              float* __restrict__ out) {
+  __shared__ float t[3][32][33];
+  const int X0 = blockIdx.x * 32, Y0 = blockIdx.y * 32;
+  int ax, ay, bx, by;
+  orient_src(o, w, h, X0, Y0, ax, ay);
+  orient_src(o, w, h, X0 + 31, Y0 + 31, bx, by);
+  const int sx0 = ax < bx ? ax : bx, sy0 = ay < by ? ay : by;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int sx = sx0 + threadIdx.x, sy = sy0 + j;
+    if (sx >= 0 && sx < w && sy >= 0 && sy < h) {
+      const float* p = in + ((size_t)sy * w + sx) * 3;
+      t[0][j][threadIdx.x] = p[0];
+      t[1][j][threadIdx.x] = p[1];
+      t[2][j][threadIdx.x] = p[2];
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int x = X0 + threadIdx.x, y = Y0 + j;
+    if (x >= ow || y >= oh) continue;
+    int sx, sy;
+    orient_src(o, w, h, x, y, sx, sy);
+    float* q = out + ((size_t)y * ow + x) * 3;
+    q[0] = t[0][sy - sy0][sx - sx0];
+    q[1] = t[1][sy - sy0][sx - sx0];
+    q[2] = t[2][sy - sy0][sx - sx0];
+  }
+}
+
+// apply_orientation: out is (h x w) for orientations 5-8, else (w x h)
+cudaError_t ds_launch_orientation(cudaStream_t st, const float* in, int w, int h, int o, float* out) {
+  const bool swap = o >= 5 && o <= 8;
+  const int ow = swap ? h : w, oh = swap ? w : h;
+  if (ow == 0 || oh == 0) return cudaSuccess;
+  if (o < 2 || o > 8)  // the identity (and unknown codes, which the reference leaves alone)
+    return cudaMemcpyAsync(out, in, (size_t)w * h * 3 * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  dim3 grid((ow + 31) / 32, (oh + 31) / 32);
+  orient_kernel<<<grid, dim3(32, 8), 0, st>>>(in, w, h, o, ow, oh, out);
+  return cudaGetLastError();
+}

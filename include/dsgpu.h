@@ -173,6 +173,12 @@ int dsgpu_cfa_clip_levels(dsgpu_ctx* ctx, const float* cfa, int w, int h, const 
 int dsgpu_reconstruct_highlights(dsgpu_ctx* ctx, float* rgb, const float* clip, int w, int h, const float mul[3],
                                  const float raw_clip[3], unsigned flags);
 
+/* EXIF orientation (1-8) of an interleaved RGB image: out is h x w (width
+ * h) for 5-8, else w x h; other codes copy. out must not alias in. Replaces
+ * apply_orientation, decode.rs:414-426 (exact: a permutation). */
+int dsgpu_apply_orientation(dsgpu_ctx* ctx, const float* in_rgb, int w, int h, int orientation, float* out_rgb,
+                            unsigned flags);
+
 /* Strong denoise of an interleaved linear RGB image, amount 0..100: Oklab L
  * through NLM (search 3, patch 1, h = sigma (0.6 + 1.6 amount/100)), chroma
  * through guided filters. Replaces denoise, enhance.rs:75-92. */

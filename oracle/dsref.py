@@ -242,3 +242,17 @@ def reconstruct_highlights(img: np.ndarray, clip: np.ndarray, mul, raw_clip) -> 
     lib().dsref_reconstruct_highlights(out, c, out.shape[1], out.shape[0], np.ascontiguousarray(mul, np.float32),
                                        np.ascontiguousarray(raw_clip, np.float32))
     return out
+
+
+def apply_orientation(img: np.ndarray, o: int) -> np.ndarray:
+    """decode.rs:414-426 on an (h, w, 3) array: output pixel (x, y) takes the
+    source pixel the reference's match arm names."""
+    h, w = img.shape[:2]
+    if o in (5, 6, 7, 8):
+        oh, ow = w, h
+    else:
+        oh, ow = h, w
+    y, x = np.mgrid[0:oh, 0:ow]
+    src = {2: (w - 1 - x, y), 3: (w - 1 - x, h - 1 - y), 4: (x, h - 1 - y), 5: (y, x), 6: (y, h - 1 - x),
+           7: (w - 1 - y, h - 1 - x), 8: (w - 1 - y, x)}.get(o, (x, y))
+    return img[src[1], src[0]]

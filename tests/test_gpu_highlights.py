@@ -1,4 +1,4 @@
-"""Highlight reconstruction on the GPU (cfa_clip_levels, reconstruct_highlights,
+"""Highlight reconstruction and orientation on the GPU (cfa_clip_levels, reconstruct_highlights,
 demosaic.rs:419-502) against the oracle, bit for bit, and the develop path
 with DSGPU_HIGHLIGHTS (Engine::base's order: RCD, highlights, then NLM)."""
 import numpy as np
@@ -71,3 +71,13 @@ def test_develop_with_highlights(ctx, oracle, pat):
     assert np.abs(got - exp).max() <= 2e-4
     plain = ds.develop_u16(raw, pat, 512, white, MUL, hp, 4, 2, ctx=ctx).data
     assert np.abs(plain - got).max() > 1e-3  # the flag changed the result
+
+
+@pytest.mark.parametrize("o", range(0, 10))
+@pytest.mark.parametrize("hw", [(37, 70), (64, 64), (5, 130)])
+def test_apply_orientation(ctx, oracle, o, hw):
+    img = np.random.default_rng(o).uniform(0, 1, hw + (3,)).astype(np.float32)
+    got = ds.apply_orientation(ds.Image3(hw[1], hw[0], img), o, ctx=ctx)
+    exp = oracle.apply_orientation(img, o)
+    assert (got.h, got.w) == exp.shape[:2]
+    np.testing.assert_array_equal(got.data, exp)
