@@ -409,7 +409,10 @@ def run_ours(args):
         ctx.profile(False)
         ctx.set_stream(stream.cuda_stream)
         return {"value": ws * W * H * k / t / 1e6, "unit": "Mpix/s", "h2d_bytes_per_step": W * H * 2,
-                "d2h_bytes_per_step": W * H * 12, "copy_ms_per_step": copy_ms / k}
+                "d2h_bytes_per_step": W * H * 12, "copy_marks_ms_per_step": copy_ms / k,
+                "copies": "H2D of the raw, then (plain path) the RGB result copied back band by band on a "
+                          "second stream while the next band's NLM runs; copy_marks_ms spans those streams, "
+                          "overlap included"}
 
     plain = device_timed(step_plain)
     learned = device_timed(step_learned)

@@ -186,6 +186,55 @@ int run_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h
   return DSGPU_OK;
 }
 
+// Host-buffer develop, second half: NLM in bands of tile rows on the context
+// stream, each band's rows copied to the host on the copy stream as soon as
+// the band is done (so the 12 B/px result copy overlaps the next band's NLM);
+// the clip plane is copied first. Returns when everything is in host memory.
+int nlm_bands_to_host(dsgpu_ctx* ctx, const float* mid, int w, int h, float h_param, int search, int patch,
+                      unsigned flags, const float* drgb, float* out_rgb, const float* dclip, float* out_clip) {
+  constexpr int BANDS = 8;
+  if (!ctx->copy) DS_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  while (ctx->band_ev.size() < BANDS + 1) {
+    cudaEvent_t e;
+    DS_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->band_ev.push_back(e);
+  }
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  const int bands = ty < BANDS ? ty : BANDS;
+  cudaEvent_t ca = ctx->profiling ? take_event(ctx) : nullptr, cb = ca ? take_event(ctx) : nullptr;
+  if (ca && !cb) {
+    ctx->pool.push_back(ca);
+    ca = nullptr;
+  }
+  DS_TRY(cudaEventRecord(ctx->band_ev[BANDS], ctx->stream));  // demosaic (and clip plane) done
+  DS_TRY(cudaStreamWaitEvent(ctx->copy, ctx->band_ev[BANDS], 0));
+  if (ca) DS_TRY(cudaEventRecord(ca, ctx->copy));
+  if (out_clip)
+    DS_TRY(cudaMemcpyAsync(out_clip, dclip, (size_t)w * h * sizeof(float), cudaMemcpyDeviceToHost, ctx->copy));
+  {
+    StageMark mark(ctx, DSGPU_STAGE_NLM);
+    for (int b = 0; b < bands; b++) {
+      const int t0 = (int)((long long)ty * b / bands), t1 = (int)((long long)ty * (b + 1) / bands);
+      DS_TRY(ds_launch_nlm_rows(ctx->stream, mid, w, h, 3, h_param, search, patch, t0, t1, (float*)drgb,
+                                (flags & DSGPU_FP16_STAGING) != 0));
+      ctx->launches += 1;
+      DS_TRY(cudaEventRecord(ctx->band_ev[b], ctx->stream));
+      DS_TRY(cudaStreamWaitEvent(ctx->copy, ctx->band_ev[b], 0));
+      const size_t r0 = (size_t)t0 * th, r1 = (size_t)t1 * th < (size_t)h ? (size_t)t1 * th : (size_t)h;
+      const size_t row = (size_t)w * 3;
+      DS_TRY(cudaMemcpyAsync(out_rgb + r0 * row, drgb + r0 * row, (r1 - r0) * row * sizeof(float),
+                             cudaMemcpyDeviceToHost, ctx->copy));
+    }
+  }
+  if (cb) {
+    DS_TRY(cudaEventRecord(cb, ctx->copy));
+    ctx->marks.push_back({DSGPU_STAGE_COPY, ca, cb});
+  }
+  DS_TRY(cudaStreamSynchronize(ctx->copy));
+  return DSGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -245,6 +294,8 @@ int dsgpu_destroy(dsgpu_ctx* ctx) {
   }
   for (auto e : ctx->pool) cudaEventDestroy(e);
   ds_batch_free(ctx->batch);
+  for (auto e : ctx->band_ev) cudaEventDestroy(e);
+  if (ctx->copy) cudaStreamDestroy(ctx->copy);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return DSGPU_OK;
@@ -531,6 +582,9 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
     DS_TRY(ds_launch_highlights(ctx->stream, (float*)mid, hl_clip, w, h, mul, hl_rc, hl_work, &launches));
     ctx->launches += 2 + launches;
   }
+  if ((flags & DSGPU_HOST) && search > 0)  // overlap the result's copy to the host with NLM
+    return nlm_bands_to_host(ctx, (const float*)mid, w, h, h_param, search, patch, flags, (const float*)drgb,
+                             out_rgb, (const float*)dclip, out_clip);
   DS_CHECK(run_nlm(ctx, (const float*)mid, w, h, 3, h_param, search, patch, (float*)drgb, flags));
   return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));
 }

@@ -28,6 +28,8 @@ struct dsgpu_ctx {
   std::vector<ds_mark> marks;       // stage events recorded while profiling
   std::vector<cudaEvent_t> pool;    // idle events
   DsBatch* batch = nullptr;         // batched develop: descriptors, graph, autotune table
+  cudaStream_t copy = nullptr;      // host-buffer calls: device-to-host copies overlapping compute
+  std::vector<cudaEvent_t> band_ev; // one per band of a pipelined call
 };
 
 // Makes ctx->device current for the duration of a call and restores the

@@ -87,6 +87,8 @@ cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int ch
 cudaError_t ds_launch_nlm_dev_h(cudaStream_t st, const float* in, int w, int h, int channels, const float* h_dev,
                                 int search, int patch, float* out);
 void ds_nlm_tile_grid(int w, int h, int patch, int* tiles_x, int* tiles_y, int* tile_w, int* tile_h);
+cudaError_t ds_launch_nlm_rows(cudaStream_t st, const float* in, int w, int h, int channels, float h_param,
+                               int search, int patch, int ty0, int ty1, float* out, bool fp16_staging);
 cudaError_t ds_launch_nlm_tiles(cudaStream_t st, const float* in, int w, int h, int channels, float h_param,
                                 int search, int patch, const unsigned char* flags, float* out);
 // denoise composite (enhance.rs:75-92) and its parts

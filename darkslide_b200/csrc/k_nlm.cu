@@ -255,15 +255,16 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* _
                                                                   int S, float sigma, const float* __restrict__ h_dev,
                                                                   float norm2_log2e,
                                                                   const unsigned char* __restrict__ tile_flags,
-                                                                  float* __restrict__ out) {
+                                                                  float* __restrict__ out, int ty0) {
+  const int ty = blockIdx.y + ty0;  // tile row (a launch may cover a band of tile rows)
   // tile-list mode (the learned path's fallback): only flagged tiles run
-  if (tile_flags && !tile_flags[blockIdx.y * gridDim.x + blockIdx.x]) return;
+  if (tile_flags && !tile_flags[ty * gridDim.x + blockIdx.x]) return;
   if (h_dev) {  // strength computed on the device (enhance.rs:40 floor included)
     const float hh = *h_dev;
     sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
   }
   extern __shared__ float4 smem4[];
-  nlm_tile<P, F16>(in, W, H, C, S, sigma, out, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float*>(smem4));
+  nlm_tile<P, F16>(in, W, H, C, S, sigma, out, blockIdx.x, ty, blockIdx.z, reinterpret_cast<float*>(smem4));
 }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -315,16 +316,22 @@ cudaError_t launch_nlm_batch_p(cudaStream_t st, const ds_batch_frame* frames, in
   return cudaGetLastError();
 }
 
+// tile rows [ty0, ty1) (ty1 < 0: to the last)
 template <int P, bool F16>
 cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, int S, float sigma,
-                         const float* h_dev, float norm2_log2e, const unsigned char* flags, float* out) {
+                         const float* h_dev, float norm2_log2e, const unsigned char* flags, float* out, int ty0,
+                         int ty1) {
   constexpr int TY = HRW - 2 * P;
+  const int tiles_y = (h + TY - 1) / TY;
+  if (ty1 < 0 || ty1 > tiles_y) ty1 = tiles_y;
+  if (ty0 >= ty1) return cudaSuccess;
   const size_t smem = nlm_smem_bytes(S, P, F16);
   cudaError_t e =
       cudaFuncSetAttribute(nlm_tile_kernel<P, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((w + TX - 1) / TX, (h + TY - 1) / TY, C);
-  nlm_tile_kernel<P, F16><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags, out);
+  dim3 grid((w + TX - 1) / TX, ty1 - ty0, C);
+  nlm_tile_kernel<P, F16><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags, out,
+                                                            ty0);
   return cudaGetLastError();
 }
 
@@ -334,26 +341,27 @@ namespace {
 
 template <bool F16>
 cudaError_t dispatch_nlm_t(cudaStream_t st, const float* in, int w, int h, int C, int S, int P, float sigma,
-                           const float* h_dev, float* out, const unsigned char* flags) {
+                           const float* h_dev, float* out, const unsigned char* flags, int ty0, int ty1) {
   const float norm = P == 0 ? 1.0f : 1.0f / (float)(2 * P + 1);
   const float n2l = norm * norm * 1.4426950408889634f;
   switch (P) {
-    case 0: return launch_nlm_p<0, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 1: return launch_nlm_p<1, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 2: return launch_nlm_p<2, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 3: return launch_nlm_p<3, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 4: return launch_nlm_p<4, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 5: return launch_nlm_p<5, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 6: return launch_nlm_p<6, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
-    case 7: return launch_nlm_p<7, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out);
+    case 0: return launch_nlm_p<0, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
+    case 1: return launch_nlm_p<1, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
+    case 2: return launch_nlm_p<2, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
+    case 3: return launch_nlm_p<3, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
+    case 4: return launch_nlm_p<4, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
+    case 5: return launch_nlm_p<5, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
+    case 6: return launch_nlm_p<6, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
+    case 7: return launch_nlm_p<7, F16>(st, in, w, h, C, S, sigma, h_dev, n2l, flags, out, ty0, ty1);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t dispatch_nlm(cudaStream_t st, const float* in, int w, int h, int C, int S, int P, float sigma,
-                         const float* h_dev, float* out, const unsigned char* flags = nullptr, bool f16 = false) {
-  return f16 ? dispatch_nlm_t<true>(st, in, w, h, C, S, P, sigma, h_dev, out, flags)
-             : dispatch_nlm_t<false>(st, in, w, h, C, S, P, sigma, h_dev, out, flags);
+                         const float* h_dev, float* out, const unsigned char* flags = nullptr, bool f16 = false,
+                         int ty0 = 0, int ty1 = -1) {
+  return f16 ? dispatch_nlm_t<true>(st, in, w, h, C, S, P, sigma, h_dev, out, flags, ty0, ty1)
+             : dispatch_nlm_t<false>(st, in, w, h, C, S, P, sigma, h_dev, out, flags, ty0, ty1);
 }
 
 }  // namespace
@@ -370,6 +378,14 @@ cudaError_t ds_launch_nlm(cudaStream_t st, const float* in, int w, int h, int ch
   const float norm = patch == 0 ? 1.0f : 1.0f / (float)(2 * patch + 1);
   const double sig2 = (double)norm * (double)norm / (double)h2 * 1.4426950408889634;
   return dispatch_nlm(st, in, w, h, channels, search, patch, (float)sqrt(sig2), nullptr, out, nullptr, fp16_staging);
+}
+
+// NLM of the tile rows [ty0, ty1) only (the rows ty0*(64-2P) .. of the output)
+cudaError_t ds_launch_nlm_rows(cudaStream_t st, const float* in, int w, int h, int channels, float h_param,
+                               int search, int patch, int ty0, int ty1, float* out, bool fp16_staging) {
+  if (search <= 0) return cudaErrorInvalidValue;
+  return dispatch_nlm(st, in, w, h, channels, search, patch, ds_nlm_sigma(h_param, patch), nullptr, out, nullptr,
+                      fp16_staging, ty0, ty1);
 }
 
 // NLM tile geometry (the fallback's flag grid): tiles_x x tiles_y of 64 x (64 - 2P)

@@ -296,3 +296,22 @@ def test_row_band_split_on_gpu(ctx):
         # bands place the NLM tiles differently, which changes the order of
         # the FMA sums: equal to ~20 ulps
         assert np.abs(got - full).max() <= 1e-5
+
+
+@pytest.mark.parametrize("hw", [(4000, 600), (37, 1201), (64, 58)])
+def test_develop_host_buffers_equal_device_path(ctx, hw):
+    """With host buffers the develop call runs NLM in bands of tile rows and
+    copies each band back while the next one computes; the result must equal
+    the device-buffer call bit for bit (RGB and clip plane)."""
+    import torch
+
+    w, h = hw
+    sc = ds.Scene(seed=9, w=w, h=h, pattern=ds.GRBG, black=512, white=16383, gain=0.5, read_sigma=6)
+    raw = sc.render_host()
+    white = [16383.0] * 3
+    mul = [2.0, 1.0, 1.0 / 0.7]
+    host, hclip = ds.develop_u16(raw, ds.GRBG, 512, white, mul, 0.02, 10, 3, with_clip=True, ctx=ctx)
+    dev_img, dclip = ds.develop_u16(torch.from_numpy(raw).cuda(), ds.GRBG, 512, white, mul, 0.02, 10, 3,
+                                    with_clip=True, ctx=ctx)
+    np.testing.assert_array_equal(host.data, dev_img.data.cpu().numpy())
+    np.testing.assert_array_equal(hclip.data, dclip.data.cpu().numpy())
