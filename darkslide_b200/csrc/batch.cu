@@ -1,10 +1,11 @@
 // Batched develop (dsgpu_rcd_nlm_batch) and the tile-shape autotuner.
 //
-// A batch is n frames of any sizes, CFA layouts, levels and strengths. Their
-// tiles are numbered consecutively (frame-major), and one CUDA graph runs
-//   descriptor upload (pinned host -> device) -> zero the per-frame tile
-//   counters -> start stamp -> persistent RCD kernel over every frame's RCD
-//   tiles -> persistent NLM kernel over every frame's NLM tiles
+// A batch is n frames of any sizes, CFA layouts, levels and strengths. One
+// CUDA graph runs
+//   descriptor and work-queue upload (pinned host -> device) -> zero the
+//   counters -> start stamp -> ONE persistent kernel that takes the RCD and
+//   NLM tiles of every frame from a work queue ordered RCD(0), RCD(1),
+//   NLM(0), RCD(2), NLM(1), ... (batch_fused_kernel, k_demosaic.cu)
 // on the context stream (captured on a private stream, since capture is not
 // allowed on the legacy default stream). The NLM kernel stamps the device clock when a
 // frame's last tile finishes, which gives the per-frame completion times.
@@ -13,8 +14,8 @@
 // same layout (pointers, levels, strengths) goes through the descriptors.
 //
 // RCD tile shape per frame: from the context's autotune table, filled by
-// dsgpu_autotune (timings of the batched kernels on synthetic frames of each
-// size class). Every shape produces the same output bit for bit, so the
+// dsgpu_autotune (timings of the separate batched RCD and NLM kernels on
+// synthetic frames of each size class). Every shape produces the same output bit for bit, so the
 // table changes speed only.
 #include <cstring>
 #include <vector>
@@ -45,7 +46,11 @@ constexpr int DEFAULT_NLM_PER_SM = 2;  // the NLM kernel's occupancy limit
 struct DsBatch {
   ds_batch_frame* d_frames = nullptr;
   ds_batch_frame* h_frames = nullptr;      // pinned: the graph's upload source
-  unsigned* d_done = nullptr;              // NLM tiles finished per frame
+  unsigned* d_done = nullptr;              // NLM tiles finished per frame (the tuner's NLM runs)
+  ds_batch_seg* d_segs = nullptr;          // work queue of the fused kernel
+  ds_batch_seg* h_segs = nullptr;          // pinned
+  int* d_ctr = nullptr;                    // fused-kernel counters (see ds_batch_ctr_nlm)
+  int* h_status = nullptr;                 // pinned copy of the status word
   unsigned long long* d_stamps = nullptr;  // [0] batch start, [1 + f] frame f done (device ns)
   unsigned long long* h_stamps = nullptr;  // pinned
   cudaEvent_t done_ev = nullptr;           // after the last launched batch
@@ -64,6 +69,10 @@ void ds_batch_free(DsBatch* b) {
   if (b->cap) cudaStreamDestroy(b->cap);
   cudaFree(b->d_frames);
   cudaFree(b->d_done);
+  cudaFree(b->d_segs);
+  cudaFree(b->d_ctr);
+  cudaFreeHost(b->h_segs);
+  cudaFreeHost(b->h_status);
   cudaFree(b->d_stamps);
   cudaFreeHost(b->h_frames);
   cudaFreeHost(b->h_stamps);
@@ -79,6 +88,11 @@ int batch_state(dsgpu_ctx* ctx, DsBatch** out) {
     cudaError_t e = cudaMalloc(&b->d_frames, DSGPU_BATCH_MAX * sizeof(ds_batch_frame));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_done, DSGPU_BATCH_MAX * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_stamps, (DSGPU_BATCH_MAX + 1) * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_segs, 2 * DSGPU_BATCH_MAX * sizeof(ds_batch_seg));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ctr, ds_batch_ctr_nlm(DSGPU_BATCH_MAX) * sizeof(int) +
+                                                        DSGPU_BATCH_MAX * sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_segs, 2 * DSGPU_BATCH_MAX * sizeof(ds_batch_seg));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_status, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_frames, DSGPU_BATCH_MAX * sizeof(ds_batch_frame));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_stamps, (DSGPU_BATCH_MAX + 1) * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done_ev, cudaEventDisableTiming);
@@ -137,8 +151,9 @@ void describe(ds_batch_frame& d, const dsgpu_frame& fr, ds_pat pat, int shape, i
   d.out = fr.out_rgb;
   d.rcd_shape = shape;
   d.rcd_tiles_x = (fr.w + tw - 1) / tw;
+  d.rcd_tiles = d.rcd_tiles_x * ((fr.h + th - 1) / th);
   d.rcd_tile0 = *rcd_total;
-  *rcd_total += d.rcd_tiles_x * ((fr.h + th - 1) / th);
+  *rcd_total += d.rcd_tiles;
   int tx, ty, ntw, nth;
   ds_nlm_tile_grid(fr.w, fr.h, patch, &tx, &ty, &ntw, &nth);
   d.nlm_tiles_x = tx;
@@ -204,6 +219,18 @@ int dsgpu_rcd_nlm_batch(dsgpu_ctx* ctx, const dsgpu_frame* frames, int n, int se
     sig.push_back(frames[i].h);
     sig.push_back(shape);
   }
+  // the fused kernel's work queue: RCD(0), RCD(1), NLM(0), RCD(2), NLM(1), ..., NLM(n-1)
+  int nseg = 0, item = 0;
+  auto push = [&](int kind, int f) {
+    const ds_batch_frame& d = b->h_frames[f];
+    b->h_segs[nseg++] = ds_batch_seg{kind, f, item};
+    item += kind == 0 ? d.rcd_tiles : d.nlm_tiles_x * d.nlm_tiles_y * 3;
+  };
+  for (int f = 0; f < n; f++) {
+    push(0, f);
+    if (f > 0) push(1, f - 1);
+  }
+  push(1, n - 1);
   if (!b->exec || sig != b->sig) {
     if (b->exec) {
       cudaGraphExecDestroy(b->exec);
@@ -213,12 +240,14 @@ int dsgpu_rcd_nlm_batch(dsgpu_ctx* ctx, const dsgpu_frame* frames, int n, int se
     cudaStream_t st = b->cap;  // captured here, launched on the context stream
     DS_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaMemcpyAsync(b->d_frames, b->h_frames, n * sizeof(ds_batch_frame), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_done, 0, n * sizeof(unsigned), st);
-    if (e == cudaSuccess) e = ds_launch_stamp(st, b->d_stamps);
-    if (e == cudaSuccess) e = ds_launch_rcd_batch(st, b->d_frames, n, rcd_total, 2 * sms);
     if (e == cudaSuccess)
-      e = ds_launch_nlm_batch(st, b->d_frames, n, nlm_total, search, patch, nlm_per_sm * sms, b->d_done,
-                              b->d_stamps + 1);
+      e = cudaMemcpyAsync(b->d_segs, b->h_segs, nseg * sizeof(ds_batch_seg), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(b->d_ctr, 0, ds_batch_ctr_nlm(DSGPU_BATCH_MAX) * sizeof(int) + n * sizeof(int), st);
+    if (e == cudaSuccess) e = ds_launch_stamp(st, b->d_stamps);
+    if (e == cudaSuccess)
+      e = ds_launch_batch_fused(st, b->d_frames, n, b->d_segs, nseg, rcd_total + nlm_total, search, patch,
+                                nlm_per_sm * sms, b->d_ctr, DSGPU_BATCH_MAX, b->d_stamps + 1);
     cudaGraph_t graph = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
     if (e == cudaSuccess) e = e2;
@@ -234,8 +263,13 @@ int dsgpu_rcd_nlm_batch(dsgpu_ctx* ctx, const dsgpu_frame* frames, int n, int se
   DS_TRY(cudaEventRecord(b->done_ev, ctx->stream));
   b->in_flight = true;
   b->last_n = n;
-  ctx->launches += 3;
-  if (!(flags & DSGPU_ASYNC)) DS_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->launches += 2;
+  if (!(flags & DSGPU_ASYNC)) {
+    DS_TRY(cudaMemcpyAsync(b->h_status, b->d_ctr + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    DS_TRY(cudaStreamSynchronize(ctx->stream));
+    b->in_flight = false;
+    if (*b->h_status != 0) return *b->h_status;  // a tile waited in vain for its frame's demosaic
+  }
   return DSGPU_OK;
 }
 
@@ -248,6 +282,8 @@ int dsgpu_batch_frame_ms(dsgpu_ctx* ctx, double* frame_ms, int n) {
   DS_TRY(cudaEventSynchronize(b->done_ev));
   b->in_flight = false;
   DS_TRY(cudaMemcpy(b->h_stamps, b->d_stamps, (b->last_n + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  DS_TRY(cudaMemcpy(b->h_status, b->d_ctr + 1, sizeof(int), cudaMemcpyDeviceToHost));
+  if (*b->h_status != 0) return *b->h_status;  // the batch stopped early: no valid times
   for (int i = 0; i < n; i++) frame_ms[i] = (double)(long long)(b->h_stamps[1 + i] - b->h_stamps[0]) * 1e-6;
   return DSGPU_OK;
 }

@@ -43,10 +43,24 @@ struct ds_batch_frame {
   float* out;       // NLM output, w*h*3
   int rcd_shape;    // index into the RCD tile shapes (ds_rcd_batch_shape)
   int rcd_tiles_x;
+  int rcd_tiles;    // RCD tiles of this frame
   int rcd_tile0;
   int nlm_tiles_x, nlm_tiles_y;
   int nlm_tile0;
 };
+
+// A run of work items of the fused batch kernel: the RCD (kind 0) or NLM
+// (kind 1) tiles of one frame, items [start, next segment's start).
+struct ds_batch_seg {
+  int kind, frame, start;
+};
+// Counters of the fused kernel: [0] next work item, [1] status, then the
+// RCD and NLM tiles finished per frame.
+constexpr int DS_BATCH_CTR_RCD = 2;
+inline int ds_batch_ctr_nlm(int max_frames) { return DS_BATCH_CTR_RCD + max_frames; }
+cudaError_t ds_launch_batch_fused(cudaStream_t st, const ds_batch_frame* frames, int n, const ds_batch_seg* segs,
+                                  int nseg, int total_items, int search, int patch, int grid, int* counters,
+                                  int max_frames, unsigned long long* stamps);
 
 // batched kernels: one persistent launch each over all frames' tiles
 constexpr int DS_RCD_SHAPES = 5;

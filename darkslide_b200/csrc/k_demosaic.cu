@@ -7,6 +7,7 @@
 #include <cfloat>
 
 #include "internal.cuh"
+#include "nlm_tile.cuh"
 
 namespace {
 
@@ -568,6 +569,108 @@ __global__ void hl_apply_kernel(float* __restrict__ img, const float* __restrict
   for (int c = 0; c < 3; c++) img[3 * i + c] = p[c] + (top - p[c]) * t * 0.5f;
 }
 
+__device__ __forceinline__ unsigned long long batch_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// The whole batch in one persistent launch: CTAs take work items from a
+// global counter in queue order RCD(0), RCD(1), NLM(0), RCD(2), NLM(1), ...,
+// so a frame's NLM starts right after its demosaic (per-frame latency) while
+// the next frame's demosaic is in flight. An NLM tile first waits, bounded by
+// 2 s of device clock, until its frame's RCD tiles are all done; items are
+// taken in queue order by resident CTAs and RCD items never wait, so the wait
+// always ends unless a tile failed, in which case counters[1] gets
+// DSGPU_ERR_TIMEOUT and the CTA stops. When a frame's last NLM tile is done,
+// stamps[f] = the device clock. The tile bodies are those of the one-frame
+// kernels, so every frame's output equals the one-frame path's bit for bit.
+template <int P>
+__global__ void __launch_bounds__(RCD_THREADS, 2) batch_fused_kernel(const ds_batch_frame* __restrict__ frames,
+                                                                     int n, const ds_batch_seg* __restrict__ segs,
+                                                                     int nseg, int total, int S, int* counters,
+                                                                     int max_frames,
+                                                                     unsigned long long* __restrict__ stamps) {
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  __shared__ int item, go;
+  unsigned* rcd_done = reinterpret_cast<unsigned*>(counters + DS_BATCH_CTR_RCD);
+  unsigned* nlm_done = reinterpret_cast<unsigned*>(counters + DS_BATCH_CTR_RCD + max_frames);
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) item = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    const int t = item;
+    if (t >= total) break;
+    int lo = 0, hi = nseg - 1;  // the segment holding item t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (segs[mid].start <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const ds_batch_seg sg = segs[lo];
+    const ds_batch_frame& F = frames[sg.frame];
+    const int local = t - sg.start;
+    if (sg.kind == 0) {
+      const int ty = local / F.rcd_tiles_x, tx = local - ty * F.rcd_tiles_x;
+      const SrcU16 src{F.src};
+      switch (F.rcd_shape) {
+        case 0: rcd_tile<SrcU16, 32, 32>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+        case 1: rcd_tile<SrcU16, 64, 16>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+        case 2: rcd_tile<SrcU16, 48, 24>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+        case 3: rcd_tile<SrcU16, 24, 48>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+        default: rcd_tile<SrcU16, 16, 64>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();  // the tile's output before its count
+        atomicAdd(&rcd_done[sg.frame], 1u);
+      }
+    } else {
+      if (tid == 0) {
+        const unsigned need = (unsigned)F.rcd_tiles;
+        const unsigned long long t0 = batch_clock_ns();
+        int ok = 1;
+        while ((unsigned)atomicAdd(&rcd_done[sg.frame], 0u) < need) {
+          if (batch_clock_ns() - t0 > 2000000000ull) {
+            ok = 0;
+            atomicExch(&counters[1], DSGPU_ERR_TIMEOUT);
+            break;
+          }
+          __nanosleep(200);
+        }
+        __threadfence();  // the frame's demosaiced pixels before the tile reads them
+        go = ok;
+      }
+      __syncthreads();
+      if (!go) break;
+      const int per = F.nlm_tiles_x * F.nlm_tiles_y;
+      const int ch = local / per, r = local - ch * per;
+      const int ty = r / F.nlm_tiles_x, tx = r - ty * F.nlm_tiles_x;
+      nlmk::nlm_tile<P>(F.rgb, F.w, F.h, 3, S, F.sigma, F.out, tx, ty, ch, smem);
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&nlm_done[sg.frame], 1u) + 1u == (unsigned)(3 * per)) stamps[sg.frame] = batch_clock_ns();
+      }
+    }
+    __syncthreads();  // every thread has read `item` and is done with shared memory
+  }
+}
+
+template <int P>
+cudaError_t launch_batch_fused_p(cudaStream_t st, const ds_batch_frame* frames, int n, const ds_batch_seg* segs,
+                                 int nseg, int total, int S, int grid, int* counters, int max_frames,
+                                 unsigned long long* stamps) {
+  const size_t nlm = nlmk::nlm_smem_bytes(S, P);
+  const size_t smem = nlm > RCD_BATCH_SMEM ? nlm : RCD_BATCH_SMEM;
+  cudaError_t e = cudaFuncSetAttribute(batch_fused_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  batch_fused_kernel<P><<<grid, RCD_THREADS, smem, st>>>(frames, n, segs, nseg, total, S, counters, max_frames,
+                                                         stamps);
+  return cudaGetLastError();
+}
+
 template <class Src>
 cudaError_t launch_rcd(cudaStream_t st, Src src, int w, int h, ds_pat pat, const float mul[3], float* out_rgb,
                        float* out_clip) {
@@ -779,4 +882,23 @@ cudaError_t ds_launch_orientation(cudaStream_t st, const float* in, int w, int h
   dim3 grid((ow + 31) / 32, (oh + 31) / 32);
   orient_kernel<<<grid, dim3(32, 8), 0, st>>>(in, w, h, o, ow, oh, out);
   return cudaGetLastError();
+}
+
+cudaError_t ds_launch_batch_fused(cudaStream_t st, const ds_batch_frame* frames, int n, const ds_batch_seg* segs,
+                                  int nseg, int total_items, int search, int patch, int grid, int* counters,
+                                  int max_frames, unsigned long long* stamps) {
+  if (n <= 0 || total_items <= 0) return cudaSuccess;
+  if (search <= 0 || search > DSGPU_NLM_MAX_SEARCH) return cudaErrorInvalidValue;
+  static_assert(nlmk::NLM_THREADS == RCD_THREADS, "one block size for both tile bodies");
+  switch (patch) {
+    case 0: return launch_batch_fused_p<0>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    case 1: return launch_batch_fused_p<1>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    case 2: return launch_batch_fused_p<2>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    case 3: return launch_batch_fused_p<3>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    case 4: return launch_batch_fused_p<4>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    case 5: return launch_batch_fused_p<5>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    case 6: return launch_batch_fused_p<6>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    case 7: return launch_batch_fused_p<7>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
+    default: return cudaErrorInvalidValue;
+  }
 }

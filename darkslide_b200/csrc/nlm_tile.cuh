@@ -1,0 +1,226 @@
+// The NLM tile body (enhance.rs:36-72) shared by the one-frame kernels
+// (k_nlm.cu) and the fused batch kernel (k_demosaic.cu); the design notes are
+// at the top of k_nlm.cu. Everything here has internal linkage.
+#pragma once
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
+#include "internal.cuh"
+
+namespace {
+namespace nlmk {
+
+constexpr int NLM_THREADS = 256;
+constexpr int TX = 64;   // tile width
+constexpr int HRW = 64;  // H rows per offset (TY + 2P)
+constexpr int SEG = 16;  // phase-A segment width
+constexpr int HP = TX + 1;  // odd H pitch
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ float ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+constexpr int HBR = HRW + 4;  // H rows allocated: phase B of the last quarter reads past row 63
+
+// Plane pitch: odd and fixed per P (sized for the largest search radius) so
+// that every shared address offset is a compile-time constant.
+__host__ __device__ constexpr int nlm_pitch(int P) { return (TX + 2 * (DSGPU_NLM_MAX_SEARCH + P + 1)) | 1; }
+
+struct NlmGeom {
+  int R, PW, PH, PHA;  // halo, region width, region height, allocated rows
+};
+
+__host__ __device__ inline NlmGeom nlm_geom(int S, int P) {
+  NlmGeom g;
+  const int TY = HRW - 2 * P;
+  g.R = S + P + 1;
+  g.PW = TX + 2 * g.R;
+  g.PH = TY + 2 * g.R;
+  g.PHA = g.PH + 4;  // phase B of the last quarter reads up to 3 rows past the region
+  return g;
+}
+
+// plane bytes (f32, or f16 when staged in half precision), rounded to 16
+size_t nlm_plane_bytes(int S, int P, bool f16) {
+  const NlmGeom g = nlm_geom(S, P);
+  return ((size_t)nlm_pitch(P) * g.PHA * (f16 ? 2 : 4) + 15) / 16 * 16;
+}
+
+size_t nlm_smem_bytes(int S, int P, bool f16 = false) {
+  return nlm_plane_bytes(S, P, f16) + (size_t)4 * HBR * HP * sizeof(float);
+}
+
+__device__ __forceinline__ float ldp(const float* p) { return *p; }
+__device__ __forceinline__ float ldp(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ void stp(float* p, float v) { *p = v; }
+__device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v); }
+
+// One 64 x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
+// image; smem holds nlm_smem_bytes(S, P, F16) bytes.
+// F16 (the precision variant): the pre-scaled plane is staged in half
+// precision, centred on the tile's centre sample (NLM weights depend only on
+// differences, so the offset costs nothing there and keeps the half-precision
+// error of the staged values small; it is added back to the result), while
+// distances, weights and sums stay in FP32 and the weight sum (the
+// normalisation) is accumulated with Kahan compensation.
+template <int P, bool F16 = false>
+__device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
+                                         float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
+  using T = typename std::conditional<F16, __half, float>::type;
+  constexpr int TY = HRW - 2 * P;
+  constexpr int DW = SEG + 2 * P;  // differences per phase-A segment
+  constexpr int RB = (TY + 3) / 4; // phase-B rows per thread (a quarter of the tile)
+  constexpr int PP = nlm_pitch(P);
+  const NlmGeom g = nlm_geom(S, P);
+  T* PL = reinterpret_cast<T*>(smem);  // scaled plane, pitch PP
+  float* HB = reinterpret_cast<float*>(reinterpret_cast<char*>(smem) +
+                                       ((size_t)PP * g.PHA * sizeof(T) + 15) / 16 * 16);  // 4 offsets x HBR rows x HP
+
+  const int X0 = tile_x * TX, Y0 = tile_y * TY;
+  const int tid = threadIdx.x;
+  const int ox0 = X0 - g.R, oy0 = Y0 - g.R;  // global site of plane (0,0)
+
+  float off = 0.f;  // F16: the tile's centre sample
+  if (F16) off = in[((size_t)clampi(Y0 + TY / 2, 0, H - 1) * W + clampi(X0 + TX / 2, 0, W - 1)) * C + ch];
+  for (int i = tid; i < g.PW * g.PH; i += NLM_THREADS) {
+    const int ly = i / g.PW, lx = i - ly * g.PW;
+    const int gx = clampi(ox0 + lx, 0, W - 1), gy = clampi(oy0 + ly, 0, H - 1);
+    const float v = in[((size_t)gy * W + gx) * C + ch];
+    stp(&PL[ly * PP + lx], F16 ? (v - off) * sigma : v * sigma);
+  }
+  for (int i = tid; i < (g.PHA - g.PH) * PP; i += NLM_THREADS) stp(&PL[g.PH * PP + i], 0.f);
+
+  // ---- phase-A role: H row `arow` (tile row arow - P), segment at ax0
+  const int arow = tid & (HRW - 1);
+  const int ax0 = (tid >> 6) * SEG;
+  const int aprow = clampi(Y0 + arow - P, 0, H - 1) - oy0;  // plane row of the clamped H row
+  const bool xin = (X0 - P >= 0) && (X0 + TX + P <= W);
+  const int acol0 = ax0 - P + g.R;  // plane column of difference 0 (interior tiles)
+  // ---- phase-B role: column bcol, rows [brow0, brow0 + RB) (clipped to TY)
+  const int bcol = tid & (TX - 1);
+  const int brow0 = (tid >> 6) * RB;
+
+  __syncthreads();
+  float pv[DW];  // centre samples of this thread's phase-A segment
+#pragma unroll
+  for (int k = 0; k < DW; k++) {
+    const int col = xin ? acol0 + k : clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
+    pv[k] = ldp(&PL[aprow * PP + col]);
+  }
+  float a[RB], s[RB], cs[F16 ? RB : 1];  // cs: Kahan compensation of s (F16)
+#pragma unroll
+  for (int r = 0; r < RB; r++) {
+    a[r] = 0.f;
+    s[r] = 0.f;
+    if (F16) cs[r] = 0.f;
+  }
+
+  // One 2x2 block of offsets {dx0, dx0+1} x {dy0, dy0+NJ-1}.
+  auto block = [&](int dx0, int dy0, auto nj_tag) {
+    constexpr int NJ = decltype(nj_tag)::value;
+    // phase A: horizontal sums, stored NEGATED (-sum d^2) so that phase B's
+    // vertical sum is the ex2 argument itself
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+      const T* qrow = PL + (aprow + dy0 + j) * PP + dx0;
+      float d0[DW], d1[DW];
+      if (xin) {
+        float q[DW + 1];
+#pragma unroll
+        for (int k = 0; k <= DW; k++) q[k] = ldp(&qrow[acol0 + k]);
+#pragma unroll
+        for (int k = 0; k < DW; k++) {
+          d0[k] = pv[k] - q[k];
+          d1[k] = pv[k] - q[k + 1];
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < DW; k++) {
+          const int col = clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
+          d0[k] = pv[k] - ldp(&qrow[col]);
+          d1[k] = pv[k] - ldp(&qrow[col + 1]);
+        }
+      }
+      float h0 = 0.f, h1 = 0.f;
+#pragma unroll
+      for (int k = 0; k <= 2 * P; k++) {
+        h0 = fmaf(-d0[k], d0[k], h0);
+        h1 = fmaf(-d1[k], d1[k], h1);
+      }
+      float* H0 = HB + (j * 2 + 0) * (HBR * HP) + arow * HP + ax0;
+      float* H1 = HB + (j * 2 + 1) * (HBR * HP) + arow * HP + ax0;
+      H0[0] = h0;
+      H1[0] = h1;
+#pragma unroll
+      for (int k = 1; k < SEG; k++) {
+        h0 = fmaf(-d0[k + 2 * P], d0[k + 2 * P], h0);
+        h0 = fmaf(d0[k - 1], d0[k - 1], h0);
+        h1 = fmaf(-d1[k + 2 * P], d1[k + 2 * P], h1);
+        h1 = fmaf(d1[k - 1], d1[k - 1], h1);
+        H0[k] = h0;
+        H1[k] = h1;
+      }
+    }
+    __syncthreads();
+    // phase B: vertical sums, weights, accumulation for (dx0 + i, dy0 + j)
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      if (dx0 + i <= S) {  // false only for the dx tail of an odd search width
+        const T* qc = PL + (brow0 + g.R + dy0) * PP + bcol + g.R + dx0 + i;
+        float qv[RB + NJ - 1];
+#pragma unroll
+        for (int r = 0; r < RB + NJ - 1; r++) qv[r] = ldp(&qc[r * PP]);
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+          const float* hc = HB + (j * 2 + i) * (HBR * HP) + brow0 * HP + bcol;
+          float hv[RB + 2 * P];
+#pragma unroll
+          for (int r = 0; r < RB + 2 * P; r++) hv[r] = hc[r * HP];
+          float v = 0.f;
+#pragma unroll
+          for (int r = 0; r <= 2 * P; r++) v += hv[r];
+#pragma unroll
+          for (int r = 0; r < RB; r++) {
+            if (r > 0) v = v + hv[r + 2 * P] - hv[r - 1];
+            const float wgt = ex2(v);
+            a[r] = fmaf(wgt, qv[r + j], a[r]);
+            if (F16) {  // Kahan: s[r] + cs[r] carries the sum of weights
+              const float y = wgt - cs[r];
+              const float t = s[r] + y;
+              cs[r] = (t - s[r]) - y;
+              s[r] = t;
+            } else {
+              s[r] += wgt;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  };
+
+  int dy0 = -S;
+  for (; dy0 + 1 <= S; dy0 += 2)
+    for (int dx0 = -S; dx0 <= S; dx0 += 2) block(dx0, dy0, std::integral_constant<int, 2>{});
+  if (dy0 <= S)  // the dy tail of an odd search width
+    for (int dx0 = -S; dx0 <= S; dx0 += 2) block(dx0, dy0, std::integral_constant<int, 1>{});
+
+  const float inv_sigma = 1.0f / sigma;
+#pragma unroll
+  for (int r = 0; r < RB; r++) {
+    const int y = brow0 + r;
+    const int gx = X0 + bcol, gy = Y0 + y;
+    if (y < TY && gx < W && gy < H) {
+      const float o = __fdiv_rn(a[r] * inv_sigma, fmaxf(F16 ? s[r] - cs[r] : s[r], 1e-12f));
+      out[((size_t)gy * W + gx) * C + ch] = F16 ? o + off : o;
+    }
+  }
+}
+
+}  // namespace nlmk
+}  // namespace

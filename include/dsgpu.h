@@ -223,10 +223,11 @@ int dsgpu_develop_u16_noalloc(void* cuda_stream, const uint16_t* raw, int w, int
 /* ------------------------------------------------------------ batched develop
  * The survey's dsgpu_rcd_nlm_batch: many frames of different sizes, CFA
  * layouts, levels and strengths through dsgpu_develop_u16's path in one
- * CUDA graph launch that holds one persistent RCD kernel and one persistent
- * NLM kernel over the tiles of all frames (the reference develops one frame
- * per call, pipeline/mod.rs:172-252). Each frame's output equals
- * dsgpu_develop_u16's on the same frame bit for bit. */
+ * CUDA graph launch holding ONE persistent kernel that takes the RCD and NLM
+ * tiles of every frame from a work queue (a frame's NLM starts right after
+ * its demosaic; the reference develops one frame per call,
+ * pipeline/mod.rs:172-252). Each frame's output equals dsgpu_develop_u16's
+ * on the same frame bit for bit. */
 typedef struct dsgpu_frame {
   const uint16_t* raw;  /* device, h rows of pitch_elems */
   size_t pitch_elems;
@@ -248,7 +249,8 @@ typedef struct dsgpu_frame {
  * from the context's autotune table (dsgpu_autotune), else 32 x 32. */
 int dsgpu_rcd_nlm_batch(dsgpu_ctx* ctx, const dsgpu_frame* frames, int n, int search, int patch, unsigned flags);
 /* Completion time of each frame of the last batch, ms after the batch started
- * on the device (measured with the device clock; waits for the batch). */
+ * on the device (measured with the device clock; waits for the batch).
+ * Returns the batch's own status when it stopped early (DSGPU_ERR_TIMEOUT). */
 int dsgpu_batch_frame_ms(dsgpu_ctx* ctx, double* frame_ms, int n);
 /* Autotuner: for each size class (w, h) = (sizes[2i], sizes[2i+1]), time the
  * batched RCD kernel with every tile shape and the batched NLM kernel with 1
