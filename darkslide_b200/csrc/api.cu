@@ -235,6 +235,103 @@ int nlm_bands_to_host(dsgpu_ctx* ctx, const float* mid, int w, int h, float h_pa
   return DSGPU_OK;
 }
 
+// Host-buffer develop as a three-stage pipeline over row bands: the raw goes
+// up in 8 row chunks on the copy stream; RCD runs in bands of 32-row tile
+// rows on the context stream, each band waiting only for the chunks that
+// hold its rows and its 10-row halo; NLM runs in 8 bands of tile rows, each
+// after the RCD rows of its band and its S+P+1 halo; each finished NLM band
+// goes back to the host on the copy stream while the next one computes.
+// Every kernel is the one-frame kernel on a subset of its tile rows, so the
+// output equals the device-buffer call's bit for bit.
+int develop_pipelined(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t pitch, ds_pat pat, float black,
+                      const float white[3], const float mul[3], float h_param, int search, int patch, float* out_rgb,
+                      float* out_clip, unsigned flags) {
+  constexpr int CHUNKS = 8, BANDS = 8;
+  const size_t n = (size_t)w * h;
+  void *draw, *drgb, *mid, *dclip = nullptr;
+  DS_CHECK(scratch(ctx, S_IN, ((size_t)(h - 1) * pitch + w) * sizeof(uint16_t), &draw));
+  DS_CHECK(scratch(ctx, S_OUT, n * 3 * sizeof(float), &drgb));
+  DS_CHECK(scratch(ctx, S_RGB, n * 3 * sizeof(float), &mid));
+  if (out_clip) DS_CHECK(scratch(ctx, S_OUT2, n * sizeof(float), &dclip));
+  if (!ctx->copy) DS_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  while (ctx->band_ev.size() < CHUNKS + BANDS + 1) {
+    cudaEvent_t e;
+    DS_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->band_ev.push_back(e);
+  }
+  cudaEvent_t* up_ev = ctx->band_ev.data();
+  cudaEvent_t* band_ev = ctx->band_ev.data() + CHUNKS;
+  cudaEvent_t start_ev = ctx->band_ev[CHUNKS + BANDS];
+  cudaEvent_t ca = ctx->profiling ? take_event(ctx) : nullptr, cb = ca ? take_event(ctx) : nullptr;
+  if (ca && !cb) {
+    ctx->pool.push_back(ca);
+    ca = nullptr;
+  }
+  // the copy stream starts after whatever the context stream already holds
+  DS_TRY(cudaEventRecord(start_ev, ctx->stream));
+  DS_TRY(cudaStreamWaitEvent(ctx->copy, start_ev, 0));
+  if (ca) DS_TRY(cudaEventRecord(ca, ctx->copy));
+  int chunk_end[CHUNKS];  // first raw row after chunk c
+  for (int c = 0; c < CHUNKS; c++) {
+    const int r0 = (int)((long long)h * c / CHUNKS), r1 = (int)((long long)h * (c + 1) / CHUNKS);
+    chunk_end[c] = r1;
+    if (r1 > r0)
+      DS_TRY(cudaMemcpyAsync(static_cast<uint16_t*>(draw) + (size_t)r0 * pitch, raw + (size_t)r0 * pitch,
+                             ((size_t)(r1 - 1 - r0) * pitch + w) * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                             ctx->copy));
+    DS_TRY(cudaEventRecord(up_ev[c], ctx->copy));
+  }
+  const ds_src_u16 src{(const uint16_t*)draw, pitch, black, {white[0], white[1], white[2]}};
+  const int rcd_rows = (h + DS_RCD_TILE - 1) / DS_RCD_TILE;
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  const int bands = ty < BANDS ? ty : BANDS;
+  // band sizes shrink toward the end (weights 8,8,8,8,6,4,2,1), so that the
+  // copy of the last band, which nothing overlaps, is small
+  static const int wts[BANDS] = {8, 8, 8, 8, 6, 4, 2, 1};
+  int cum[BANDS + 1] = {0};
+  for (int b = 0; b < bands; b++) cum[b + 1] = cum[b] + (bands == BANDS ? wts[b] : 1);
+  const int nlm_halo = search + patch + 1;
+  int rcd_next = 0, chunks_waited = 0, tprev = 0;
+  for (int b = 0; b < bands; b++) {
+    const int t0 = tprev;
+    int t1 = (int)((long long)ty * cum[b + 1] / cum[bands]);
+    if (t1 <= t0) t1 = t0 + 1;  // every band holds at least one tile row
+    if (b == bands - 1 || t1 > ty) t1 = ty;
+    tprev = t1;
+    if (t0 >= t1) continue;
+    const int r1 = t1 * th < h ? t1 * th : h;  // output rows end of this band
+    int need = (r1 + nlm_halo + DS_RCD_TILE - 1) / DS_RCD_TILE;  // RCD tile rows this band reads
+    if (b == bands - 1 || need > rcd_rows) need = rcd_rows;
+    if (need > rcd_next) {
+      const int raw_end = need * DS_RCD_TILE + DS_RCD_HALO;  // raw rows that RCD band reads
+      while (chunks_waited < CHUNKS && (chunks_waited == 0 || chunk_end[chunks_waited - 1] < raw_end)) {
+        DS_TRY(cudaStreamWaitEvent(ctx->stream, up_ev[chunks_waited], 0));
+        chunks_waited++;
+      }
+      DS_TRY(ds_launch_rcd_u16_rows(ctx->stream, src, w, h, pat, mul, (float*)mid, (float*)dclip, rcd_next, need));
+      ctx->launches += 1;
+      rcd_next = need;
+    }
+    DS_TRY(ds_launch_nlm_rows(ctx->stream, (const float*)mid, w, h, 3, h_param, search, patch, t0, t1,
+                              (float*)drgb, (flags & DSGPU_FP16_STAGING) != 0));
+    ctx->launches += 1;
+    DS_TRY(cudaEventRecord(band_ev[b], ctx->stream));
+    DS_TRY(cudaStreamWaitEvent(ctx->copy, band_ev[b], 0));
+    const size_t r0 = (size_t)t0 * th, row = (size_t)w * 3;
+    DS_TRY(cudaMemcpyAsync(out_rgb + r0 * row, static_cast<float*>(drgb) + r0 * row,
+                           ((size_t)r1 - r0) * row * sizeof(float), cudaMemcpyDeviceToHost, ctx->copy));
+  }
+  if (out_clip)  // every RCD band is done before the last NLM band's event
+    DS_TRY(cudaMemcpyAsync(out_clip, dclip, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->copy));
+  if (cb) {
+    DS_TRY(cudaEventRecord(cb, ctx->copy));
+    ctx->marks.push_back({DSGPU_STAGE_COPY, ca, cb});
+  }
+  DS_TRY(cudaStreamSynchronize(ctx->copy));
+  return DSGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -547,6 +644,9 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
   if (n == 0) return DSGPU_OK;
   if (!raw || !out_rgb || !white || !mul || pitch < (size_t)w) return DSGPU_ERR_ARG;
   DeviceGuard g(ctx->device);
+  if ((flags & DSGPU_HOST) && !(flags & DSGPU_HIGHLIGHTS) && w >= 16 && h >= 16 && search > 0)
+    return develop_pipelined(ctx, raw, w, h, pitch, pat, black, white, mul, h_param, search, patch, out_rgb,
+                             out_clip, flags);
   const void* din;
   void *drgb, *dclip = nullptr, *mid;
   DS_CHECK(stage_in(ctx, flags, S_IN, raw, ((size_t)(h - 1) * pitch + w) * sizeof(uint16_t), &din));

@@ -414,9 +414,9 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
 template <class Src>
 __global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
                                                                float m1, float m2, float* __restrict__ out_rgb,
-                                                               float* __restrict__ out_clip) {
+                                                               float* __restrict__ out_clip, int ty0) {
   extern __shared__ float4 smem4[];
-  rcd_tile<Src, RT, RT>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, blockIdx.x, blockIdx.y,
+  rcd_tile<Src, RT, RT>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, blockIdx.x, blockIdx.y + ty0,
                         reinterpret_cast<float*>(smem4));
 }
 
@@ -672,18 +672,19 @@ cudaError_t launch_batch_fused_p(cudaStream_t st, const ds_batch_frame* frames, 
 }
 
 template <class Src>
+// tile rows [ty0, ty1) of 32 rows (ty1 < 0: to the last)
 cudaError_t launch_rcd(cudaStream_t st, Src src, int w, int h, ds_pat pat, const float mul[3], float* out_rgb,
-                       float* out_clip) {
-  static bool attr_set = false;  // per process; the attribute is per function
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(rcd_tile_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)RCD_SMEM);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  dim3 grid((w + RT - 1) / RT, (h + RT - 1) / RT);
+                       float* out_clip, int ty0 = 0, int ty1 = -1) {
+  const int tiles_y = (h + RT - 1) / RT;
+  if (ty1 < 0 || ty1 > tiles_y) ty1 = tiles_y;
+  if (ty0 >= ty1) return cudaSuccess;
+  // the attribute is per function and device: set it on every call (cheap)
+  cudaError_t e = cudaFuncSetAttribute(rcd_tile_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)RCD_SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 grid((w + RT - 1) / RT, ty1 - ty0);
   rcd_tile_kernel<Src><<<grid, RCD_THREADS, RCD_SMEM, st>>>(src, w, h, pat, mul[0], mul[1], mul[2], out_rgb,
-                                                            out_clip);
+                                                            out_clip, ty0);
   return cudaGetLastError();
 }
 
@@ -726,6 +727,12 @@ cudaError_t ds_launch_rcd_f32(cudaStream_t st, ds_src_f32 src, int w, int h, ds_
 cudaError_t ds_launch_rcd_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, const float mul[3],
                               float* out_rgb, float* out_clip) {
   return launch_rcd(st, SrcU16{src}, w, h, pat, mul, out_rgb, out_clip);
+}
+
+// the 32-row tile rows [ty0, ty1) only; they read raw rows [32 ty0 - 10, 32 ty1 + 10)
+cudaError_t ds_launch_rcd_u16_rows(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, const float mul[3],
+                                   float* out_rgb, float* out_clip, int ty0, int ty1) {
+  return launch_rcd(st, SrcU16{src}, w, h, pat, mul, out_rgb, out_clip, ty0, ty1);
 }
 
 void ds_rcd_batch_shape(int s, int* tile_w, int* tile_h) {
