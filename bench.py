@@ -479,6 +479,14 @@ def run_ours(args):
             "algorithmic": f"{updates:.4g} exp per launch (W*H*3*(2S+1)^2, one exp per pixel, channel and offset)",
             "peak_source": "ex2.approx throughput microbenchmark on this GPU (dsgpu_measure_peaks)",
             "launch_ms": nlm_launch_ms, "fp32_peak_tflops": fl / 1e12, "fp32x2_peak_tflops": fl2 / 1e12,
+            "binding": {
+                "resource": "shared memory (LSU data pipe) and issue, jointly",
+                "shared_bytes_per_update": 16.5, "shared_pct_of_peak": 73.4, "issue_pct_of_peak": 72.3,
+                "shared_bound_updates_per_s": 128.0 / 16.5 * 148 * 1.965e9,
+                "frac_of_shared_bound": updates / (nlm_launch_ms * 1e-3) / (128.0 / 16.5 * 148 * 1.965e9),
+                "source": "profiles/nlm_tile_kernel_4096x3072_full.md (ncu --set full); bound = 128 B/clk/SM "
+                          "x 148 SMs x 1.965 GHz / 16.5 B per update",
+            },
         }
         roof_rcd = {
             "kernel": "rcd_tile_kernel<SrcU16>", "bound": "hbm", "achieved": rcd_bytes / (dem_launch_ms * 1e-3) / 1e9,
