@@ -5,6 +5,7 @@
     python -m darkslide_b200.profile_case develop [--w W --h H]
     python -m darkslide_b200.profile_case denoise  # enhance::denoise, amount 50
     python -m darkslide_b200.profile_case cnn      # the learned stand-in (8 conv layers)
+    python -m darkslide_b200.profile_case batch --frames 8 --w 2048 --h 1536   # one batched graph launch
 
 Each case does one warm-up call and `--reps` timed calls on cuda:0 and
 prints the mean device time per call (CUDA events).
@@ -23,7 +24,8 @@ from darkslide_b200 import _lib
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise", "cnn"])
+    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise", "cnn", "batch"])
+    ap.add_argument("--frames", type=int, default=8, help="batch: frames of w x h")
     ap.add_argument("--w", type=int, default=0)
     ap.add_argument("--h", type=int, default=0)
     ap.add_argument("--reps", type=int, default=2)
@@ -55,7 +57,20 @@ def main():
         cfa = ds.normalize_u16(raw, ds.RGGB, 512, white, ctx=ctx).data
     st.synchronize()
 
+    frames = None
+    if a.case == "batch":  # a batch of equal frames, alternating CFA layouts
+        pats = [ds.RGGB, ds.BGGR, ds.GRBG, ds.GBRG]
+        with torch.cuda.stream(st):
+            frames = [ds.BatchFrame(raw, pats[k % 4], 512, white, mul, hp,
+                                    torch.empty((h, w, 3), dtype=torch.float32, device=dev))
+                      for k in range(a.frames)]
+        st.synchronize()
+
     def call():
+        if a.case == "batch":
+            with torch.cuda.stream(st):
+                ds.develop_batch(frames, a.search, a.patch, ctx=ctx, sync=False)
+            return
         if a.case == "nlm":
             r = L.dsgpu_nlm(ctx.handle, vp(rgb.data_ptr()), w, h, 3, float(hp), a.search, a.patch, vp(out.data_ptr()),
                             _lib.DSGPU_ASYNC | xflags)
@@ -90,7 +105,8 @@ def main():
     e1.record(st)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
-    print(f"{a.case} {w}x{h}: {ms:.3f} ms per call, {w * h / ms / 1e3:.1f} Mpix/s")
+    px = w * h * (a.frames if a.case == "batch" else 1)
+    print(f"{a.case} {w}x{h}: {ms:.3f} ms per call, {px / ms / 1e3:.1f} Mpix/s")
 
 
 if __name__ == "__main__":
