@@ -569,6 +569,19 @@ __global__ void hl_apply_kernel(float* __restrict__ img, const float* __restrict
   for (int c = 0; c < 3; c++) img[3 * i + c] = p[c] + (top - p[c]) * t * 0.5f;
 }
 
+// One RCD tile of a batch frame (local tile index), with the frame's tile shape.
+__device__ __noinline__ void rcd_batch_tile(const ds_batch_frame& F, int local, float* smem) {
+  const int ty = local / F.rcd_tiles_x, tx = local - ty * F.rcd_tiles_x;
+  const SrcU16 src{F.src};
+  switch (F.rcd_shape) {
+    case 0: rcd_tile<SrcU16, 32, 32>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    case 1: rcd_tile<SrcU16, 64, 16>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    case 2: rcd_tile<SrcU16, 48, 24>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    case 3: rcd_tile<SrcU16, 24, 48>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    default: rcd_tile<SrcU16, 16, 64>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+  }
+}
+
 __device__ __forceinline__ unsigned long long batch_clock_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -612,15 +625,7 @@ __global__ void __launch_bounds__(RCD_THREADS, 2) batch_fused_kernel(const ds_ba
     const ds_batch_frame& F = frames[sg.frame];
     const int local = t - sg.start;
     if (sg.kind == 0) {
-      const int ty = local / F.rcd_tiles_x, tx = local - ty * F.rcd_tiles_x;
-      const SrcU16 src{F.src};
-      switch (F.rcd_shape) {
-        case 0: rcd_tile<SrcU16, 32, 32>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-        case 1: rcd_tile<SrcU16, 64, 16>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-        case 2: rcd_tile<SrcU16, 48, 24>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-        case 3: rcd_tile<SrcU16, 24, 48>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-        default: rcd_tile<SrcU16, 16, 64>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-      }
+      rcd_batch_tile(F, local, smem);  // out of line: keeps the NLM body's registers to itself
       __syncthreads();
       if (tid == 0) {
         __threadfence();  // the tile's output before its count
