@@ -41,13 +41,20 @@ PATTERNS = [ds.RGGB, ds.BGGR, ds.GRBG, ds.GBRG]
 SEARCH, PATCH = 10, 3
 
 
-def draw_virtual(seed: int, w: int, h: int):
-    """A frame size log-uniform in 512..9504 px on the long side (aspect 1,
-    4:3 or 3:2) holding a w x h window at an even position: (W, H, x0, y0)."""
+CAMERA_SIZES = [(4000, 3000), (6000, 4000), (8256, 5504), (9504, 6336)]
+
+
+def draw_virtual(seed: int, w: int, h: int, scenes: str = "any"):
+    """A scene size holding a w x h window at an even position: (W, H, x0,
+    y0). scenes="any": log-uniform in 512..9504 px on the long side (aspect 1,
+    4:3 or 3:2); scenes="camera": one of the camera sizes the path is run on."""
     rng = np.random.default_rng(seed ^ 0xF00D)
-    L = float(np.exp(rng.uniform(np.log(512), np.log(9504))))
-    aspect = (1.0, 4 / 3, 1.5)[rng.integers(3)]
-    W, H = max(w, int(L)), max(h, int(L / aspect))
+    if scenes == "camera":
+        W, H = CAMERA_SIZES[int(rng.integers(len(CAMERA_SIZES)))]
+    else:
+        L = float(np.exp(rng.uniform(np.log(512), np.log(9504))))
+        aspect = (1.0, 4 / 3, 1.5)[rng.integers(3)]
+        W, H = max(w, int(L)), max(h, int(L / aspect))
     x0 = 2 * int(rng.integers(0, (W - w) // 2 + 1))
     y0 = 2 * int(rng.integers(0, (H - h) // 2 + 1))
     return W, H, x0, y0
@@ -65,8 +72,8 @@ def make_frame(seed: int, w: int, h: int, dev, ctx=None, bits=None, gain=None, r
     g_draw, r_draw = float(rng.uniform(0.25, 1.0)), float(rng.uniform(2.0, 12.0))
     bits = bits or b_draw
     black, white = (256, 4095) if bits == 12 else (512, 16383)
-    if virtual == "draw":
-        virtual = draw_virtual(seed, w, h)
+    if virtual in ("draw", "camera"):
+        virtual = draw_virtual(seed, w, h, "camera" if virtual == "camera" else "any")
     W, H, x0, y0 = virtual or (w, h, 0, 0)
     sc = ds.Scene(seed=seed, w=W, h=H, pattern=pattern, black=black, white=white,
                   gain=gain if gain is not None else g_draw,
@@ -89,7 +96,7 @@ def psnr(a, b, peak=1.0):
 
 def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=64, mix=8, warmup=500,
           clip_factor=3.0, seed=0, out=None, resume=None, log_every=200, verbose=True, dataset=200000,
-          relative=False):
+          relative=False, scenes="any"):
     import torch
 
     dev = torch.device("cuda", 0)
@@ -113,7 +120,8 @@ def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=
             queue.extend(int(f) for f in rng.permutation(n_frames))
         for _ in range(mix):
             fseed = seed * 100003 + 1 + queue.pop()
-            rgb, tgt, hp, _, _ = make_frame(fseed, frame, frame, dev, ctx, virtual="draw")
+            rgb, tgt, hp, _, _ = make_frame(fseed, frame, frame, dev, ctx,
+                                            virtual="camera" if scenes == "camera" else "draw")
             pos = np.random.default_rng(fseed ^ 0x5EED).integers(0, frame - crop + 1, (crops_per_frame, 2))
             pool.extend((rgb, tgt, hp, int(y), int(x)) for y, x in pos)
         order = rng.permutation(len(pool))
@@ -222,6 +230,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=500)
     ap.add_argument("--clip", type=float, default=3.0, help="clip factor x initial median gradient norm (0: off)")
     ap.add_argument("--relative-loss", action="store_true", help="weight squared errors by 1 / strength^2")
+    ap.add_argument("--scenes", default="any", choices=["any", "camera"],
+                    help="scene sizes the training windows come from")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     ap.add_argument("--resume", default=None)
@@ -229,7 +239,7 @@ def main():
     a = ap.parse_args()
     net, losses, secs = train(a.crops, a.batch, a.crop, a.lr, frame=a.frame, mix=a.mix, warmup=a.warmup,
                               clip_factor=a.clip, seed=a.seed, out=a.out, resume=a.resume, dataset=a.dataset,
-                              relative=a.relative_loss)
+                              relative=a.relative_loss, scenes=a.scenes)
     print(f"trained {a.crops} crop visits of a {a.dataset}-crop set in {secs:.1f} s", flush=True)
     if a.eval:
         evaluate(net, a.eval)
