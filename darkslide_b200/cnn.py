@@ -1,15 +1,17 @@
 """The learned stand-in for NLM (include/dsgpu.h, "learned path").
 
-A residual CNN of 8 conv3x3 layers (4 -> 48 x 7 -> 3, ReLU; dilations
-1, 2, 3, 4, 3, 2, 1, 1, a 35 x 35 receptive field): input the
-demosaiced RGB plus a constant channel STRENGTH_SCALE * h (h = the NLM
+A residual CNN of 8 conv3x3 layers (7 -> 48 x 7 -> 3, ReLU; dilations
+1, 2, 3, 4, 3, 2, 1, 1, a 35 x 35 receptive field): input the demosaiced
+RGB split into its 3x3 local mean and the remainder (so that BF16 keeps the
+remainder's precision) plus a constant channel STRENGTH_SCALE * h (h = the NLM
 strength of enhance.rs:36), output input + network. It is trained on the GPU,
 by the library's own BF16 tensor-core forward/backward kernels and Adam, to
 reproduce plain NLM; `infer` runs it and falls back to NLM on tiles whose
 removed component fails a residual check.
 
 Checkpoints are a small versioned binary: magic b"DSCNN1\\0\\0", u32 version
-(2: the dilated network; version 1 held the undilated one and is refused),
+(3: the dilated network on the local-mean split input; versions 1-2 held
+earlier networks and are refused),
 u32 parameter count, i64 Adam step, u64 data seed, then parameters, Adam m and
 Adam v as little-endian float32.
 """
@@ -24,10 +26,10 @@ from . import _lib
 from ._lib import Context, DsgpuError, default_context, lib
 
 STRENGTH_SCALE = 50.0
-LAYERS = [(4, 48)] + [(48, 48)] * 6 + [(48, 3)]  # (cin, cout)
+LAYERS = [(7, 48)] + [(48, 48)] * 6 + [(48, 3)]  # (cin, cout)
 DILATIONS = [1, 2, 3, 4, 3, 2, 1, 1]
 MAGIC = b"DSCNN1\0\0"
-VERSION = 2
+VERSION = 3
 
 
 def param_count() -> int:

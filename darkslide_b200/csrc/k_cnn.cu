@@ -1,7 +1,7 @@
 // The learned stand-in for NLM: a residual CNN of 8 conv3x3 layers
-// (4 -> 48 -> ... -> 48 -> 3, ReLU between; dilations 1,2,3,4,3,2,1,1),
-// input = demosaiced RGB plus a constant map of the NLM strength, output =
-// input RGB + network output.
+// (7 -> 48 -> ... -> 48 -> 3, ReLU between; dilations 1,2,3,4,3,2,1,1),
+// input = demosaiced RGB split into its 3x3 local mean and the remainder
+// (cnn_input_px) plus the NLM strength, output = input RGB + network output.
 // It is trained on the GPU to reproduce plain NLM (enhance.rs:36-72) and
 // runs with NLM as the per-tile fallback.
 //
@@ -291,24 +291,52 @@ __global__ void reduce_grads_kernel(const float* __restrict__ wpart, int nw, int
   }
 }
 
-// out = in RGB (fp32) and a constant strength channel -> NHWC16 bf16
-__global__ void pack_input_kernel(const float* __restrict__ rgb, size_t n, const float* __restrict__ strength_map,
-                                  float strength, bf16* __restrict__ x) {
+// The network's input at one pixel (8 bf16 values): channels 0-2 the RGB
+// minus its 3x3 local mean (clamped at the image edges), 3-5 that mean, 6 the
+// strength, 7 zero. The mean is taken in FP32 (row by row, then / 9) before
+// anything is rounded to BF16, so the detail the network sees keeps BF16's
+// relative precision at its own small magnitude instead of the pixel level's.
+__device__ __forceinline__ void cnn_input_px(const float* __restrict__ rgb, int W, int H, int x, int y, float strength,
+                                             bf16* v) {
+  const float* c = rgb + ((size_t)y * W + x) * 3;
+  float m[3] = {0.f, 0.f, 0.f};
+  for (int dy = -1; dy <= 1; dy++) {
+    const int yy = y + dy < 0 ? 0 : (y + dy >= H ? H - 1 : y + dy);
+    for (int dx = -1; dx <= 1; dx++) {
+      const int xx = x + dx < 0 ? 0 : (x + dx >= W ? W - 1 : x + dx);
+      const float* q = rgb + ((size_t)yy * W + xx) * 3;
+#pragma unroll
+      for (int k = 0; k < 3; k++) m[k] = m[k] + q[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    m[k] = __fdiv_rn(m[k], 9.0f);
+    v[k] = __float2bfloat16_rn(c[k] - m[k]);
+    v[3 + k] = __float2bfloat16_rn(m[k]);
+  }
+  v[6] = __float2bfloat16_rn(strength);
+  v[7] = __float2bfloat16_rn(0.f);
+}
+
+// B crops of H x W RGB (fp32) and their strength (map or constant) -> NHWC16 bf16
+__global__ void pack_input_kernel(const float* __restrict__ rgb, int B, int H, int W,
+                                  const float* __restrict__ strength_map, float strength, bf16* __restrict__ x) {
+  const size_t n = (size_t)B * H * W;
   const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
+  const int b = (int)(p / ((size_t)H * W));
+  const int r = (int)(p - (size_t)b * H * W), py = r / W, px = r - py * W;
   __align__(16) bf16 v[16];
-  v[0] = __float2bfloat16_rn(rgb[p * 3]);
-  v[1] = __float2bfloat16_rn(rgb[p * 3 + 1]);
-  v[2] = __float2bfloat16_rn(rgb[p * 3 + 2]);
-  v[3] = __float2bfloat16_rn(strength_map ? strength_map[p] : strength);
+  cnn_input_px(rgb + (size_t)b * H * W * 3, W, H, px, py, strength_map ? strength_map[p] : strength, v);
 #pragma unroll
-  for (int k = 4; k < 16; k++) v[k] = __float2bfloat16_rn(0.f);
+  for (int k = 8; k < 16; k++) v[k] = __float2bfloat16_rn(0.f);
   reinterpret_cast<uint4*>(x + p * 16)[0] = reinterpret_cast<uint4*>(v)[0];
   reinterpret_cast<uint4*>(x + p * 16)[1] = reinterpret_cast<uint4*>(v)[1];
 }
 
-// The tensor-core engine's input: [2][hp][wp][8] bf16 (channels 0-2 RGB, 3 the
-// strength, 4-15 zero; columns w..wp-1 and rows h..hp-1 zero).
+// The tensor-core engine's input: [2][hp][wp][8] bf16 (block 0 as above,
+// block 1 zero; columns w..wp-1 and rows h..hp-1 zero).
 __global__ void pack_input_tc_kernel(const float* __restrict__ rgb, int w, int h, int wp, int hp, float strength,
                                      bf16* __restrict__ x) {
   const size_t n = (size_t)wp * hp;
@@ -316,14 +344,11 @@ __global__ void pack_input_tc_kernel(const float* __restrict__ rgb, int w, int h
   if (p >= n) return;
   const int py = (int)(p / wp), px = (int)(p - (size_t)py * wp);
   __align__(16) bf16 v[8];
-#pragma unroll
-  for (int k = 0; k < 8; k++) v[k] = __float2bfloat16_rn(0.f);
   if (px < w && py < h) {
-    const size_t q = (size_t)py * w + px;
-    v[0] = __float2bfloat16_rn(rgb[q * 3]);
-    v[1] = __float2bfloat16_rn(rgb[q * 3 + 1]);
-    v[2] = __float2bfloat16_rn(rgb[q * 3 + 2]);
-    v[3] = __float2bfloat16_rn(strength);
+    cnn_input_px(rgb, w, h, px, py, strength, v);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = __float2bfloat16_rn(0.f);
   }
   reinterpret_cast<uint4*>(x)[p] = reinterpret_cast<uint4*>(v)[0];
   reinterpret_cast<uint4*>(x)[n + p] = make_uint4(0u, 0u, 0u, 0u);
@@ -525,7 +550,7 @@ struct LayerSpec {
 constexpr int NL = 8;
 // Dilations 1, 2, 3, 4, 3, 2, 1, 1: a 35 x 35 receptive field (8 undilated
 // layers see 17 x 17), covering NLM's 27 x 27 support at 7x7 / 21x21.
-constexpr LayerSpec LAYERS[NL] = {{4, 48, 16, 48, 1},  {48, 48, 48, 48, 2}, {48, 48, 48, 48, 3},
+constexpr LayerSpec LAYERS[NL] = {{7, 48, 16, 48, 1},  {48, 48, 48, 48, 2}, {48, 48, 48, 48, 3},
                                   {48, 48, 48, 48, 4}, {48, 48, 48, 48, 3}, {48, 48, 48, 48, 2},
                                   {48, 48, 48, 48, 1}, {48, 3, 48, 8, 1}};
 
@@ -698,7 +723,8 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
   const size_t n = (size_t)B * H * W;
   cudaError_t e = ds_cnn_pack(net, st);
   if (e != cudaSuccess) return e;
-  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, strength_map, strength, net->act[0]);
+  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, B, H, W, strength_map, strength,
+                                                                  net->act[0]);
   if ((e = forward(net, st, net->act[0], rgb, B, H, W, net->act, net->out)) != cudaSuccess) return e;
   const int lgrid = 512;
   mse_kernel<<<lgrid, CNN_THREADS, 0, st>>>(net->out, tgt, n, strength_map, strength, net->relative_loss, net->dy8,
@@ -803,7 +829,7 @@ cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, i
     return ds_cnn_forward_tc(st, net->ib, net->ia, net->ib, h, w, wf, bs, dil, rgb, out, net->err, net->mark_a,
                              net->mark_b);
   }
-  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, n, nullptr, strength, net->ib);
+  pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, 1, h, w, nullptr, strength, net->ib);
   bf16* acts[NL] = {net->ib, net->ia, net->ib, net->ia, net->ib, net->ia, net->ib, net->ia};
   return forward(net, st, net->ib, rgb, 1, h, w, acts, out, net->mark_a, net->mark_b);
 }

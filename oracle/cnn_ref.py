@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY: the checker for the GPU CNN kernels' gradients.
 Same layer table, padding (zero, "same") and parameter layout as the
-library: per layer weights [9 taps][cout][cin] (tap = ky*3 + kx, offset
+library: input packing (pack_input); per layer weights [9 taps][cout][cin] (tap = ky*3 + kx, offset
 ((ky-1) d, (kx-1) d) for the layer's dilation d) then biases [cout];
 loss = sum((out - target)^2) / (3 n).
 """
@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
-LAYERS = [(4, 48)] + [(48, 48)] * 6 + [(48, 3)]
+LAYERS = [(7, 48)] + [(48, 48)] * 6 + [(48, 3)]
 DILATIONS = [1, 2, 3, 4, 3, 2, 1, 1]
 
 
@@ -47,11 +47,28 @@ def conv_back(x, w, dy, d=1):
     return dxp[:, d:H + d, d:W + d, :], dw, dy.sum(axis=(0, 1, 2))
 
 
-def forward(params, rgb, strength):
-    """strength: a scalar or a [B, H, W] map."""
+def pack_input(rgb, strength):
+    """The network's input [B, H, W, 7] from float32 RGB [B, H, W, 3] and a
+    strength (scalar or [B, H, W] map), as the library forms it (float32):
+    channels 0-2 the RGB minus its 3x3 local mean (clamped edges; summed row
+    by row, then / 9), 3-5 that mean, 6 the strength."""
+    rgb = np.asarray(rgb, np.float32)
+    B, H, W, _ = rgb.shape
+    pad = np.pad(rgb, ((0, 0), (1, 1), (1, 1), (0, 0)), mode="edge")
+    m = np.zeros_like(rgb)
+    for dy in range(3):
+        for dx in range(3):
+            m = m + pad[:, dy:dy + H, dx:dx + W, :]
+    m = m / np.float32(9)
+    smap = np.broadcast_to(np.asarray(strength, np.float32)[..., None], rgb.shape[:3] + (1,))
+    return np.concatenate([rgb - m, m, smap], axis=-1).astype(np.float32)
+
+
+def forward(params, x, rgb):
+    """out = rgb + network(x) for a packed input x [B, H, W, 7] (pack_input)."""
     layers = unpack(np.asarray(params, np.float64))
-    smap = np.broadcast_to(np.asarray(strength, np.float64)[..., None], rgb.shape[:3] + (1,))
-    x = np.concatenate([rgb, smap], axis=-1).astype(np.float64)
+    x = np.asarray(x, np.float64)
+    rgb = np.asarray(rgb, np.float64)
     acts = [x]
     for i, (w, b) in enumerate(layers):
         y = conv(acts[-1], w, b, DILATIONS[i])
@@ -59,11 +76,11 @@ def forward(params, rgb, strength):
     return rgb + acts[-1], acts
 
 
-def gradients(params, rgb, strength, target, weight=None):
-    """(flat gradient, loss_sum) of sum(weight * (out - target)^2) / (3 n);
-    weight: None (1), a scalar or a [B, H, W] map."""
+def gradients(params, x, rgb, target, weight=None):
+    """(flat gradient, loss_sum) of sum(weight * (out - target)^2) / (3 n) for
+    out = forward(params, x, rgb); weight: None (1), a scalar or a [B, H, W] map."""
     layers = unpack(np.asarray(params, np.float64))
-    out, acts = forward(params, rgb, strength)
+    out, acts = forward(params, x, rgb)
     n = rgb.shape[0] * rgb.shape[1] * rgb.shape[2]
     d = out - target
     wt = 1.0 if weight is None else np.broadcast_to(np.asarray(weight, np.float64)[..., None], d.shape)

@@ -3,7 +3,7 @@
 
 The GPU keeps weights, inputs, activations and gradients in BF16 (8-bit
 mantissa) with FP32 accumulation, so it is compared with an FP64 reference fed
-the same BF16-rounded weights and inputs: outputs to 2e-2 of their scale,
+the same BF16-rounded weights and packed inputs (cnn_ref.pack_input): outputs to 2e-2 of their scale,
 gradients per layer by cosine similarity >= 0.995 and relative L2 error
 <= 5e-2."""
 import os
@@ -46,8 +46,8 @@ def test_forward_matches_fp64(torch_dev):
     rgb = np.random.default_rng(1).uniform(0.05, 0.9, (37, 45, 3)).astype(np.float32)
     out = net.infer(ds.Image3(45, 37, rgb), 0.01).data
     s = 0.01 * cnn.STRENGTH_SCALE
-    ref, _ = C.forward(C.bf16_round(p), C.bf16_round(rgb)[None], float(C.bf16_round(np.float32([s]))[0]))
-    ref = ref[0] - C.bf16_round(rgb) + rgb  # the residual adds the fp32 input
+    ref, _ = C.forward(C.bf16_round(p), C.bf16_round(C.pack_input(rgb[None], s)), rgb[None])
+    ref = ref[0]
     scale = np.abs(ref - rgb).max()
     assert np.abs(out - ref).max() <= 2e-2 * max(scale, 1e-3)
 
@@ -65,7 +65,7 @@ def test_gradients_match_fp64(torch_dev, crop):
     s = 0.5
     g, loss = net.gradients(trgb, s, ttgt)
     g = g.cpu().numpy()
-    gr, loss_r = C.gradients(C.bf16_round(p), C.bf16_round(rgb), float(C.bf16_round(np.float32([s]))[0]), tgt)
+    gr, loss_r = C.gradients(C.bf16_round(p), C.bf16_round(C.pack_input(rgb, s)), rgb, tgt)
     assert abs(loss - loss_r) <= 2e-2 * loss_r
     for i, (ws, bs, _) in enumerate(cnn.layer_slices()):
         for sl in (ws, bs):
@@ -90,7 +90,7 @@ def test_relative_loss_gradients_match_fp64(torch_dev):
     smap = np.stack([np.full((crop, crop), 0.3, np.float32), np.full((crop, crop), 1.7, np.float32)])
     g, loss = net.gradients(trgb, 0.0, ttgt, strength_map=torch.from_numpy(smap).to(dev))
     g = g.cpu().numpy()
-    gr, loss_r = C.gradients(C.bf16_round(p), C.bf16_round(rgb), C.bf16_round(smap), tgt,
+    gr, loss_r = C.gradients(C.bf16_round(p), C.bf16_round(C.pack_input(rgb, smap)), rgb, tgt,
                              weight=1.0 / smap.astype(np.float64) ** 2)
     assert abs(loss - loss_r) <= 2e-2 * loss_r
     for i, (ws, bs, _) in enumerate(cnn.layer_slices()):
@@ -189,8 +189,8 @@ def test_tensor_core_engine_matches_mma_sync_and_fp64(torch_dev, hw):
     tc = net.infer(ds.Image3(w, h, rgb), 0.01).data
     net.set_engine(False)
     ms = net.infer(ds.Image3(w, h, rgb), 0.01).data
-    ref, _ = C.forward(C.bf16_round(p), C.bf16_round(rgb)[None], float(C.bf16_round(np.float32([0.5]))[0]))
-    ref = ref[0] - C.bf16_round(rgb) + rgb
+    ref, _ = C.forward(C.bf16_round(p), C.bf16_round(C.pack_input(rgb[None], 0.5)), rgb[None])
+    ref = ref[0]
     scale = max(np.abs(ref - rgb).max(), 1e-3)
     assert np.isfinite(tc).all()
     assert np.abs(tc - ms).max() <= 2e-2 * scale
