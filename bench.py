@@ -410,9 +410,10 @@ def run_ours(args):
         ctx.set_stream(stream.cuda_stream)
         return {"value": ws * W * H * k / t / 1e6, "unit": "Mpix/s", "h2d_bytes_per_step": W * H * 2,
                 "d2h_bytes_per_step": W * H * 12, "copy_marks_ms_per_step": copy_ms / k,
-                "copies": "H2D of the raw, then (plain path) the RGB result copied back band by band on a "
-                          "second stream while the next band's NLM runs; copy_marks_ms spans those streams, "
-                          "overlap included"}
+                "copies": "both paths run as a band pipeline: the raw goes up in 8 row chunks on a second "
+                          "stream, demosaic and denoise (NLM, or the network with an 18-row halo plus its "
+                          "fallback) run in bands of rows, and each finished band's RGB is copied back while "
+                          "the next band computes; copy_marks_ms spans the copy stream, overlap included"}
 
     plain = device_timed(step_plain)
     learned = device_timed(step_learned)

@@ -41,6 +41,10 @@ int ds_cnn_take_status(DsCnn* net, cudaStream_t st);
 cudaError_t ds_cnn_denoise(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float h_param, int search,
                            int patch, float tau, float strength_scale, float* out, unsigned char* flags_scratch,
                            unsigned* count_dev);
+cudaError_t ds_cnn_reserve(DsCnn* net, int w, int h);
+cudaError_t ds_cnn_denoise_band(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, int r0, int r1, int halo,
+                                float h_param, int search, int patch, float tau, float strength_scale, float* out,
+                                float* band_out, unsigned char* flags_scratch, unsigned* count_dev);
 
 
 namespace {
@@ -950,7 +954,7 @@ int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, in
     DS_TRY(ds_cnn_infer(c->net, ctx->stream, (const float*)din, w, h, strength, (float*)dout));
     hidden.done = true;
   }
-  ctx->launches += 2 + 8 + 8;
+  ctx->launches += 1 + 8;  // input packing + 8 conv layers
   DS_CHECK(finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float)));
   return (flags & DSGPU_ASYNC) ? DSGPU_OK : ds_cnn_take_status(c->net, ctx->stream);
 }
@@ -996,7 +1000,7 @@ int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, 
                           DSGPU_CNN_STRENGTH_SCALE, (float*)dout, fl, cnt));
     hidden.done = true;
   }
-  ctx->launches += 2 + 8 + 8 + (tau > 0.f ? 2 : 0);
+  ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0);
   if (!(flags & DSGPU_ASYNC)) DS_CHECK(ds_cnn_take_status(c->net, ctx->stream));
   if (fallback_tiles) {
     unsigned hc = 0;
@@ -1007,6 +1011,116 @@ int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, 
     *fallback_tiles = (int)hc;
   }
   return finish(ctx, flags, out_rgb, dout, n * 3 * sizeof(float));
+}
+
+// Host-buffer learned develop as a three-stage pipeline over row bands, like
+// develop_pipelined: the raw goes up in 8 row chunks on the copy stream; RCD
+// runs in bands of its tile rows on the context stream, each waiting only for
+// the chunks it reads; the network runs in 8 bands of NLM tile rows, each on
+// its rows plus an 18-row halo above and below (the 8 dilated 3x3 layers reach
+// 1+2+3+4+3+2+1+1 = 17 rows, the input's 3x3 local mean one more), so that
+// the band's own rows come out as the whole-frame network computes them;
+// the residual check and the NLM fallback follow on the band's tiles; each
+// finished band goes back to the host on the copy stream while the next one
+// computes.
+static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw, int w, int h, size_t pitch,
+                                 ds_pat pat, float black, const float white[3], const float mul[3], float h_param,
+                                 int search, int patch, float tau, float* out_rgb, float* out_clip) {
+  constexpr int CHUNKS = 8, BANDS = 8, HALO = 18;
+  const size_t n = (size_t)w * h, row = (size_t)w * 3;
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  const int bands = ty < BANDS ? ty : BANDS;
+  // band sizes shrink toward the end (weights 8,8,8,8,6,4,2,1), so that the
+  // copy of the last band, which nothing overlaps, is small
+  static const int wts[BANDS] = {8, 8, 8, 8, 6, 4, 2, 1};
+  int cum[BANDS + 1] = {0};
+  for (int b = 0; b < bands; b++) cum[b + 1] = cum[b] + (bands == BANDS ? wts[b] : 1);
+  int bt[BANDS + 1] = {0};  // tile row where band b starts
+  int max_rows = 0;
+  for (int b = 0; b < bands; b++) {
+    int t1 = (int)((long long)ty * cum[b + 1] / cum[bands]);
+    if (t1 <= bt[b]) t1 = bt[b] + 1;  // every band holds at least one tile row
+    if (b == bands - 1 || t1 > ty) t1 = ty;
+    bt[b + 1] = t1 > bt[b] ? t1 : bt[b];
+    const int r0 = bt[b] * th, r1 = bt[b + 1] * th < h ? bt[b + 1] * th : h;
+    const int a0 = r0 - HALO > 0 ? r0 - HALO : 0, a1 = r1 + HALO < h ? r1 + HALO : h;
+    if (a1 - a0 > max_rows) max_rows = a1 - a0;
+  }
+  void *draw, *drgb, *mid, *band, *dclip = nullptr;
+  unsigned char* fl;
+  unsigned* cnt;
+  DS_CHECK(scratch(ctx, S_IN, ((size_t)(h - 1) * pitch + w) * sizeof(uint16_t), &draw));
+  DS_CHECK(scratch(ctx, S_OUT, n * 3 * sizeof(float), &drgb));
+  DS_CHECK(scratch(ctx, S_RGB, n * 3 * sizeof(float), &mid));
+  DS_CHECK(scratch(ctx, S_WORK, (size_t)max_rows * row * sizeof(float), &band));
+  if (out_clip) DS_CHECK(scratch(ctx, S_OUT2, n * sizeof(float), &dclip));
+  DS_CHECK(fallback_scratch(ctx, w, h, patch, &fl, &cnt));
+  DS_TRY(ds_cnn_reserve(net, w, max_rows));
+  if (!ctx->copy) DS_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  while (ctx->band_ev.size() < CHUNKS + BANDS + 1) {
+    cudaEvent_t e;
+    DS_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->band_ev.push_back(e);
+  }
+  cudaEvent_t* up_ev = ctx->band_ev.data();
+  cudaEvent_t* band_ev = ctx->band_ev.data() + CHUNKS;
+  cudaEvent_t start_ev = ctx->band_ev[CHUNKS + BANDS];
+  cudaEvent_t ca = ctx->profiling ? take_event(ctx) : nullptr, cb = ca ? take_event(ctx) : nullptr;
+  if (ca && !cb) {
+    ctx->pool.push_back(ca);
+    ca = nullptr;
+  }
+  DS_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned), ctx->stream));
+  // the copy stream starts after whatever the context stream already holds
+  DS_TRY(cudaEventRecord(start_ev, ctx->stream));
+  DS_TRY(cudaStreamWaitEvent(ctx->copy, start_ev, 0));
+  if (ca) DS_TRY(cudaEventRecord(ca, ctx->copy));
+  int chunk_end[CHUNKS];  // first raw row after chunk c
+  for (int c = 0; c < CHUNKS; c++) {
+    const int r0 = (int)((long long)h * c / CHUNKS), r1 = (int)((long long)h * (c + 1) / CHUNKS);
+    chunk_end[c] = r1;
+    if (r1 > r0)
+      DS_TRY(cudaMemcpyAsync(static_cast<uint16_t*>(draw) + (size_t)r0 * pitch, raw + (size_t)r0 * pitch,
+                             ((size_t)(r1 - 1 - r0) * pitch + w) * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                             ctx->copy));
+    DS_TRY(cudaEventRecord(up_ev[c], ctx->copy));
+  }
+  const ds_src_u16 src{(const uint16_t*)draw, pitch, black, {white[0], white[1], white[2]}};
+  const int rcd_rows = (h + DS_RCD_TILE - 1) / DS_RCD_TILE;
+  const int reach = HALO > search + patch + 1 ? HALO : search + patch + 1;  // RCD rows a band reads past its end
+  int rcd_next = 0, chunks_waited = 0;
+  for (int b = 0; b < bands; b++) {
+    if (bt[b] >= bt[b + 1]) continue;
+    const int r0 = bt[b] * th, r1 = bt[b + 1] * th < h ? bt[b + 1] * th : h;
+    int need = (r1 + reach + DS_RCD_TILE - 1) / DS_RCD_TILE;  // RCD tile rows this band reads
+    if (b == bands - 1 || need > rcd_rows) need = rcd_rows;
+    if (need > rcd_next) {
+      const int raw_end = need * DS_RCD_TILE + DS_RCD_HALO;  // raw rows that RCD band reads
+      while (chunks_waited < CHUNKS && (chunks_waited == 0 || chunk_end[chunks_waited - 1] < raw_end)) {
+        DS_TRY(cudaStreamWaitEvent(ctx->stream, up_ev[chunks_waited], 0));
+        chunks_waited++;
+      }
+      DS_TRY(ds_launch_rcd_u16_rows(ctx->stream, src, w, h, pat, mul, (float*)mid, (float*)dclip, rcd_next, need));
+      ctx->launches += 1;
+      rcd_next = need;
+    }
+    DS_TRY(ds_cnn_denoise_band(net, ctx->stream, (const float*)mid, w, h, r0, r1, HALO, h_param, search, patch, tau,
+                               DSGPU_CNN_STRENGTH_SCALE, (float*)drgb, (float*)band, fl, cnt));
+    ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0);
+    DS_TRY(cudaEventRecord(band_ev[b], ctx->stream));
+    DS_TRY(cudaStreamWaitEvent(ctx->copy, band_ev[b], 0));
+    DS_TRY(cudaMemcpyAsync(out_rgb + (size_t)r0 * row, static_cast<float*>(drgb) + (size_t)r0 * row,
+                           (size_t)(r1 - r0) * row * sizeof(float), cudaMemcpyDeviceToHost, ctx->copy));
+  }
+  if (out_clip)  // every RCD band is done before the last band's event
+    DS_TRY(cudaMemcpyAsync(out_clip, dclip, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->copy));
+  if (cb) {
+    DS_TRY(cudaEventRecord(cb, ctx->copy));
+    ctx->marks.push_back({DSGPU_STAGE_COPY, ca, cb});
+  }
+  DS_TRY(cudaStreamSynchronize(ctx->copy));
+  return ds_cnn_take_status(net, ctx->stream);
 }
 
 int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* c, const uint16_t* raw, int w, int h, size_t pitch,
@@ -1022,6 +1136,9 @@ int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* c, const uint16_t* raw, int
   if (!raw || !out_rgb || !white || !mul || pitch < (size_t)w || search < 1) return DSGPU_ERR_ARG;
   if (w < 16 || h < 16) return DSGPU_ERR_UNSUPPORTED;
   DeviceGuard g(ctx->device);
+  if (flags & DSGPU_HOST)
+    return develop_cnn_pipelined(ctx, c->net, raw, w, h, pitch, pat, black, white, mul, h_param, search, patch, tau,
+                                 out_rgb, out_clip);
   const void* din;
   void *drgb, *dclip = nullptr, *mid;
   unsigned char* fl;
@@ -1043,9 +1160,10 @@ int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* c, const uint16_t* raw, int
     DS_TRY(ds_cnn_denoise(c->net, ctx->stream, (const float*)mid, w, h, h_param, search, patch, tau,
                           DSGPU_CNN_STRENGTH_SCALE, (float*)drgb, fl, cnt));
     hidden.done = true;
-    ctx->launches += 2 + 8 + 8 + (tau > 0.f ? 2 : 0);
+    ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0);
   }
-  return finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float));
+  DS_CHECK(finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float)));
+  return (flags & DSGPU_ASYNC) ? DSGPU_OK : ds_cnn_take_status(c->net, ctx->stream);
 }
 
 // ------------------------------------------------------------------ scenes

@@ -109,6 +109,9 @@ cudaError_t ds_launch_nlm_rows(cudaStream_t st, const float* in, int w, int h, i
                                int search, int patch, int ty0, int ty1, float* out, bool fp16_staging);
 cudaError_t ds_launch_nlm_tiles(cudaStream_t st, const float* in, int w, int h, int channels, float h_param,
                                 int search, int patch, const unsigned char* flags, float* out);
+cudaError_t ds_launch_nlm_tiles_rows(cudaStream_t st, const float* in, int w, int h, int channels, float h_param,
+                                     int search, int patch, const unsigned char* flags, int ty0, int ty1,
+                                     float* out);
 // denoise composite (enhance.rs:75-92) and its parts
 size_t ds_denoise_scratch_bytes(int w, int h);
 size_t ds_noise_scratch_bytes(int w, int h);

@@ -456,12 +456,13 @@ __global__ void pack_weights_kernel(const float* __restrict__ w, int cout, int c
 // the NLM strength, h / 1.5), or when the output is not finite.
 __global__ void residual_check_kernel(const float* __restrict__ in, const float* __restrict__ out, int w, int h,
                                       int tile_w, int tile_h, float limit2, unsigned char* __restrict__ flags,
-                                      unsigned* __restrict__ count) {
+                                      unsigned* __restrict__ count, int ty0) {
   __shared__ float s[CNN_THREADS];
   __shared__ int bad;
   if (threadIdx.x == 0) bad = 0;
   __syncthreads();
-  const int x0 = blockIdx.x * tile_w, y0 = blockIdx.y * tile_h;
+  const int ty = blockIdx.y + ty0;  // tile row (a launch may cover a band of tile rows)
+  const int x0 = blockIdx.x * tile_w, y0 = ty * tile_h;
   float acc = 0.f;
   int n = 0;
   for (int i = threadIdx.x; i < tile_w * tile_h; i += CNN_THREADS) {
@@ -486,7 +487,7 @@ __global__ void residual_check_kernel(const float* __restrict__ in, const float*
     const int tw = min(tile_w, w - x0), th = min(tile_h, h - y0);
     const float mean = s[0] / (float)(3 * tw * th);
     const unsigned char f = (bad || !(mean <= limit2)) ? 1 : 0;
-    flags[blockIdx.y * gridDim.x + blockIdx.x] = f;
+    flags[ty * gridDim.x + blockIdx.x] = f;
     if (f) atomicAdd(count, 1u);
   }
   (void)n;
@@ -792,12 +793,12 @@ cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr) {
 }
 
 // Inference on a whole (w x h) RGB image; out = input + network(input).
-cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out) {
-  const size_t n = (size_t)w * h;
-  // the tensor-core engine pads rows to 4 pixels and planes to 12 rows (a
-  // multiple of every dilation)
-  const int wp = (w + 3) / 4 * 4, hp = (h + 11) / 12 * 12;
-  const size_t na = (size_t)wp * hp;
+// Grows the inference activations to hold a w x h frame (the tensor-core
+// engine pads rows to 4 pixels and planes to 12 rows, a multiple of every
+// dilation). cudaFree synchronises the device, so a caller that runs the
+// network on bands of different heights reserves the largest one first.
+cudaError_t ds_cnn_reserve(DsCnn* net, int w, int h) {
+  const size_t na = (size_t)((w + 3) / 4 * 4) * ((h + 11) / 12 * 12);
   cudaError_t e = cudaSuccess;
   if (net->infer_px < na) {
     if (net->ia) cudaFree(net->ia);
@@ -808,6 +809,15 @@ cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, i
     if ((e = cudaMalloc(&net->ib, na * 48 * sizeof(bf16))) != cudaSuccess) return e;
     net->infer_px = na;
   }
+  return e;
+}
+
+cudaError_t ds_cnn_infer(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float strength, float* out) {
+  const size_t n = (size_t)w * h;
+  const int wp = (w + 3) / 4 * 4, hp = (h + 11) / 12 * 12;
+  const size_t na = (size_t)wp * hp;
+  cudaError_t e = ds_cnn_reserve(net, w, h);
+  if (e != cudaSuccess) return e;
   if ((e = ds_cnn_pack(net, st)) != cudaSuccess) return e;
   // ping-pong: input packed into ib (16 ch), layers alternate ia/ib
   if (net->use_tc) {
@@ -868,7 +878,35 @@ cudaError_t ds_cnn_denoise(DsCnn* net, cudaStream_t st, const float* rgb, int w,
   if ((e = cudaMemsetAsync(count_dev, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
   const float sigma = h_param / 1.5f;
   residual_check_kernel<<<dim3(tx, ty), CNN_THREADS, 0, st>>>(rgb, out, w, h, tw, th, tau * tau * sigma * sigma,
-                                                              flags_scratch, count_dev);
+                                                              flags_scratch, count_dev, 0);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return ds_launch_nlm_tiles(st, rgb, w, h, 3, h_param, search, patch, flags_scratch, out);
+}
+
+// The same for output rows [r0, r1) only, r0 a multiple of the NLM tile
+// height: the network runs on rows [r0 - halo, r1 + halo) (clipped to the
+// frame) into band_out, whose rows [r0, r1) are exact when halo covers the
+// receptive field (35 rows, plus 1 for the input's local mean); they are
+// copied into out, then the residual check and the NLM fallback run on the
+// NLM tile rows of the band. count_dev must be zeroed before the first band.
+cudaError_t ds_cnn_denoise_band(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, int r0, int r1, int halo,
+                                float h_param, int search, int patch, float tau, float strength_scale, float* out,
+                                float* band_out, unsigned char* flags_scratch, unsigned* count_dev) {
+  const int a0 = r0 - halo > 0 ? r0 - halo : 0, a1 = r1 + halo < h ? r1 + halo : h;
+  const size_t row = (size_t)w * 3;
+  cudaError_t e = ds_cnn_infer(net, st, rgb + (size_t)a0 * row, w, a1 - a0, h_param * strength_scale, band_out);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(out + (size_t)r0 * row, band_out + (size_t)(r0 - a0) * row,
+                           (size_t)(r1 - r0) * row * sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+    return e;
+  if (tau <= 0.f) return cudaSuccess;
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  const int t0 = r0 / th, t1 = (r1 + th - 1) / th;
+  const float sigma = h_param / 1.5f;
+  residual_check_kernel<<<dim3(tx, t1 - t0), CNN_THREADS, 0, st>>>(rgb, out, w, h, tw, th,
+                                                                   tau * tau * sigma * sigma, flags_scratch,
+                                                                   count_dev, t0);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return ds_launch_nlm_tiles_rows(st, rgb, w, h, 3, h_param, search, patch, flags_scratch, t0, t1, out);
 }

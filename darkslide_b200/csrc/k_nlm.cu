@@ -199,6 +199,15 @@ cudaError_t ds_launch_nlm_tiles(cudaStream_t st, const float* in, int w, int h, 
   return dispatch_nlm(st, in, w, h, channels, search, patch, (float)sqrt(sig2), nullptr, out, flags);
 }
 
+// NLM on the flagged tiles of tile rows [ty0, ty1) only.
+cudaError_t ds_launch_nlm_tiles_rows(cudaStream_t st, const float* in, int w, int h, int channels, float h_param,
+                                     int search, int patch, const unsigned char* flags, int ty0, int ty1,
+                                     float* out) {
+  if (search <= 0) return cudaErrorInvalidValue;
+  return dispatch_nlm(st, in, w, h, channels, search, patch, ds_nlm_sigma(h_param, patch), nullptr, out, flags, false,
+                      ty0, ty1);
+}
+
 // The same with the strength h read from device memory (search > 0).
 cudaError_t ds_launch_nlm_dev_h(cudaStream_t st, const float* in, int w, int h, int channels, const float* h_dev,
                                 int search, int patch, float* out) {

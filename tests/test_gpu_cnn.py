@@ -257,3 +257,44 @@ def test_trained_network_gain(torch_dev):
 
     t_plain, t_learned = timed(plain), timed(learned)
     assert t_learned * 1.3 < t_plain, (t_plain, t_learned)
+
+
+@pytest.mark.parametrize("w,h", [(2048, 1536), (1000, 777), (300, 130), (96, 40)])
+@pytest.mark.parametrize("tau", [3.0, 0.5, 0.0])
+def test_host_buffer_learned_develop_equals_device_call(torch_dev, w, h, tau):
+    """With host buffers (DSGPU_HOST) the learned develop runs as a band
+    pipeline: the network on bands of rows with an 18-row halo, the residual
+    check and NLM fallback per band, copies overlapped. Its output and clip
+    plane equal the device-buffer call's bit for bit (tau 0.5 sends many tiles
+    to the fallback, tau 0 none)."""
+    from darkslide_b200 import _lib, cnn
+
+    torch, dev = torch_dev
+    ctx = ds.Context(0)
+    net = cnn.ResidualCNN(ctx)
+    net.load(os.path.join(os.path.dirname(cnn.__file__), "weights", "cnn_nlm.bin"))
+    L = _lib.lib()
+    vp = __import__("ctypes").c_void_p
+    pat = ds.GRBG.codes()
+    white = np.full(3, 16383, np.float32)
+    mul = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
+    scene = ds.Scene(seed=w + h, w=w, h=h, pattern=ds.GRBG, black=512, white=16383, gain=0.5, read_sigma=8)
+    hpar = 1.5 * scene.sigma_norm()
+    raw = scene.render(dev, ctx=ctx)
+    torch.cuda.synchronize()
+    o = torch.empty((h, w, 3), dtype=torch.float32, device=dev)
+    oc = torch.empty((h, w), dtype=torch.float32, device=dev)
+    ctx.check(L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, vp(raw.data_ptr()), w, h, w, vp(pat.ctypes.data),
+                                      512.0, vp(white.ctypes.data), vp(mul.ctypes.data), float(hpar), 10, 3,
+                                      tau, vp(o.data_ptr()), vp(oc.data_ptr()), 0), "develop_cnn device")
+    raw_h = raw.cpu().pin_memory()
+    out_h = torch.full((h, w, 3), -1.0, dtype=torch.float32).pin_memory()
+    clip_h = torch.full((h, w), -1.0, dtype=torch.float32).pin_memory()
+    for _ in range(2):  # the second call reuses the context's buffers and events
+        ctx.check(L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, vp(raw_h.data_ptr()), w, h, w,
+                                          vp(pat.ctypes.data), 512.0, vp(white.ctypes.data), vp(mul.ctypes.data),
+                                          float(hpar), 10, 3, tau, vp(out_h.data_ptr()), vp(clip_h.data_ptr()),
+                                          _lib.DSGPU_HOST), "develop_cnn host")
+        np.testing.assert_array_equal(out_h.numpy(), o.cpu().numpy())
+        np.testing.assert_array_equal(clip_h.numpy(), oc.cpu().numpy())
+        out_h.fill_(-1.0)
