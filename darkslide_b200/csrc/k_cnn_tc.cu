@@ -15,18 +15,20 @@
 // tile, zero-filled outside the image. The epilogue's stores of a block are
 // 512 contiguous bytes per warp.
 //
-// Pipeline. The staged input goes through a ring of 6 shared-memory slots,
-// one per (tile, 16-channel K step), so TMA runs up to two tiles ahead of
-// the MMAs and a slot is released after a third of a tile's MMAs.
+// Pipeline. The staged input goes through a ring of shared-memory slots, one
+// per (tile, 16-channel K step): 6 for tiles of 4 output rows (TMA runs up to
+// two tiles of a 48-channel input ahead of the MMAs), 3 for tiles of 10.
 //
 // Stacked taps. Input row j feeds output rows j, j-1, j-2 through weight
 // rows ky = 0, 1, 2. The three ky weight blocks are stacked along N, and the
 // output-row accumulators are laid out in TMEM in descending row order, so
 // one MMA per (input row, kx, 16 channels) with N = 3 x 48 covers all three
-// output rows (N = 48 or 96 at the tile's top and bottom edges). A 128 x 48 x
-// 16 MMA is bound by reading its 4 KB A operand from shared memory, not by
-// math, so stacking cuts the tensor time per output row by ~1.7x. The first
-// MMA into an output row's accumulator is split off with accumulate = 0.
+// output rows (N = 48 or 96 at the tile's top and bottom edges). Measured on
+// B200, a 128 x N x 16 BF16 MMA from shared memory costs the same for every N
+// up to 144 (76 cycles back to back; ~120 cycles inside this pipeline, where
+// commits are interleaved), so the time goes with the number of MMAs and
+// stacking the taps divides it by ~1.7. The first MMA into an output row's
+// accumulator is split off with accumulate = 0.
 //
 // Roles (one persistent CTA of 320 threads per SM, weights staged once):
 //   warp 9  TMA producer: the K steps of tile k into ring slots;
@@ -34,9 +36,10 @@
 //           accumulate) into TMEM accumulator set k % 2, then tcgen05.commit
 //           to release the smem stage and to hand the set to the epilogue;
 //   warps 0-7  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (pixels)
-//           of output rows 2 (w / 4) and 2 (w / 4) + 1 with tcgen05.ld, adds
-//           bias, applies ReLU or the residual and stores straight to global
-//           memory; each warp releases the accumulator set after its reads.
+//           of its TR / 2 output rows with tcgen05.ld, adds bias, applies
+//           ReLU (packing to BF16 in registers) or keeps the residual, hands
+//           the accumulator set back, and only then stores straight to
+//           global memory, so the next tile's MMAs never wait for stores.
 // Every mbarrier wait is bounded in time (2 s); a wait that gives up sets a
 // CTA-wide abort flag, which every other wait honours, reports
 // DSGPU_ERR_TIMEOUT through `err`, and the CTA waits (bounded) for its copies
@@ -55,19 +58,35 @@ typedef __nv_bfloat16 bf16;
 constexpr int TC_EPI_WARPS = 8;                    // two per TMEM lane quarter
 constexpr int TC_THREADS = 32 * (TC_EPI_WARPS + 2);  // + MMA warp + TMA warp
 constexpr int TC_M = 128;                          // pixels per MMA (one output-row segment)
-constexpr int TC_TR = 4;                           // output rows per tile
+// output rows per tile: 4 where a tile's accumulators are 48 columns a row
+// (two sets of 4 x 48 fit in half of TMEM each); 10 for the output layer (16
+// columns a row), which cuts its MMAs per output row by a fifth (its staged
+// rows carry 2 halo rows per 10 instead of per 4). Taller tiles for the
+// 48-channel layers measured slower (one accumulator set only).
+constexpr int TC_TR_WIDE = 4, TC_TR_NARROW = 10;
 constexpr int TC_PG = 4;                           // pixels per TMA element group (64-byte box rows)
 constexpr int TC_PW = TC_M + 2 * TC_PG;            // staged pixels per row: x0-4 .. x0+131
-constexpr int TC_PR = TC_TR + 2;                   // staged rows
-constexpr int TC_SLAB = TC_PW * TC_PR * 16;        // bytes per 8-channel block (13056, 128-B multiple)
-constexpr int TC_SUB = 2 * TC_SLAB;                // one ring slot: the 16 channels of one K step
-constexpr int TC_RING = 6;                         // ring slots (two tiles of a 48-channel input)
-static_assert(TC_SLAB % 128 == 0, "TMA destinations must stay 128-byte aligned");
 constexpr int TC_TMEM_COLS = 512;                  // accumulator sets at columns 0 and 256
 constexpr size_t TC_MIN_SMEM = 120 * 1024;         // keeps one CTA per SM (the TMEM plan assumes it)
 constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
 
 enum { TC_RELU = 0, TC_RESID = 1 };
+
+// Shape of a tile of TR output rows: PR staged rows; SLAB bytes per 8-channel
+// block of the staged tile; a ring slot (SUB) holds the 16 channels of one K
+// step; RING slots; NSETS TMEM accumulator sets of TR * NK columns (two when
+// they fit in half of TMEM, so the epilogue of one tile overlaps the MMAs of
+// the next; else one).
+template <int TR, int NK>
+struct TcShape {
+  static constexpr int PR = TR + 2;
+  static constexpr int SLAB = TC_PW * PR * 16;
+  static constexpr int SUB = 2 * SLAB;
+  static constexpr int RING = TR <= 4 ? 6 : 3;
+  static constexpr int NSETS = TR * NK <= 256 ? 2 : 1;
+  static_assert(SLAB % 128 == 0, "TMA destinations must stay 128-byte aligned");
+  static_assert(TR * NK <= TC_TMEM_COLS && TR % 2 == 0, "accumulators fit TMEM; two epilogue warps per lane quarter");
+};
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -169,16 +188,18 @@ __device__ __forceinline__ void mma_commit(unsigned bar) {
 // wt: [9][COUT_G][CIN] bf16; NK: output channels per ky block (COUT_G padded
 // to a multiple of 16); y: [COUT_G/8][Hp][Wp][8] bf16 (ReLU; padding columns
 // written as zero, padding rows left alone) or yf: [H][W][3] fp32 = resid +
-// conv (residual). DIL: dilation of the taps. A tile is TC_TR output rows
+// conv (residual). DIL: dilation of the taps. A tile is TR output rows
 // DIL apart (y0, y0 + DIL, ...) by 128 pixels; on that subsampled row grid a
 // dilated conv is an undilated one, so the staging and the stacked-tap MMAs
 // are the same for every DIL.
-template <int CIN, int COUT_G, int NK, int EPI, int DIL>
+template <int CIN, int COUT_G, int NK, int EPI, int DIL, int TR>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     conv_tc_kernel(const __grid_constant__ CUtensorMap xmap, int H, int W, const bf16* __restrict__ wt,
                    const float* __restrict__ bias, bf16* __restrict__ y, const float* __restrict__ resid,
                    float* __restrict__ yf, int* __restrict__ err) {
-  static_assert(CIN % 16 == 0 && NK % 16 == 0 && NK >= COUT_G && TC_TR * NK <= 256 && 3 * NK <= 256, "shapes");
+  static_assert(CIN % 16 == 0 && NK % 16 == 0 && NK >= COUT_G && 3 * NK <= 256, "shapes");
+  typedef TcShape<TR, NK> S;
+  constexpr int TC_PR = S::PR, TC_SLAB = S::SLAB, TC_SUB = S::SUB, TC_RING = S::RING, NSETS = S::NSETS;
   constexpr int CB = CIN / 8;              // 8-channel blocks of the input
   constexpr int KS = CIN / 16;             // K steps (ring slots) per tile
   constexpr int A_BYTES = TC_RING * TC_SUB;
@@ -233,8 +254,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const unsigned tmem = *tmem_slot;
 
-  // row bands of DIL * TC_TR rows, each split into DIL tiles by row residue
-  const int tiles_x = (W + TC_M - 1) / TC_M, tiles_y = (H + DIL * TC_TR - 1) / (DIL * TC_TR) * DIL;
+  // row bands of DIL * TR rows, each split into DIL tiles by row residue
+  const int tiles_x = (W + TC_M - 1) / TC_M, tiles_y = (H + DIL * TR - 1) / (DIL * TR) * DIL;
   const int ntiles = tiles_x * tiles_y;
   const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   // tile k of this CTA: first pixel x0, first output row y0 (then y0 + DIL, ...)
@@ -243,7 +264,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int ty = t / tiles_x;
     x0 = (t - ty * tiles_x) * TC_M;
     const int band = ty / DIL;
-    y0 = band * DIL * TC_TR + (ty - band * DIL);
+    y0 = band * DIL * TR + (ty - band * DIL);
   };
 
   if (warp == TC_EPI_WARPS + 1) {
@@ -260,7 +281,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           if (!(ok = mbar_wait(empty(q), ((g / TC_RING) & 1) ^ 1, abort_flag))) break;
           mbar_expect_tx(full(q), TX_BYTES);
           const unsigned dst = smem_u32(As) + (unsigned)(q * TC_SUB);
-          // staged rows y0 - DIL, y0, ..., y0 + TC_TR * DIL: residue y0 % DIL, quotients from y0 / DIL - 1
+          // staged rows y0 - DIL, y0, ..., y0 + TR * DIL: residue y0 % DIL, quotients from y0 / DIL - 1
           const int yr = y0 % DIL, yq = y0 / DIL - 1;
           tma_load_5d(dst, &xmap, x0 / TC_PG - 1, yr, yq, 2 * kc, full(q));
           tma_load_5d(dst + TC_SLAB, &xmap, x0 / TC_PG - 1, yr, yq, 2 * kc + 1, full(q));
@@ -278,8 +299,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       int g = 0, k = 0;
       bool ok = true;
       for (; k < my_tiles && ok; k++) {
-        const int s = k & 1;
-        if (!(ok = mbar_wait(tempty(s), ((k >> 1) & 1) ^ 1, abort_flag))) break;
+        const int s = k % NSETS, use = k / NSETS;  // accumulator set and how often it was used before
+        if (!(ok = mbar_wait(tempty(s), (use & 1) ^ 1, abort_flag))) break;
         const unsigned dbase = tmem + (unsigned)(s * 256);
 #pragma unroll 1
         for (int kc = 0; kc < KS; kc++, g++) {
@@ -292,10 +313,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           const unsigned long long bdesc = bdesc0 + (unsigned long long)(2 * kc * NS);
 #pragma unroll
           for (int j = 0; j < TC_PR; j++) {
-            const int ky_lo = j - (TC_TR - 1) > 0 ? j - (TC_TR - 1) : 0;
+            const int ky_lo = j - (TR - 1) > 0 ? j - (TR - 1) : 0;
             const int ky_hi = j < 2 ? j : 2;
             const int nky = ky_hi - ky_lo + 1;
-            const unsigned dcol = dbase + (unsigned)((TC_TR - 1 - j + ky_lo) * NK);  // accumulator of row j - ky_lo
+            const unsigned dcol = dbase + (unsigned)((TR - 1 - j + ky_lo) * NK);  // accumulator of row j - ky_lo
 #pragma unroll
             for (int kx = 0; kx < 3; kx++) {
               // staged pixel 0 is x0 - 4: output pixel x0 + m reads x0 + m + (kx - 1) DIL
@@ -331,15 +352,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
     }
   } else {
-    // ---------------- epilogue: warp w owns TMEM lanes 32 (w % 4)..+31 (pixels), rows 2 (w / 4)..+1
-    constexpr int RPW = TC_TR / (TC_EPI_WARPS / 4);  // output rows per epilogue warp
+    // ---------------- epilogue: warp w owns TMEM lanes 32 (w % 4)..+31 (pixels) and RPW output rows.
+    // It reads all its rows out of TMEM first (bias and ReLU applied, packed to BF16 in registers),
+    // hands the accumulator set back, then stores: the MMAs of the next tile need not wait for
+    // the stores, which matters when a single set holds the tile.
+    constexpr int RPW = TR / (TC_EPI_WARPS / 4);  // output rows per epilogue warp
+    constexpr int PK = EPI == TC_RELU ? COUT_G / 2 : 3;  // per row: BF16 pairs, or the 3 residual floats
     const int quarter = warp & 3, r0 = (warp >> 2) * RPW;
     const int Hp = (H + 11) / 12 * 12;
     const size_t plane = (size_t)Hp * Wp;
     for (int k = 0; k < my_tiles; k++) {
-      const int s = k & 1;
+      const int s = k % NSETS, use = k / NSETS;
       bool ok = true;
-      if (lane == 0) ok = mbar_wait(tfull(s), (k >> 1) & 1, abort_flag);
+      if (lane == 0) ok = mbar_wait(tfull(s), use & 1, abort_flag);
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -347,37 +372,51 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       tile_xy(k, x0, y0);
       const unsigned tbase = tmem + (unsigned)(s * 256) + ((unsigned)(quarter * 32) << 16);
       const int px = x0 + quarter * 32 + lane;
+      const bool in = px < W;  // padding columns are written as zero
+      unsigned pk[RPW][PK];
 #pragma unroll
-      for (int r = r0; r < r0 + RPW; r++) {
-        unsigned u[NK];
-        const unsigned col = tbase + (unsigned)((TC_TR - 1 - r) * NK);
+      for (int i = 0; i < RPW; i++) {
+        const unsigned col = tbase + (unsigned)((TR - 1 - (r0 + i)) * NK);
+        if (EPI == TC_RELU) {
 #pragma unroll
-        for (int c = 0; c < NK / 16; c++) tmem_ld16_async(col + c * 16, u + c * 16);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (r == r0 + RPW - 1) {  // this warp's reads of set s done: hand it back to the MMA warp
-          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-          __syncwarp();
-          if (lane == 0) mbar_arrive(tempty(s));
+          for (int c16 = 0; c16 < COUT_G; c16 += 16) {  // 16 columns at a time keeps the registers low
+            unsigned u[16];
+            tmem_ld16_async(col + c16, u);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int c = c16; c < c16 + 16 && c < COUT_G; c += 2) {
+              __nv_bfloat162 o = __floats2bfloat162_rn(
+                  in ? fmaxf(__uint_as_float(u[c - c16]) + bias_s[c], 0.f) : 0.f,
+                  in ? fmaxf(__uint_as_float(u[c - c16 + 1]) + bias_s[c + 1], 0.f) : 0.f);
+              pk[i][c / 2] = *reinterpret_cast<unsigned*>(&o);
+            }
+          }
+        } else {
+          unsigned u[16];
+          tmem_ld16_async(col, u);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int c = 0; c < PK; c++) pk[i][c] = __float_as_uint(__uint_as_float(u[c]) + bias_s[c]);
         }
-        const int gy = y0 + r * DIL;
+      }
+      // this warp's reads of set s done: hand it back to the MMA warp
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty(s));
+#pragma unroll
+      for (int i = 0; i < RPW; i++) {
+        const int gy = y0 + (r0 + i) * DIL;
         if (gy >= H || px >= Wp) continue;
         if (EPI == TC_RELU) {
           const size_t pix = (size_t)gy * Wp + px;
-          const bool in = px < W;  // padding columns are written as zero
 #pragma unroll
-          for (int c = 0; c < COUT_G; c += 8) {
-            __align__(16) __nv_bfloat162 o[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-              o[q] = __floats2bfloat162_rn(
-                  in ? fmaxf(__uint_as_float(u[c + 2 * q]) + bias_s[c + 2 * q], 0.f) : 0.f,
-                  in ? fmaxf(__uint_as_float(u[c + 2 * q + 1]) + bias_s[c + 2 * q + 1], 0.f) : 0.f);
-            *reinterpret_cast<uint4*>(y + ((size_t)(c / 8) * plane + pix) * 8) = *reinterpret_cast<uint4*>(o);
-          }
-        } else if (px < W) {
+          for (int c = 0; c < COUT_G; c += 8)
+            *reinterpret_cast<uint4*>(y + ((size_t)(c / 8) * plane + pix) * 8) =
+                make_uint4(pk[i][c / 2], pk[i][c / 2 + 1], pk[i][c / 2 + 2], pk[i][c / 2 + 3]);
+        } else if (in) {
           const size_t pix = (size_t)gy * W + px;
 #pragma unroll
-          for (int c = 0; c < 3; c++) yf[pix * 3 + c] = resid[pix * 3 + c] + (__uint_as_float(u[c]) + bias_s[c]);
+          for (int c = 0; c < 3; c++) yf[pix * 3 + c] = resid[pix * 3 + c] + __uint_as_float(pk[i][c]);
         }
       }
     }
@@ -401,12 +440,13 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-template <int CIN, int COUT_G, int NK, int EPI, int DIL>
+template <int CIN, int COUT_G, int NK, int EPI, int DIL, int TR>
 cudaError_t launch_tc_d(cudaStream_t st, const bf16* x, int H, int W, const bf16* wt, const float* bias, bf16* y,
                         const float* resid, float* yf, int* err) {
   static_assert(DIL >= 1 && DIL <= TC_PG && 12 % DIL == 0, "the staged row holds a halo of up to 4 pixels");
-  constexpr size_t need = (size_t)TC_RING * TC_SUB + (size_t)3 * (CIN / 8) * 3 * NK * 16 + NK * 4 +
-                         (2 * TC_RING + 4) * 8 + 16;
+  typedef TcShape<TR, NK> S;
+  constexpr size_t need = (size_t)S::RING * S::SUB + (size_t)3 * (CIN / 8) * 3 * NK * 16 + NK * 4 +
+                         (2 * S::RING + 4) * 8 + 16;
   constexpr size_t smem = need > TC_MIN_SMEM ? need : TC_MIN_SMEM;
   static_assert(need <= 227 * 1024, "shared memory");
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -419,32 +459,33 @@ cudaError_t launch_tc_d(cudaStream_t st, const bf16* x, int H, int W, const bf16
                               (cuuint64_t)(CIN / 8)};
   const cuuint64_t strides[4] = {16 * TC_PG, (cuuint64_t)Wp * 16, (cuuint64_t)Wp * 16 * DIL,
                                  (cuuint64_t)Wp * Hp * 16};
-  const cuuint32_t box[5] = {8 * TC_PG, (cuuint32_t)(TC_PW / TC_PG), 1, (cuuint32_t)TC_PR, 1};
+  const cuuint32_t box[5] = {8 * TC_PG, (cuuint32_t)(TC_PW / TC_PG), 1, (cuuint32_t)S::PR, 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(x), dims, strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT_G, NK, EPI, DIL>,
+  cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT_G, NK, EPI, DIL, TR>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int tiles = ((W + TC_M - 1) / TC_M) * ((H + DIL * TC_TR - 1) / (DIL * TC_TR) * DIL);
+  const int tiles = ((W + TC_M - 1) / TC_M) * ((H + DIL * TR - 1) / (DIL * TR) * DIL);
   const int grid = tiles < sms ? tiles : sms;
-  conv_tc_kernel<CIN, COUT_G, NK, EPI, DIL><<<grid, TC_THREADS, smem, st>>>(map, H, W, wt, bias, y, resid, yf, err);
+  conv_tc_kernel<CIN, COUT_G, NK, EPI, DIL, TR><<<grid, TC_THREADS, smem, st>>>(map, H, W, wt, bias, y, resid, yf,
+                                                                                err);
   return cudaGetLastError();
 }
 
-template <int CIN, int COUT_G, int NK, int EPI>
+template <int CIN, int COUT_G, int NK, int EPI, int TR = (NK > 16 ? TC_TR_WIDE : TC_TR_NARROW)>
 cudaError_t launch_tc(cudaStream_t st, int dil, const bf16* x, int H, int W, const bf16* wt, const float* bias,
                       bf16* y, const float* resid, float* yf, int* err) {
   switch (dil) {
-    case 1: return launch_tc_d<CIN, COUT_G, NK, EPI, 1>(st, x, H, W, wt, bias, y, resid, yf, err);
-    case 2: return launch_tc_d<CIN, COUT_G, NK, EPI, 2>(st, x, H, W, wt, bias, y, resid, yf, err);
-    case 3: return launch_tc_d<CIN, COUT_G, NK, EPI, 3>(st, x, H, W, wt, bias, y, resid, yf, err);
-    case 4: return launch_tc_d<CIN, COUT_G, NK, EPI, 4>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 1: return launch_tc_d<CIN, COUT_G, NK, EPI, 1, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 2: return launch_tc_d<CIN, COUT_G, NK, EPI, 2, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 3: return launch_tc_d<CIN, COUT_G, NK, EPI, 3, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 4: return launch_tc_d<CIN, COUT_G, NK, EPI, 4, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
     default: return cudaErrorInvalidValue;
   }
 }
