@@ -283,8 +283,9 @@ def run_batched(ctx, dev, steps: int, warmup: int, seed: int = 4) -> dict:
                              "max": float(np.max(lat)),
                              "definition": "device clock from the batch's start to the end of the frame's last "
                                            "NLM tile, over all frames of the timed batches"},
-        "launch": "one CUDA graph per batch: descriptor upload, start stamp, persistent RCD kernel, persistent "
-                  "NLM kernel over all frames' tiles",
+        "launch": "one CUDA graph per batch: descriptor upload, start stamp, one persistent kernel that takes "
+                  "the RCD and NLM tiles of all frames from one work queue (a frame's NLM tiles after its RCD "
+                  "tiles)",
         "gpu_launches_per_batch": launches / steps, "autotune_s": tune_s, "autotune": table,
     }
 
