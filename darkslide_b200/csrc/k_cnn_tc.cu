@@ -16,8 +16,8 @@
 // 512 contiguous bytes per warp.
 //
 // Pipeline. The staged input goes through a ring of shared-memory slots, one
-// per (tile, 16-channel K step): 6 for tiles of 4 output rows (TMA runs up to
-// two tiles of a 48-channel input ahead of the MMAs), 3 for tiles of 10.
+// per (tile, 16-channel K step): 6 for tiles of up to 5 output rows (TMA runs
+// up to two tiles of a 48-channel input ahead of the MMAs), 3 for taller ones.
 //
 // Stacked taps. Input row j feeds output rows j, j-1, j-2 through weight
 // rows ky = 0, 1, 2. The three ky weight blocks are stacked along N, and the
@@ -36,7 +36,7 @@
 //           accumulate) into TMEM accumulator set k % 2, then tcgen05.commit
 //           to release the smem stage and to hand the set to the epilogue;
 //   warps 0-7  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (pixels)
-//           of its TR / 2 output rows with tcgen05.ld, adds bias, applies
+//           of its half of the tile's rows with tcgen05.ld, adds bias, applies
 //           ReLU (packing to BF16 in registers) or keeps the residual, hands
 //           the accumulator set back, and only then stores straight to
 //           global memory, so the next tile's MMAs never wait for stores.
@@ -58,12 +58,15 @@ typedef __nv_bfloat16 bf16;
 constexpr int TC_EPI_WARPS = 8;                    // two per TMEM lane quarter
 constexpr int TC_THREADS = 32 * (TC_EPI_WARPS + 2);  // + MMA warp + TMA warp
 constexpr int TC_M = 128;                          // pixels per MMA (one output-row segment)
-// output rows per tile: 4 where a tile's accumulators are 48 columns a row
-// (two sets of 4 x 48 fit in half of TMEM each); 10 for the output layer (16
-// columns a row), which cuts its MMAs per output row by a fifth (its staged
-// rows carry 2 halo rows per 10 instead of per 4). Taller tiles for the
-// 48-channel layers measured slower (one accumulator set only).
-constexpr int TC_TR_WIDE = 4, TC_TR_NARROW = 10;
+// Output rows per tile, per layer (measured at 24 MP; every choice gives the
+// same output bit for bit): the staged rows carry 2 halo rows per tile, whose
+// MMAs cost as much as full ones, so taller tiles issue fewer MMAs per output
+// row, as long as two accumulator sets (TR x NK columns each) still fit in
+// TMEM and the staging ring in shared memory. 48 -> 48 layers: 5 rows
+// (1.155 -> 1.11 ms against 4; 10 rows, one accumulator set, 1.20-1.25 ms);
+// the 16 -> 48 input layer: 4 (5: 1.6% slower); the 48 -> 3 output layer
+// (16 columns a row): 10 (1.05 -> 0.80 ms against 4).
+constexpr int TC_TR_HIDDEN = 5, TC_TR_INPUT = 4, TC_TR_OUTPUT = 10;
 constexpr int TC_PG = 4;                           // pixels per TMA element group (64-byte box rows)
 constexpr int TC_PW = TC_M + 2 * TC_PG;            // staged pixels per row: x0-4 .. x0+131
 constexpr int TC_TMEM_COLS = 512;                  // accumulator sets at columns 0 and 256
@@ -82,10 +85,10 @@ struct TcShape {
   static constexpr int PR = TR + 2;
   static constexpr int SLAB = TC_PW * PR * 16;
   static constexpr int SUB = 2 * SLAB;
-  static constexpr int RING = TR <= 4 ? 6 : 3;
+  static constexpr int RING = TR <= 5 ? 6 : 3;
   static constexpr int NSETS = TR * NK <= 256 ? 2 : 1;
   static_assert(SLAB % 128 == 0, "TMA destinations must stay 128-byte aligned");
-  static_assert(TR * NK <= TC_TMEM_COLS && TR % 2 == 0, "accumulators fit TMEM; two epilogue warps per lane quarter");
+  static_assert(TR * NK <= TC_TMEM_COLS, "accumulators fit TMEM");
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -356,9 +359,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // It reads all its rows out of TMEM first (bias and ReLU applied, packed to BF16 in registers),
     // hands the accumulator set back, then stores: the MMAs of the next tile need not wait for
     // the stores, which matters when a single set holds the tile.
-    constexpr int RPW = TR / (TC_EPI_WARPS / 4);  // output rows per epilogue warp
+    constexpr int RPW = (TR + 1) / 2;  // output rows per epilogue warp (the second four may hold one fewer)
     constexpr int PK = EPI == TC_RELU ? COUT_G / 2 : 3;  // per row: BF16 pairs, or the 3 residual floats
-    const int quarter = warp & 3, r0 = (warp >> 2) * RPW;
+    static_assert(TC_EPI_WARPS == 8, "two epilogue warps per TMEM lane quarter");
+    const int quarter = warp & 3, r0 = (warp >> 2) * RPW, rn = TR - r0 < RPW ? TR - r0 : RPW;
     const int Hp = (H + 11) / 12 * 12;
     const size_t plane = (size_t)Hp * Wp;
     for (int k = 0; k < my_tiles; k++) {
@@ -376,6 +380,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       unsigned pk[RPW][PK];
 #pragma unroll
       for (int i = 0; i < RPW; i++) {
+        if (i >= rn) break;
         const unsigned col = tbase + (unsigned)((TR - 1 - (r0 + i)) * NK);
         if (EPI == TC_RELU) {
 #pragma unroll
@@ -405,6 +410,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       if (lane == 0) mbar_arrive(tempty(s));
 #pragma unroll
       for (int i = 0; i < RPW; i++) {
+        if (i >= rn) break;
         const int gy = y0 + (r0 + i) * DIL;
         if (gy >= H || px >= Wp) continue;
         if (EPI == TC_RELU) {
@@ -478,7 +484,8 @@ cudaError_t launch_tc_d(cudaStream_t st, const bf16* x, int H, int W, const bf16
   return cudaGetLastError();
 }
 
-template <int CIN, int COUT_G, int NK, int EPI, int TR = (NK > 16 ? TC_TR_WIDE : TC_TR_NARROW)>
+template <int CIN, int COUT_G, int NK, int EPI,
+          int TR = (NK <= 16 ? TC_TR_OUTPUT : (CIN >= 48 ? TC_TR_HIDDEN : TC_TR_INPUT))>
 cudaError_t launch_tc(cudaStream_t st, int dil, const bf16* x, int H, int W, const bf16* wt, const float* bias,
                       bf16* y, const float* resid, float* yf, int* err) {
   switch (dil) {
