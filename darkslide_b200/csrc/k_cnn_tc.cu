@@ -214,8 +214,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   unsigned char* Bs = sm + A_BYTES;
   float* bias_s = reinterpret_cast<float*>(sm + A_BYTES + B_BYTES);  // NK floats
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + A_BYTES + B_BYTES + NK * 4);
-  // bars: full[TC_RING], empty[TC_RING], tfull[2], tempty[2]
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * TC_RING + 4);
+  // bars: full[TC_RING], empty[TC_RING], tfull[2], tempty[2], drain
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * TC_RING + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot) + 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned bar0 = smem_u32(bars);
@@ -223,6 +223,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   auto empty = [&](int q) { return bar0 + 8u * (TC_RING + q); };
   auto tfull = [&](int s) { return bar0 + 8u * (2 * TC_RING + s); };
   auto tempty = [&](int s) { return bar0 + 8u * (2 * TC_RING + 2 + s); };
+  const unsigned drain = bar0 + 8u * (2 * TC_RING + 4);
+  // Slot release. When the ring holds exactly NSETS tiles, tile k's slots are next filled for tile
+  // k + NSETS, which uses the same accumulator set: the producer then waits for that set's
+  // completion commit of tile k, and the MMA warp commits once per tile instead of once per K step
+  // (every tcgen05.commit slows the MMA stream down). The set's next phase needs tile k + NSETS's
+  // own loads, so this parity wait cannot be overtaken.
+  constexpr bool TILE_RELEASE = TC_RING % KS == 0 && TC_RING / KS == NSETS;
   const int Wp = (W + TC_PG - 1) / TC_PG * TC_PG;
 
   for (int i = tid; i < 3 * CB * NS; i += TC_THREADS) {
@@ -248,6 +255,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       mbar_init(tfull(s), 1);
       mbar_init(tempty(s), TC_EPI_WARPS);
     }
+    mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
@@ -281,7 +289,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         bool ok = true;
         for (int kc = 0; kc < KS; kc++, g++) {
           const int q = g % TC_RING;
-          if (!(ok = mbar_wait(empty(q), ((g / TC_RING) & 1) ^ 1, abort_flag))) break;
+          if (TILE_RELEASE) {
+            if (kc == 0 && k >= NSETS && !(ok = mbar_wait(tfull(k % NSETS), ((k - NSETS) / NSETS) & 1, abort_flag)))
+              break;
+          } else if (!(ok = mbar_wait(empty(q), ((g / TC_RING) & 1) ^ 1, abort_flag))) {
+            break;
+          }
           mbar_expect_tx(full(q), TX_BYTES);
           const unsigned dst = smem_u32(As) + (unsigned)(q * TC_SUB);
           // staged rows y0 - DIL, y0, ..., y0 + TR * DIL: residue y0 % DIL, quotients from y0 / DIL - 1
@@ -343,14 +356,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               }
             }
           }
-          mma_commit(empty(q));  // ring slot q free once these MMAs have read it
+          if (!TILE_RELEASE) mma_commit(empty(q));  // ring slot q free once these MMAs have read it
         }
         if (ok) mma_commit(tfull(s));  // accumulator set s complete
       }
-      if (g > 0) {  // MMAs in flight (abort only): the last commit covers all of them
+      if (g > 0) {  // MMAs still in flight (after an abort): one commit covers them all
+        mma_commit(drain);
         const unsigned long long t0 = globaltimer_ns();
-        const int h = g - 1;
-        while (!mbar_test(empty(h % TC_RING), (h / TC_RING) & 1) && globaltimer_ns() - t0 < TC_WAIT_NS) {
+        while (!mbar_test(drain, 0) && globaltimer_ns() - t0 < TC_WAIT_NS) {
         }
       }
     }
@@ -452,7 +465,7 @@ cudaError_t launch_tc_d(cudaStream_t st, const bf16* x, int H, int W, const bf16
   static_assert(DIL >= 1 && DIL <= TC_PG && 12 % DIL == 0, "the staged row holds a halo of up to 4 pixels");
   typedef TcShape<TR, NK> S;
   constexpr size_t need = (size_t)S::RING * S::SUB + (size_t)3 * (CIN / 8) * 3 * NK * 16 + NK * 4 +
-                         (2 * S::RING + 4) * 8 + 16;
+                         (2 * S::RING + 5) * 8 + 16;
   constexpr size_t smem = need > TC_MIN_SMEM ? need : TC_MIN_SMEM;
   static_assert(need <= 227 * 1024, "shared memory");
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
