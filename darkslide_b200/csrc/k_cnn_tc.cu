@@ -18,6 +18,9 @@
 // Pipeline. The staged input goes through a ring of shared-memory slots, one
 // per (tile, 16-channel K step): 6 for tiles of up to 5 output rows (TMA runs
 // up to two tiles of a 48-channel input ahead of the MMAs), 3 for taller ones.
+// A slot is released by the tcgen05.commit of its K step's MMAs, or, where the
+// ring holds exactly one tile per accumulator set, by the tile's completion
+// commit (fewer commits: each one slows the MMA stream).
 //
 // Stacked taps. Input row j feeds output rows j, j-1, j-2 through weight
 // rows ky = 0, 1, 2. The three ky weight blocks are stacked along N, and the
