@@ -42,6 +42,7 @@ cudaError_t ds_cnn_denoise(DsCnn* net, cudaStream_t st, const float* rgb, int w,
                            int patch, float tau, float strength_scale, float* out, unsigned char* flags_scratch,
                            unsigned* count_dev);
 cudaError_t ds_cnn_reserve(DsCnn* net, int w, int h);
+int ds_cnn_halo_rows();
 cudaError_t ds_cnn_denoise_band(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, int r0, int r1, int halo,
                                 float h_param, int search, int patch, float tau, float strength_scale, float* out,
                                 float* band_out, unsigned char* flags_scratch, unsigned* count_dev);
@@ -190,6 +191,25 @@ int run_nlm(dsgpu_ctx* ctx, const float* in, int w, int h, int channels, float h
   return DSGPU_OK;
 }
 
+// A pipelined host-buffer call queues copies into the caller's host buffers on
+// the copy stream while kernels are still being launched. If a launch fails
+// midway, the call must not return while those copies can still run: the
+// caller may free or reuse its buffers as soon as the error comes back. This
+// guard waits for both streams on every early return (and clears the sticky
+// error state of a failed launch); the success path disarms it after its own
+// synchronisation.
+struct PipelineDrain {
+  dsgpu_ctx* ctx;
+  bool armed = true;
+  explicit PipelineDrain(dsgpu_ctx* c) : ctx(c) {}
+  ~PipelineDrain() {
+    if (!armed) return;
+    if (ctx->copy) cudaStreamSynchronize(ctx->copy);
+    cudaStreamSynchronize(ctx->stream);
+    cudaGetLastError();
+  }
+};
+
 // Host-buffer develop, second half: NLM in bands of tile rows on the context
 // stream, each band's rows copied to the host on the copy stream as soon as
 // the band is done (so the 12 B/px result copy overlaps the next band's NLM);
@@ -198,6 +218,7 @@ int nlm_bands_to_host(dsgpu_ctx* ctx, const float* mid, int w, int h, float h_pa
                       unsigned flags, const float* drgb, float* out_rgb, const float* dclip, float* out_clip) {
   constexpr int BANDS = 8;
   if (!ctx->copy) DS_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  PipelineDrain drain_guard(ctx);
   while (ctx->band_ev.size() < BANDS + 1) {
     cudaEvent_t e;
     DS_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -236,6 +257,7 @@ int nlm_bands_to_host(dsgpu_ctx* ctx, const float* mid, int w, int h, float h_pa
     ctx->marks.push_back({DSGPU_STAGE_COPY, ca, cb});
   }
   DS_TRY(cudaStreamSynchronize(ctx->copy));
+  drain_guard.armed = false;
   return DSGPU_OK;
 }
 
@@ -258,6 +280,7 @@ int develop_pipelined(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
   DS_CHECK(scratch(ctx, S_RGB, n * 3 * sizeof(float), &mid));
   if (out_clip) DS_CHECK(scratch(ctx, S_OUT2, n * sizeof(float), &dclip));
   if (!ctx->copy) DS_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  PipelineDrain drain_guard(ctx);
   while (ctx->band_ev.size() < CHUNKS + BANDS + 1) {
     cudaEvent_t e;
     DS_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -333,6 +356,7 @@ int develop_pipelined(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
     ctx->marks.push_back({DSGPU_STAGE_COPY, ca, cb});
   }
   DS_TRY(cudaStreamSynchronize(ctx->copy));
+  drain_guard.armed = false;
   return DSGPU_OK;
 }
 
@@ -1026,7 +1050,8 @@ int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, 
 static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw, int w, int h, size_t pitch,
                                  ds_pat pat, float black, const float white[3], const float mul[3], float h_param,
                                  int search, int patch, float tau, float* out_rgb, float* out_clip) {
-  constexpr int CHUNKS = 8, BANDS = 8, HALO = 18;
+  constexpr int CHUNKS = 8, BANDS = 8;
+  const int halo = ds_cnn_halo_rows();  // 18 for dilations 1,2,3,4,3,2,1,1
   const size_t n = (size_t)w * h, row = (size_t)w * 3;
   int tx, ty, tw, th;
   ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
@@ -1044,7 +1069,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
     if (b == bands - 1 || t1 > ty) t1 = ty;
     bt[b + 1] = t1 > bt[b] ? t1 : bt[b];
     const int r0 = bt[b] * th, r1 = bt[b + 1] * th < h ? bt[b + 1] * th : h;
-    const int a0 = r0 - HALO > 0 ? r0 - HALO : 0, a1 = r1 + HALO < h ? r1 + HALO : h;
+    const int a0 = r0 - halo > 0 ? r0 - halo : 0, a1 = r1 + halo < h ? r1 + halo : h;
     if (a1 - a0 > max_rows) max_rows = a1 - a0;
   }
   void *draw, *drgb, *mid, *band, *dclip = nullptr;
@@ -1058,6 +1083,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
   DS_CHECK(fallback_scratch(ctx, w, h, patch, &fl, &cnt));
   DS_TRY(ds_cnn_reserve(net, w, max_rows));
   if (!ctx->copy) DS_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  PipelineDrain drain_guard(ctx);
   while (ctx->band_ev.size() < CHUNKS + BANDS + 1) {
     cudaEvent_t e;
     DS_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1088,7 +1114,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
   }
   const ds_src_u16 src{(const uint16_t*)draw, pitch, black, {white[0], white[1], white[2]}};
   const int rcd_rows = (h + DS_RCD_TILE - 1) / DS_RCD_TILE;
-  const int reach = HALO > search + patch + 1 ? HALO : search + patch + 1;  // RCD rows a band reads past its end
+  const int reach = halo > search + patch + 1 ? halo : search + patch + 1;  // RCD rows a band reads past its end
   int rcd_next = 0, chunks_waited = 0;
   for (int b = 0; b < bands; b++) {
     if (bt[b] >= bt[b + 1]) continue;
@@ -1105,7 +1131,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
       ctx->launches += 1;
       rcd_next = need;
     }
-    DS_TRY(ds_cnn_denoise_band(net, ctx->stream, (const float*)mid, w, h, r0, r1, HALO, h_param, search, patch, tau,
+    DS_TRY(ds_cnn_denoise_band(net, ctx->stream, (const float*)mid, w, h, r0, r1, halo, h_param, search, patch, tau,
                                DSGPU_CNN_STRENGTH_SCALE, (float*)drgb, (float*)band, fl, cnt));
     ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0);
     DS_TRY(cudaEventRecord(band_ev[b], ctx->stream));
@@ -1120,6 +1146,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
     ctx->marks.push_back({DSGPU_STAGE_COPY, ca, cb});
   }
   DS_TRY(cudaStreamSynchronize(ctx->copy));
+  drain_guard.armed = false;
   return ds_cnn_take_status(net, ctx->stream);
 }
 

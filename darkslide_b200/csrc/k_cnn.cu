@@ -555,7 +555,17 @@ constexpr LayerSpec LAYERS[NL] = {{7, 48, 16, 48, 1},  {48, 48, 48, 48, 2}, {48,
                                   {48, 48, 48, 48, 4}, {48, 48, 48, 48, 3}, {48, 48, 48, 48, 2},
                                   {48, 48, 48, 48, 1}, {48, 3, 48, 8, 1}};
 
+// Rows (and columns) of input beyond an output region that the network reads:
+// each layer reaches its dilation, and the input packing's 3x3 local mean one more.
+constexpr int cnn_reach() {
+  int r = 1;
+  for (int l = 0; l < NL; l++) r += LAYERS[l].dil;
+  return r;
+}
+
 }  // namespace
+
+int ds_cnn_halo_rows() { return cnn_reach(); }
 
 // ----------------------------------------------------------------- network
 
