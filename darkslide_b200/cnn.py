@@ -185,6 +185,26 @@ class ResidualCNN:
                     "dsgpu_cnn_denoise")
         return Image3(img.w, img.h, out), int(nf.value)
 
+    def develop_u16(self, raw, pattern, black: float, white, mul, h_param: float, search: int = 10, patch: int = 3,
+                    tau: float = 3.0, with_clip: bool = False):
+        """u16 raw -> normalise -> RCD -> the network, with NLM recomputing the
+        tiles that fail the residual check (dsgpu_develop_u16_cnn). A numpy raw
+        runs as the host-buffer band pipeline, a CUDA tensor on the device.
+        Returns the Image3 (and the clip Plane when ``with_clip``)."""
+        from . import Image3, Plane, _Call, _f3, _vp
+
+        c = _Call(raw, self.ctx)
+        h, w = raw.shape
+        _, p = c.inp(raw, np.uint16)
+        rgb, pr = c.out((h, w, 3))
+        clip, pc = c.out((h, w)) if with_clip else (None, ctypes.c_void_p(0))
+        pat, wh, m = pattern.codes(), _f3(white), _f3(mul)
+        c.ctx.check(lib().dsgpu_develop_u16_cnn(c.ctx.handle, self.handle, p, w, h, w, _vp(pat), float(black), _vp(wh),
+                                                _vp(m), float(h_param), int(search), int(patch), float(tau), pr, pc,
+                                                c.flags), "dsgpu_develop_u16_cnn")
+        img = Image3(w, h, rgb)
+        return (img, Plane(w, h, clip)) if with_clip else img
+
     def set_clip(self, max_norm: float) -> None:
         """Clip the global gradient norm to max_norm in train_step (0: off)."""
         self.ctx.check(lib().dsgpu_cnn_set_clip(self.ctx.handle, self.handle, float(max_norm)), "dsgpu_cnn_set_clip")

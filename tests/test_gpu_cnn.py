@@ -298,3 +298,26 @@ def test_host_buffer_learned_develop_equals_device_call(torch_dev, w, h, tau):
         np.testing.assert_array_equal(out_h.numpy(), o.cpu().numpy())
         np.testing.assert_array_equal(clip_h.numpy(), oc.cpu().numpy())
         out_h.fill_(-1.0)
+
+
+def test_python_learned_develop(torch_dev):
+    """ResidualCNN.develop_u16: the same result from a CUDA tensor (device
+    call) and from numpy (host-buffer band pipeline), with the clip plane."""
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    ctx = ds.Context(0)
+    net = cnn.ResidualCNN(ctx)
+    net.load(os.path.join(os.path.dirname(cnn.__file__), "weights", "cnn_nlm.bin"))
+    w, h = 700, 450
+    scene = ds.Scene(seed=31, w=w, h=h, pattern=ds.BGGR, black=512, white=16383, gain=0.5, read_sigma=6)
+    hp = 1.5 * scene.sigma_norm()
+    raw = scene.render(dev, ctx=ctx)
+    torch.cuda.synchronize()
+    args = (ds.BGGR, 512, [16383.0] * 3, [2.0, 1.0, 1.0 / 0.7], hp)
+    img_d, clip_d = net.develop_u16(raw, *args, with_clip=True)
+    img_h, clip_h = net.develop_u16(raw.cpu().numpy(), *args, with_clip=True)
+    np.testing.assert_array_equal(np.asarray(img_h.data), img_d.data.cpu().numpy())
+    np.testing.assert_array_equal(np.asarray(clip_h.data), clip_d.data.cpu().numpy())
+    plain = ds.develop_u16(raw, ds.BGGR, 512, [16383.0] * 3, [2.0, 1.0, 1.0 / 0.7], hp, 10, 3).data.cpu().numpy()
+    assert np.abs(img_d.data.cpu().numpy() - plain).mean() < 2e-3  # a denoised image close to NLM's
