@@ -5,6 +5,7 @@
     python -m darkslide_b200.profile_case develop [--w W --h H]
     python -m darkslide_b200.profile_case denoise  # enhance::denoise, amount 50
     python -m darkslide_b200.profile_case cnn      # the learned stand-in (8 conv layers)
+    python -m darkslide_b200.profile_case learned  # u16 -> RCD -> network + NLM fallback (committed weights)
     python -m darkslide_b200.profile_case batch --frames 8 --w 2048 --h 1536   # one batched graph launch
 
 Each case does one warm-up call and `--reps` timed calls on cuda:0 and
@@ -24,7 +25,7 @@ from darkslide_b200 import _lib
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise", "cnn", "batch"])
+    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise", "cnn", "learned", "batch"])
     ap.add_argument("--frames", type=int, default=8, help="batch: frames of w x h")
     ap.add_argument("--w", type=int, default=0)
     ap.add_argument("--h", type=int, default=0)
@@ -80,6 +81,10 @@ def main():
         elif a.case == "cnn":
             r = L.dsgpu_cnn_infer(ctx.handle, net.handle, vp(rgb.data_ptr()), w, h, 0.5, vp(out.data_ptr()),
                                   _lib.DSGPU_ASYNC)
+        elif a.case == "learned":
+            r = L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, vp(raw.data_ptr()), w, h, w, vp(pat.ctypes.data), 512.0,
+                                        vp(white.ctypes.data), vp(mul.ctypes.data), float(hp), a.search, a.patch, 3.0,
+                                        vp(out.data_ptr()), vp(0), _lib.DSGPU_ASYNC)
         elif a.case == "denoise":
             r = L.dsgpu_denoise(ctx.handle, vp(rgb.data_ptr()), w, h, 50.0, vp(out.data_ptr()), _lib.DSGPU_ASYNC)
         else:
@@ -89,10 +94,14 @@ def main():
         ctx.check(r, a.case)
 
     net = None
-    if a.case == "cnn":
+    if a.case in ("cnn", "learned"):
+        import os
+
         from darkslide_b200 import cnn
 
         net = cnn.ResidualCNN(ctx)
+        if a.case == "learned":
+            net.load(os.path.join(os.path.dirname(cnn.__file__), "weights", "cnn_nlm.bin"))
     if a.case in ("nlm", "denoise", "cnn"):  # input: the demosaiced frame
         ctx.check(L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(mul.ctypes.data),
                                    _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(0), 0), "demosaic")
