@@ -319,7 +319,11 @@ int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* net, int tensor_core_gen5);
 int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, int h, float h_param,
                       int search, int patch, float tau, float* out_rgb, int* fallback_tiles, unsigned flags);
 /* u16 raw -> normalise -> RCD -> learned denoise with NLM fallback (the
- * learned counterpart of dsgpu_develop_u16; w, h >= 16). */
+ * learned counterpart of dsgpu_develop_u16; w or h < 16 gives
+ * DSGPU_ERR_UNSUPPORTED, search < 1 DSGPU_ERR_ARG). With DSGPU_HOST the call
+ * runs as a band pipeline: chunked upload, RCD and the network in row bands
+ * (each band with the network's 18-row halo), copies back overlapped with
+ * the next band; the result is bit-identical to the device-buffer call. */
 int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* net, const uint16_t* raw, int w, int h, size_t pitch_elems,
                           const uint8_t cfa[4], float black, const float white[3], const float mul[3],
                           float h_param, int search, int patch, float tau, float* out_rgb, float* out_clip,

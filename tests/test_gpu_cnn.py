@@ -321,3 +321,47 @@ def test_python_learned_develop(torch_dev):
     np.testing.assert_array_equal(np.asarray(clip_h.data), clip_d.data.cpu().numpy())
     plain = ds.develop_u16(raw, ds.BGGR, 512, [16383.0] * 3, [2.0, 1.0, 1.0 / 0.7], hp, 10, 3).data.cpu().numpy()
     assert np.abs(img_d.data.cpu().numpy() - plain).mean() < 2e-3  # a denoised image close to NLM's
+
+
+def test_learned_develop_composes_and_rejects(torch_dev):
+    """dsgpu_develop_u16_cnn equals RCD (dsgpu_develop_u16 with search 0, an
+    identity NLM) followed by dsgpu_cnn_denoise, bit for bit, on ragged and
+    thin frames; and it rejects what the header says it rejects."""
+    from darkslide_b200 import _lib, cnn
+
+    torch, dev = torch_dev
+    ctx = ds.Context(0)
+    net = cnn.ResidualCNN(ctx)
+    net.load(os.path.join(os.path.dirname(cnn.__file__), "weights", "cnn_nlm.bin"))
+    L = _lib.lib()
+    vp = __import__("ctypes").c_void_p
+    white = np.full(3, 16383, np.float32)
+    mul = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
+    for k, (w, h, pat) in enumerate([(16, 16, ds.RGGB), (211, 16, ds.GBRG), (16, 190, ds.GRBG), (333, 257, ds.BGGR)]):
+        sc = ds.Scene(seed=900 + k, w=w, h=h, pattern=pat, black=512, white=16383, gain=0.5, read_sigma=9)
+        hp = 1.5 * sc.sigma_norm()
+        raw = sc.render(dev, ctx=ctx)
+        torch.cuda.synchronize()
+        codes = pat.codes()
+        got = torch.empty((h, w, 3), dtype=torch.float32, device=dev)
+        ctx.check(L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, vp(raw.data_ptr()), w, h, w, vp(codes.ctypes.data),
+                                          512.0, vp(white.ctypes.data), vp(mul.ctypes.data), float(hp), 10, 3, 0.5,
+                                          vp(got.data_ptr()), vp(0), 0), "develop_cnn")
+        rgb = ds.develop_u16(raw, pat, 512, white, mul, hp, 0, 3, ctx=ctx)  # search 0: RCD output
+        exp, _ = net.denoise(rgb, hp, 10, 3, 0.5)
+        np.testing.assert_array_equal(got.cpu().numpy(), exp.data.cpu().numpy())
+    raw = torch.zeros((40, 40), dtype=torch.int16, device=dev)
+    o = torch.empty((40, 40, 3), dtype=torch.float32, device=dev)
+
+    def call(w, h, search=10, patch=3, codes=ds.RGGB.codes(), rawp=None):
+        return L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, rawp if rawp is not None else vp(raw.data_ptr()), w, h,
+                                       w, vp(codes.ctypes.data), 512.0, vp(white.ctypes.data), vp(mul.ctypes.data),
+                                       0.01, search, patch, 3.0, vp(o.data_ptr()), vp(0), 0)
+
+    assert call(15, 40) == _lib.DSGPU_ERR_UNSUPPORTED
+    assert call(40, 15) == _lib.DSGPU_ERR_UNSUPPORTED
+    assert call(40, 40, search=0) == _lib.DSGPU_ERR_ARG
+    assert call(40, 40, patch=99) == _lib.DSGPU_ERR_ARG
+    assert call(40, 40, codes=np.array([0, 1, 3, 2], np.uint8)) == _lib.DSGPU_ERR_CFA
+    assert call(40, 40, rawp=vp(0)) == _lib.DSGPU_ERR_ARG
+    assert call(0, 0) == _lib.DSGPU_OK  # empty: nothing to do
