@@ -115,6 +115,14 @@ __device__ __forceinline__ void mma_bf16(unsigned tmem_d, unsigned long long a, 
       "l"(a), "l"(b), "r"(idesc), "n"(ACC));
 }
 
+// 16 columns of zeros into this warp's 32 TMEM lanes
+__device__ __forceinline__ void tmem_zero16(unsigned addr) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(addr),
+      "r"(0u)
+      : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld16_async(unsigned addr, unsigned* r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
@@ -319,7 +327,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       bool ok = true;
       for (; k < my_tiles && ok; k++) {
         const int s = k % NSETS, use = k / NSETS;  // accumulator set and how often it was used before
-        if (!(ok = mbar_wait(tempty(s), (use & 1) ^ 1, abort_flag))) break;
+        // phase `use` of tempty(s): the set zeroed (at start, then after each epilogue read-out)
+        if (!(ok = mbar_wait(tempty(s), use & 1, abort_flag))) break;
         const unsigned dbase = tmem + (unsigned)(s * 256);
 #pragma unroll 1
         for (int kc = 0; kc < KS; kc++, g++) {
@@ -342,21 +351,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               const unsigned aoff = (unsigned)(j * TC_PW + TC_PG - DIL + kx * DIL);
               const unsigned long long b = bdesc + (unsigned)(kx * CB * NS + ky_lo * NK);
               const unsigned long long a = adesc + aoff;
-              if (kx == 0 && ky_lo == 0) {
-                if (kc == 0) {  // first contribution to output row j: start its accumulator
-                  mma_bf16<0>(dcol, a, b, umma_idesc(TC_M, NK));
-                } else {
-                  mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, NK));
-                }
-                if (nky == 2) mma_bf16<1>(dcol + NK, a, b + NK, umma_idesc(TC_M, NK));
-                if (nky == 3) mma_bf16<1>(dcol + NK, a, b + NK, umma_idesc(TC_M, 2 * NK));
-              } else if (nky == 1) {
-                mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, NK));
-              } else if (nky == 2) {
-                mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, 2 * NK));
-              } else {
-                mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, 3 * NK));
-              }
+              // the epilogue hands every accumulator set back zeroed, so each MMA accumulates
+              mma_bf16<1>(dcol, a, b, umma_idesc(TC_M, nky * NK));
             }
           }
           if (!TILE_RELEASE) mma_commit(empty(q));  // ring slot q free once these MMAs have read it
@@ -381,6 +377,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int quarter = warp & 3, r0 = (warp >> 2) * RPW, rn = TR - r0 < RPW ? TR - r0 : RPW;
     const int Hp = (H + 11) / 12 * 12;
     const size_t plane = (size_t)Hp * Wp;
+    // zero this warp's rows of accumulator set s (its lane quarter), then hand the set to the MMA warp
+    auto zero_and_release = [&](int s) {
+      const unsigned zbase = tmem + (unsigned)(s * 256) + ((unsigned)(quarter * 32) << 16);
+#pragma unroll
+      for (int i = 0; i < RPW; i++) {
+        if (i >= rn) break;
+#pragma unroll
+        for (int c = 0; c < NK; c += 16) tmem_zero16(zbase + (unsigned)((TR - 1 - (r0 + i)) * NK + c));
+      }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty(s));
+    };
+    for (int s = 0; s < NSETS; s++) zero_and_release(s);
     for (int k = 0; k < my_tiles; k++) {
       const int s = k % NSETS, use = k / NSETS;
       bool ok = true;
@@ -420,10 +431,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           for (int c = 0; c < PK; c++) pk[i][c] = __float_as_uint(__uint_as_float(u[c]) + bias_s[c]);
         }
       }
-      // this warp's reads of set s done: hand it back to the MMA warp
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(tempty(s));
+      // this warp's reads of set s done: zero its rows and hand the set back to the MMA warp
+      zero_and_release(s);
 #pragma unroll
       for (int i = 0; i < RPW; i++) {
         if (i >= rn) break;
