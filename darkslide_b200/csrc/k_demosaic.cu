@@ -141,7 +141,10 @@ __global__ void superpixel_kernel(const float* __restrict__ cfa, int w, int h, d
 // slower still. Every tiling gives the same output bit for bit.
 constexpr int RTX = 32, RTY = DS_RCD_TILE;
 constexpr int RH = 10;  // halo
-constexpr int RCD_THREADS = 256;
+constexpr int RCD_THREADS = 256;  // the batch kernels' block (shared with the NLM tile body)
+// The one-frame kernel's block: 512 threads, three CTAs per SM (40 registers
+// each): 5% faster than 256 (more warps to hide shared-memory latency).
+constexpr int RCD_THREADS_1F = 512;
 // shared bytes of a TX x TY tile: 8 stage arrays of (TX+20) x (TY+20) floats + the clip bytes
 __host__ __device__ constexpr size_t rcd_smem(int tx, int ty) {
   return (size_t)8 * (tx + 2 * RH) * (ty + 2 * RH) * sizeof(float) + (size_t)(tx + 2 * RH) * (ty + 2 * RH);
@@ -166,7 +169,7 @@ __device__ __forceinline__ float sq(float v) { return v * v; }
 // rcd_smem(TXT, TYT) bytes. The value at every site depends only on the
 // frame and the site's global coordinates, so any tiling gives the same
 // output bit for bit.
-template <class Src, int TXT, int TYT>
+template <class Src, int TXT, int TYT, int NT = RCD_THREADS>
 __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
                                          float* __restrict__ out_rgb, float* __restrict__ out_clip, int tile_x,
                                          int tile_y, float* smem) {
@@ -190,7 +193,7 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   const float eps = 1e-5f;
 
   // stage 0: load with clamped coordinates
-  for (int i = tid; i < RA; i += RCD_THREADS) {
+  for (int i = tid; i < RA; i += NT) {
     const int ly = i / RSX, lx = i - ly * RSX;
     const int gx = clampi(gx0 + lx, 0, W - 1), gy = clampi(gy0 + ly, 0, H - 1);
     const int col = pat.at(gx, gy);
@@ -204,7 +207,7 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   const int w1 = RSX, w2 = 2 * RSX, w3 = 3 * RSX, w4 = 4 * RSX;
 
   // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, edge-3) of the staged region
-  for (int i = tid; i < (RSX - 6) * (RSY - 6); i += RCD_THREADS) {
+  for (int i = tid; i < (RSX - 6) * (RSY - 6); i += NT) {
     const int ly = 3 + i / (RSX - 6), lx = 3 + i % (RSX - 6);
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RSX + lx;
@@ -231,7 +234,7 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   __syncthreads();
 
   // stage 2: vh (:173-184) and pq (:261-272) on [4, edge-4)
-  for (int i = tid; i < (RSX - 8) * (RSY - 8); i += RCD_THREADS) {
+  for (int i = tid; i < (RSX - 8) * (RSY - 8); i += NT) {
     const int ly = 4 + i / (RSX - 8), lx = 4 + i % (RSX - 8);
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RSX + lx;
@@ -273,12 +276,12 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   // stage 3: green (:203-214 init, :222-245 step 3) on [5, edge-5): (RSY-10)
   // rows x (RSX-10)/2 sites of each class
   constexpr int S3Y = RSY - 10, S3H = (RSX - 10) / 2;
-  for (int i = tid; i < S3Y * S3H; i += RCD_THREADS) {  // green sites: native sample
+  for (int i = tid; i < S3Y * S3H; i += NT) {  // green sites: native sample
     const int ly = 5 + i / S3H, lx = col_start(ly, 5, true) + 2 * (i % S3H);
     if (lx >= RSX - 5) continue;
     G[ly * RSX + lx] = C(ly * RSX + lx);
   }
-  for (int i = tid; i < S3Y * S3H; i += RCD_THREADS) {  // R/B sites
+  for (int i = tid; i < S3Y * S3H; i += NT) {  // R/B sites
     const int ly = 5 + i / S3H, lx = col_start(ly, 5, false) + 2 * (i % S3H);
     if (lx >= RSX - 5) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
@@ -316,7 +319,7 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   // samples, i.e. c. Interior green sites are never read (4.4 reads R/B
   // sites only); ring green sites keep their MHC values.
   constexpr int S4Y = RSY - 14, S4H = (RSX - 14) / 2;
-  for (int i = tid; i < S4Y * S4H; i += RCD_THREADS) {  // R/B sites
+  for (int i = tid; i < S4Y * S4H; i += NT) {  // R/B sites
     const int ly = 7 + i / S4H, lx = col_start(ly, 7, false) + 2 * (i % S4H);
     if (lx >= RSX - 7) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
@@ -348,7 +351,7 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
     R43[k] = r;
     B43[k] = b;
   }
-  for (int i = tid; i < S4Y * S4H; i += RCD_THREADS) {  // green sites of the ring
+  for (int i = tid; i < S4Y * S4H; i += NT) {  // green sites of the ring
     const int ly = 7 + i / S4H, lx = col_start(ly, 7, true) + 2 * (i % S4H);
     if (lx >= RSX - 7) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
@@ -369,7 +372,7 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
       for (int dx = -1; dx <= 1; dx++) m |= CL[k + dy * RSX + dx];
     return m ? 1.0f : 0.0f;
   };
-  for (int i = tid; i < TYT * TH; i += RCD_THREADS) {  // green sites
+  for (int i = tid; i < TYT * TH; i += NT) {  // green sites
     const int ly = RH + i / TH, lx = col_start(ly, RH, true) + 2 * (i % TH);
     if (lx >= RH + TXT) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
@@ -401,7 +404,7 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
     o[2] = b;
     if (out_clip) out_clip[(size_t)gy * W + gx] = clip_at(k);
   }
-  for (int i = tid; i < TYT * TH; i += RCD_THREADS) {  // R/B sites: values settled by stage 4
+  for (int i = tid; i < TYT * TH; i += NT) {  // R/B sites: values settled by stage 4
     const int ly = RH + i / TH, lx = col_start(ly, RH, false) + 2 * (i % TH);
     if (lx >= RH + TXT) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
@@ -416,12 +419,12 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
 }
 
 template <class Src>
-__global__ void __launch_bounds__(RCD_THREADS) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
-                                                               float m1, float m2, float* __restrict__ out_rgb,
-                                                               float* __restrict__ out_clip, int ty0) {
+__global__ void __launch_bounds__(RCD_THREADS_1F, 3) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
+                                                                      float m1, float m2, float* __restrict__ out_rgb,
+                                                                      float* __restrict__ out_clip, int ty0) {
   extern __shared__ float4 smem4[];
-  rcd_tile<Src, RTX, RTY>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, blockIdx.x, blockIdx.y + ty0,
-                        reinterpret_cast<float*>(smem4));
+  rcd_tile<Src, RTX, RTY, RCD_THREADS_1F>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, blockIdx.x,
+                                          blockIdx.y + ty0, reinterpret_cast<float*>(smem4));
 }
 
 // Tile shapes of the batched kernel (w x h); all of them fit two CTAs per SM.
@@ -692,7 +695,7 @@ cudaError_t launch_rcd(cudaStream_t st, Src src, int w, int h, ds_pat pat, const
                                        (int)RCD_SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid((w + RTX - 1) / RTX, ty1 - ty0);
-  rcd_tile_kernel<Src><<<grid, RCD_THREADS, RCD_SMEM, st>>>(src, w, h, pat, mul[0], mul[1], mul[2], out_rgb,
+  rcd_tile_kernel<Src><<<grid, RCD_THREADS_1F, RCD_SMEM, st>>>(src, w, h, pat, mul[0], mul[1], mul[2], out_rgb,
                                                             out_clip, ty0);
   return cudaGetLastError();
 }
