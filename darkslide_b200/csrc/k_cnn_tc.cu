@@ -28,10 +28,12 @@
 // one MMA per (input row, kx, 16 channels) with N = 3 x 48 covers all three
 // output rows (N = 48 or 96 at the tile's top and bottom edges). Measured on
 // B200, a 128 x N x 16 BF16 MMA from shared memory costs the same for every N
-// up to 144 (76 cycles back to back; ~120 cycles inside this pipeline, where
+// up to 144 (76 cycles back to back; ~97 cycles inside this pipeline, where
 // commits are interleaved), so the time goes with the number of MMAs and
-// stacking the taps divides it by ~1.7. The first MMA into an output row's
-// accumulator is split off with accumulate = 0.
+// stacking the taps divides it by ~1.7. Every MMA accumulates: the epilogue
+// zeroes the accumulator rows it has read (tcgen05.st) before handing a set
+// back, and zeroes both sets at start. (Starting each row with a split-off
+// accumulate = 0 MMA instead cost 15-20 % of a 48-channel layer.)
 //
 // Roles (one persistent CTA of 320 threads per SM, weights staged once):
 //   warp 9  TMA producer: the K steps of tile k into ring slots;
@@ -40,9 +42,10 @@
 //           to release the smem stage and to hand the set to the epilogue;
 //   warps 0-7  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (pixels)
 //           of its half of the tile's rows with tcgen05.ld, adds bias, applies
-//           ReLU (packing to BF16 in registers) or keeps the residual, hands
-//           the accumulator set back, and only then stores straight to
-//           global memory, so the next tile's MMAs never wait for stores.
+//           ReLU (packing to BF16 in registers) or keeps the residual, zeroes
+//           those rows, hands the accumulator set back, and only then stores
+//           straight to global memory, so the next tile's MMAs never wait for
+//           stores.
 // Every mbarrier wait is bounded in time (2 s); a wait that gives up sets a
 // CTA-wide abort flag, which every other wait honours, reports
 // DSGPU_ERR_TIMEOUT through `err`, and the CTA waits (bounded) for its copies
