@@ -1040,25 +1040,26 @@ int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, 
 // Host-buffer learned develop as a three-stage pipeline over row bands, like
 // develop_pipelined: the raw goes up in 8 row chunks on the copy stream; RCD
 // runs in bands of its tile rows on the context stream, each waiting only for
-// the chunks it reads; the network runs in 8 bands of NLM tile rows, each on
+// the chunks it reads; the network runs in 5 bands of NLM tile rows, each on
 // its rows plus an 18-row halo above and below (the 8 dilated 3x3 layers reach
 // 1+2+3+4+3+2+1+1 = 17 rows, the input's 3x3 local mean one more), so that
 // the band's own rows come out as the whole-frame network computes them;
 // the residual check and the NLM fallback follow on the band's tiles; each
 // finished band goes back to the host on the copy stream while the next one
-// computes.
+// computes. Fewer bands than the NLM pipeline: every band boundary costs 36
+// rows of network work, and the copies (53 GB/s) keep up with larger bands.
 static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw, int w, int h, size_t pitch,
                                  ds_pat pat, float black, const float white[3], const float mul[3], float h_param,
                                  int search, int patch, float tau, float* out_rgb, float* out_clip) {
-  constexpr int CHUNKS = 8, BANDS = 8;
+  constexpr int CHUNKS = 8, BANDS = 5;
   const int halo = ds_cnn_halo_rows();  // 18 for dilations 1,2,3,4,3,2,1,1
   const size_t n = (size_t)w * h, row = (size_t)w * 3;
   int tx, ty, tw, th;
   ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
   const int bands = ty < BANDS ? ty : BANDS;
-  // band sizes shrink toward the end (weights 8,8,8,8,6,4,2,1), so that the
-  // copy of the last band, which nothing overlaps, is small
-  static const int wts[BANDS] = {8, 8, 8, 8, 6, 4, 2, 1};
+  // band sizes shrink toward the end (weights 8,8,8,4,1), so that the copy of
+  // the last band, which nothing overlaps, is small
+  static const int wts[BANDS] = {8, 8, 8, 4, 1};
   int cum[BANDS + 1] = {0};
   for (int b = 0; b < bands; b++) cum[b + 1] = cum[b] + (bands == BANDS ? wts[b] : 1);
   int bt[BANDS + 1] = {0};  // tile row where band b starts
