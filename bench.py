@@ -28,6 +28,7 @@ region is bracketed by barriers and the time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -72,9 +73,11 @@ def h_param() -> float:
 
 
 class Clocks:
-    """Samples nvidia-smi during the timed region."""
+    """Samples nvidia-smi every 50 ms from before the warm-up (so that the
+    sampler is already running when the timed region starts) and summarises
+    the samples received inside the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
@@ -86,7 +89,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100",
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "50",
                  "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -97,7 +100,9 @@ class Clocks:
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
 
-    def stop(self) -> dict:
+    def stop(self, t0: float | None = None, t1: float | None = None) -> dict:
+        """Ends sampling; with t0/t1 (time.time() at the region's start and
+        end) only the samples that nvidia-smi stamped between them count."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -106,23 +111,39 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.t.join(timeout=2)
-        sm, smax, reasons, power = [], None, set(), []
+        sm, smax, reasons, power, masks = [], None, set(), [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        # bits of clocks_event_reasons.active (NVML's clocks event reason flags)
+        bits = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+                0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+                0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-                power.append(float(f[3]))
+                t = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+            if (t0 is not None and t < t0) or (t1 is not None and t > t1):
+                continue
+            try:
+                sm.append(float(f[2]))
+                smax = float(f[3])
+                power.append(float(f[4]))
+            except ValueError:
+                continue
+            try:
+                m = int(f[5], 16)
+                masks.add(f[5])
+                reasons.update(n for b, n in bits.items() if m & b)
+            except ValueError:
+                pass
+            for n, v in zip(names, f[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm),
+                "reasons": sorted(reasons), "active_masks": sorted(masks), "samples": len(sm),
                 "power_w_max": max(power) if power else None}
 
 
@@ -361,15 +382,16 @@ def run_ours(args):
         """K steps with the raw frame resident in HBM: CUDA events on the
         launching stream, clocks sampled during the region, per-stage marks."""
         ctx.set_stream(stream.cuda_stream)
+        clocks = Clocks(gpu_index)
+        clocks.start()  # running through the warm-up, so it samples from the region's first moment
         for _ in range(args.warmup):
             step()
         stream.synchronize()
-        clocks = Clocks(gpu_index)
         ctx.profile(True)
         n0 = ctx.launch_count()
         barrier()
         torch.cuda.synchronize(dev)
-        clocks.start()
+        t_start = time.time()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
@@ -377,8 +399,9 @@ def run_ours(args):
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize(dev)
+        t_end = time.time()
         barrier()
-        clk = clocks.stop()
+        clk = clocks.stop(t_start, t_end)
         r = {"ms": max_over_ranks(e0.elapsed_time(e1)), "launches": ctx.launch_count() - n0, "clocks": clk}
         for name, st in (("demosaic", _lib.DSGPU_STAGE_DEMOSAIC), ("nlm", _lib.DSGPU_STAGE_NLM),
                          ("cnn", _lib.DSGPU_STAGE_CNN), ("cnn_hidden", _lib.DSGPU_STAGE_CNN_HIDDEN)):
