@@ -36,7 +36,8 @@ DSGPU_STAGE_CNN_HIDDEN = 4
 # every symbol include/dsgpu.h and include/dsgpu_scene.h declare
 EXPORTS = [
     "dsgpu_strerror", "dsgpu_abi_version", "dsgpu_create", "dsgpu_destroy", "dsgpu_set_stream",
-    "dsgpu_get_stream", "dsgpu_synchronize", "dsgpu_trim", "dsgpu_last_error", "dsgpu_normalize_u16",
+    "dsgpu_get_stream", "dsgpu_synchronize", "dsgpu_trim", "dsgpu_last_error", "dsgpu_set_black_pattern",
+    "dsgpu_normalize_u16",
     "dsgpu_clip_plane", "dsgpu_mhc", "dsgpu_rcd", "dsgpu_demosaic", "dsgpu_box_blur", "dsgpu_nlm",
     "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_estimate_noise", "dsgpu_guided_filter",
     "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_cnn_param_count", "dsgpu_cnn_create", "dsgpu_cnn_destroy",
@@ -114,6 +115,7 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_last_error.argtypes = [vp]
             L.dsgpu_last_error.restype = ctypes.c_char_p
             L.dsgpu_normalize_u16.argtypes = [vp, vp, i, i, sz, vp, f, vp, vp, u]
+            L.dsgpu_set_black_pattern.argtypes = [vp, vp, i, i, i, i]
             L.dsgpu_clip_plane.argtypes = [vp, vp, i, i, vp, u]
             L.dsgpu_mhc.argtypes = [vp, vp, i, i, vp, vp, vp, u]
             L.dsgpu_rcd.argtypes = [vp, vp, i, i, vp, vp, vp, u]
@@ -193,6 +195,24 @@ class Context:
 
     def synchronize(self) -> None:
         self.check(lib().dsgpu_synchronize(self.handle), "dsgpu_synchronize")
+
+    def set_black_pattern(self, levels=None, origin=(0, 0)) -> None:
+        """Per-site black levels for this context's u16 calls (load_raw's
+        black_at, decode.rs:266-270): ``levels`` a (bh, bw) array of up to
+        4 x 4, indexed at uncropped sensor coordinates; ``origin`` the crop
+        origin (x, y) of the frames passed. None clears it (the scalar black
+        arguments apply again)."""
+        import numpy as np
+
+        if levels is None:
+            self.check(lib().dsgpu_set_black_pattern(self.handle, None, 0, 0, 0, 0), "dsgpu_set_black_pattern")
+            return
+        a = np.ascontiguousarray(np.asarray(levels, np.float32))
+        if a.ndim != 2:
+            raise DsgpuError(DSGPU_ERR_ARG, "set_black_pattern", "levels must be a (bh, bw) array")
+        bh, bw = a.shape
+        self.check(lib().dsgpu_set_black_pattern(self.handle, ctypes.c_void_p(a.ctypes.data), int(bw), int(bh),
+                                                 int(origin[0]), int(origin[1])), "dsgpu_set_black_pattern")
 
     def profile(self, enable: bool) -> None:
         self.check(lib().dsgpu_profile(self.handle, int(bool(enable))), "dsgpu_profile")

@@ -308,7 +308,7 @@ int develop_pipelined(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
                              ctx->copy));
     DS_TRY(cudaEventRecord(up_ev[c], ctx->copy));
   }
-  const ds_src_u16 src{(const uint16_t*)draw, pitch, black, {white[0], white[1], white[2]}};
+  const ds_src_u16 src = u16_source(ctx, draw, pitch, black, white);
   const int rcd_rows = (h + DS_RCD_TILE - 1) / DS_RCD_TILE;
   int tx, ty, tw, th;
   ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
@@ -506,6 +506,24 @@ int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s) {
   return DSGPU_OK;
 }
 
+int dsgpu_set_black_pattern(dsgpu_ctx* ctx, const float* levels, int bw, int bh, int origin_x, int origin_y) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  if (bw == 0 && bh == 0) {
+    ctx->black_bw = ctx->black_bh = 0;
+    return DSGPU_OK;
+  }
+  if (!levels || bw < 1 || bh < 1 || bw > DS_BLACK_MAX || bh > DS_BLACK_MAX || origin_x < 0 || origin_y < 0)
+    return DSGPU_ERR_ARG;
+  for (int i = 0; i < bw * bh; i++)
+    if (!(levels[i] == levels[i])) return DSGPU_ERR_ARG;  // NaN
+  ctx->black_bw = bw;
+  ctx->black_bh = bh;
+  ctx->black_x0 = origin_x % bw;
+  ctx->black_y0 = origin_y % bh;
+  for (int i = 0; i < DS_BLACK_MAX * DS_BLACK_MAX; i++) ctx->black_pat[i] = i < bw * bh ? levels[i] : 0.f;
+  return DSGPU_OK;
+}
+
 int dsgpu_normalize_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t pitch, const uint8_t cfa[4],
                         float black, const float white[3], float* out, unsigned flags) {
   if (!ctx) return DSGPU_ERR_ARG;
@@ -520,7 +538,7 @@ int dsgpu_normalize_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_
   void* dout;
   DS_CHECK(stage_in(ctx, flags, S_IN, raw, ((size_t)(h - 1) * pitch + w) * sizeof(uint16_t), &din));
   DS_CHECK(stage_out_ptr(ctx, flags, S_OUT, out, n * sizeof(float), &dout));
-  DS_TRY(ds_launch_normalize_u16(ctx->stream, (const uint16_t*)din, w, h, pitch, pat, black, white, (float*)dout));
+  DS_TRY(ds_launch_normalize_src(ctx->stream, u16_source(ctx, din, pitch, black, white), w, h, pat, (float*)dout));
   ctx->launches += 1;
   return finish(ctx, flags, out, dout, n * sizeof(float));
 }
@@ -692,11 +710,11 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
   unsigned* hl_bits = hl ? reinterpret_cast<unsigned*>(static_cast<char*>(hl_work) + ds_highlights_scratch_bytes(w, h))
                          : nullptr;
   float* hl_rc = hl ? reinterpret_cast<float*>(hl_bits + 8) : nullptr;
-  ds_src_u16 src{(const uint16_t*)din, pitch, black, {white[0], white[1], white[2]}};
+  const ds_src_u16 src = u16_source(ctx, din, pitch, black, white);
   if (w < 16 || h < 16) {
     void* cfa_f;
     DS_CHECK(scratch(ctx, S_CFA, n * sizeof(float), &cfa_f));
-    DS_TRY(ds_launch_normalize_u16(ctx->stream, (const uint16_t*)din, w, h, pitch, pat, black, white, (float*)cfa_f));
+    DS_TRY(ds_launch_normalize_src(ctx->stream, src, w, h, pat, (float*)cfa_f));
     ctx->launches += 1;
     DS_CHECK(rcd_dev(ctx, (const float*)cfa_f, w, h, pat, mul, (float*)mid, hl_clip));
   } else {
@@ -1113,7 +1131,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
                              ctx->copy));
     DS_TRY(cudaEventRecord(up_ev[c], ctx->copy));
   }
-  const ds_src_u16 src{(const uint16_t*)draw, pitch, black, {white[0], white[1], white[2]}};
+  const ds_src_u16 src = u16_source(ctx, draw, pitch, black, white);
   const int rcd_rows = (h + DS_RCD_TILE - 1) / DS_RCD_TILE;
   const int reach = halo > search + patch + 1 ? halo : search + patch + 1;  // RCD rows a band reads past its end
   int rcd_next = 0, chunks_waited = 0;
@@ -1178,7 +1196,7 @@ int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* c, const uint16_t* raw, int
   DS_CHECK(fallback_scratch(ctx, w, h, patch, &fl, &cnt));
   {
     StageMark mark(ctx, DSGPU_STAGE_DEMOSAIC);
-    ds_src_u16 src{(const uint16_t*)din, pitch, black, {white[0], white[1], white[2]}};
+    const ds_src_u16 src = u16_source(ctx, din, pitch, black, white);
     DS_TRY(ds_launch_rcd_u16(ctx->stream, src, w, h, pat, mul, (float*)mid, (float*)dclip));
     ctx->launches += 1;
   }

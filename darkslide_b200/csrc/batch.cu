@@ -138,6 +138,7 @@ void describe(ds_batch_frame& d, const dsgpu_frame& fr, ds_pat pat, int shape, i
   d.src.data = fr.raw;
   d.src.pitch = fr.pitch_elems;
   d.src.black = fr.black;
+  d.src.bw = d.src.bh = d.src.bx0 = d.src.by0 = 0;  // one black level per frame
   for (int c = 0; c < 3; c++) {
     d.src.white[c] = fr.white[c];
     d.mul[c] = fr.mul[c];

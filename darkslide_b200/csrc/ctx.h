@@ -30,7 +30,24 @@ struct dsgpu_ctx {
   DsBatch* batch = nullptr;         // batched develop: descriptors, graph, autotune table
   cudaStream_t copy = nullptr;      // host-buffer calls: device-to-host copies overlapping compute
   std::vector<cudaEvent_t> band_ev; // one per band of a pipelined call
+  // per-site black levels for the u16 entry points (dsgpu_set_black_pattern); bw == 0: none
+  int black_bw = 0, black_bh = 0, black_x0 = 0, black_y0 = 0;
+  float black_pat[DS_BLACK_MAX * DS_BLACK_MAX] = {};
 };
+
+// The u16 source of a call: the scalar black level, or the context's pattern.
+inline ds_src_u16 u16_source(const dsgpu_ctx* ctx, const void* data, size_t pitch, float black,
+                             const float white[3]) {
+  ds_src_u16 s{static_cast<const uint16_t*>(data), pitch, black, {white[0], white[1], white[2]}};
+  if (ctx->black_bw > 0) {
+    s.bw = ctx->black_bw;
+    s.bh = ctx->black_bh;
+    s.bx0 = ctx->black_x0;
+    s.by0 = ctx->black_y0;
+    for (int i = 0; i < DS_BLACK_MAX * DS_BLACK_MAX; i++) s.bpat[i] = ctx->black_pat[i];
+  }
+  return s;
+}
 
 // Makes ctx->device current for the duration of a call and restores the
 // caller's device afterwards.

@@ -21,12 +21,22 @@ struct ds_src_f32 {  // normalised float CFA (CfaImage::data)
   const float* data;
   int pitch;  // elements
 };
-struct ds_src_u16 {  // integer raw + the normalisation of decode.rs:303
+constexpr int DS_BLACK_MAX = 4;  // black-level patterns of up to 4 x 4 sites
+struct ds_src_u16 {  // integer raw + the normalisation of decode.rs:292-306
   const uint16_t* data;
   size_t pitch;  // elements
-  float black;
+  float black;   // the black level of every site while bw == 0
   float white[3];
+  // Per-site black levels (black_at, decode.rs:266-270): site (x, y) of the
+  // frame takes bpat[((y + by0) % bh) * bw + (x + bx0) % bw], the pattern
+  // being indexed at uncropped sensor coordinates (x + crop_x, y + crop_y).
+  // bw == 0 (an aggregate initialisation that stops after `white`): `black`.
+  int bw, bh, bx0, by0;
+  float bpat[DS_BLACK_MAX * DS_BLACK_MAX];
 };
+__host__ __device__ __forceinline__ float ds_black_at(const ds_src_u16& s, int x, int y) {
+  return s.bw ? s.bpat[((y + s.by0) % s.bh) * s.bw + (x + s.bx0) % s.bw] : s.black;
+}
 
 // One frame of a batched develop (u16 raw -> RCD -> NLM), as the batched
 // kernels read it from device memory. Tiles of all frames are numbered
@@ -74,6 +84,7 @@ float ds_nlm_sigma(float h_param, int patch);
 // kernel launchers (return cudaGetLastError() of the launch)
 cudaError_t ds_launch_normalize_u16(cudaStream_t st, const uint16_t* raw, int w, int h, size_t pitch, ds_pat pat,
                                     float black, const float white[3], float* out);
+cudaError_t ds_launch_normalize_src(cudaStream_t st, const ds_src_u16& src, int w, int h, ds_pat pat, float* out);
 cudaError_t ds_launch_clip_plane(cudaStream_t st, const float* cfa, int w, int h, float* out);
 cudaError_t ds_launch_mhc(cudaStream_t st, const float* cfa, int w, int h, ds_pat pat, const float mul[3],
                           float* out_rgb);

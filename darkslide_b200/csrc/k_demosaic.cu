@@ -19,14 +19,13 @@ __device__ __forceinline__ float norm_u16(uint16_t raw, float black, float white
   return __fdiv_rn((float)raw - black, fmaxf(white_c - black, 1.0f));
 }
 
-__global__ void normalize_u16_kernel(const uint16_t* __restrict__ raw, int w, int h, size_t pitch, ds_pat pat,
-                                     float black, float w0, float w1, float w2, float* __restrict__ out) {
+__global__ void normalize_u16_kernel(const ds_src_u16 src, int w, int h, ds_pat pat, float* __restrict__ out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= w) return;
   const int c = pat.at(x, y);
-  const float wc = c == 0 ? w0 : (c == 1 ? w1 : w2);
-  out[(size_t)y * w + x] = norm_u16(raw[(size_t)y * pitch + x], black, wc);
+  const float wc = c == 0 ? src.white[0] : (c == 1 ? src.white[1] : src.white[2]);
+  out[(size_t)y * w + x] = norm_u16(src.data[(size_t)y * src.pitch + x], ds_black_at(src, x, y), wc);
 }
 
 // ---------------------------------------------------------------- clip plane
@@ -159,7 +158,7 @@ struct SrcU16 {
   ds_src_u16 s;
   __device__ __forceinline__ float load(int gx, int gy, int c) const {
     const float wc = c == 0 ? s.white[0] : (c == 1 ? s.white[1] : s.white[2]);
-    return norm_u16(s.data[(size_t)gy * s.pitch + gx], s.black, wc);
+    return norm_u16(s.data[(size_t)gy * s.pitch + gx], ds_black_at(s, gx, gy), wc);
   }
 };
 
@@ -702,11 +701,16 @@ cudaError_t launch_rcd(cudaStream_t st, Src src, int w, int h, ds_pat pat, const
 
 }  // namespace
 
+cudaError_t ds_launch_normalize_src(cudaStream_t st, const ds_src_u16& src, int w, int h, ds_pat pat, float* out) {
+  dim3 grid((w + 255) / 256, h);
+  normalize_u16_kernel<<<grid, 256, 0, st>>>(src, w, h, pat, out);
+  return cudaGetLastError();
+}
+
 cudaError_t ds_launch_normalize_u16(cudaStream_t st, const uint16_t* raw, int w, int h, size_t pitch, ds_pat pat,
                                     float black, const float white[3], float* out) {
-  dim3 grid((w + 255) / 256, h);
-  normalize_u16_kernel<<<grid, 256, 0, st>>>(raw, w, h, pitch, pat, black, white[0], white[1], white[2], out);
-  return cudaGetLastError();
+  const ds_src_u16 src{raw, pitch, black, {white[0], white[1], white[2]}};
+  return ds_launch_normalize_src(st, src, w, h, pat, out);
 }
 
 cudaError_t ds_launch_clip_plane(cudaStream_t st, const float* cfa, int w, int h, float* out) {

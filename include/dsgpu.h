@@ -110,6 +110,17 @@ int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops_per_s, double* ex2_pe
 /* BF16 mma.sync (m16n8k16, FP32 accumulate) throughput microbenchmark. */
 int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s);
 
+/* Per-site black levels, as load_raw's black_at takes them from the raw's
+ * black-level record (decode.rs:266-270): a bw x bh pattern (1..4 each, row
+ * major, one value per site) indexed at UNCROPPED sensor coordinates, so
+ * that site (x, y) of a frame cropped at (origin_x, origin_y) subtracts
+ * levels[((y + origin_y) % bh) * bw + (x + origin_x) % bw]. While a pattern
+ * is set, every u16 entry point of this context (dsgpu_normalize_u16,
+ * dsgpu_develop_u16, dsgpu_develop_u16_cnn) uses it in place of its scalar
+ * black argument, in the numerator and in the white - black denominator
+ * alike (decode.rs:303). bw = bh = 0 clears it. The batch and the no-alloc
+ * entry points take the scalar black only. */
+int dsgpu_set_black_pattern(dsgpu_ctx* ctx, const float* levels, int bw, int bh, int origin_x, int origin_y);
 /* CFA normalisation of an integer raw: out = (raw - black) / max(white[c] - black, 1),
  * c the colour of the site; values are not clamped.
  * Replaces the integer branch of load_raw, decode.rs:292-306 (formula :303). */

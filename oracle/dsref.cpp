@@ -723,6 +723,23 @@ void dsref_normalize_u16(const uint16_t* raw, int w, int h, size_t pitch, const 
     }
 }
 
+// The same with load_raw's per-site black level (decode.rs:266-270): black_at
+// is the bw x bh pattern at UNCROPPED coordinates (x + ox, y + oy), used in
+// the numerator and in the white - black denominator of :303.
+void dsref_normalize_u16_bp(const uint16_t* raw, int w, int h, size_t pitch, const uint8_t cfa[4],
+                            const float* levels, int bw, int bh, int ox, int oy, const float white[3], float* out) {
+  Pat pat;
+  std::memcpy(pat.c, cfa, 4);
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < h; y++)
+    for (long x = 0; x < w; x++) {
+      const int c = pat.at(x, y);
+      const float raw_v = (float)raw[y * pitch + x];
+      const float b = levels[((y + oy) % bh) * bw + (x + ox) % bw];
+      out[y * w + x] = (raw_v - b) / std::fmax(white[c] - b, 1.0f);
+    }
+}
+
 void dsref_clip_plane_f32(const float* cfa, int w, int h, float* out) { clip_plane<float>(cfa, w, h, out); }
 
 void dsref_mhc_f32(const float* cfa, int w, int h, const uint8_t pat[4], const float mul[3], float* out) {

@@ -43,6 +43,7 @@ def lib():
         L.dsref_omp_threads.restype = i
         L.dsref_set_threads.argtypes = [i]
         L.dsref_normalize_u16.argtypes = [_u16p, i, i, sz, _u8p, f, _f32p, _f32p]
+        L.dsref_normalize_u16_bp.argtypes = [_u16p, i, i, sz, _u8p, _f32p, i, i, i, i, _f32p, _f32p]
         L.dsref_clip_plane_f32.argtypes = [_f32p, i, i, _f32p]
         L.dsref_mhc_f32.argtypes = [_f32p, i, i, _u8p, _f32p, _f32p]
         L.dsref_superpixel_f32.argtypes = [_f32p, i, i, _u8p, _f32p, _f32p, _f32p]
@@ -85,6 +86,19 @@ def normalize_u16(raw: np.ndarray, cfa, black: float, white) -> np.ndarray:
     out = np.empty((h, w), np.float32)
     wh = np.ascontiguousarray(np.broadcast_to(np.asarray(white, np.float32), (3,)))
     lib().dsref_normalize_u16(raw, w, h, w, _pat(cfa), float(black), wh, out)
+    return out
+
+
+def normalize_u16_bp(raw: np.ndarray, cfa, levels, origin, white) -> np.ndarray:
+    """decode.rs:266-306 with a per-site black pattern ``levels`` (bh, bw),
+    indexed at uncropped coordinates (x + origin[0], y + origin[1])."""
+    raw = np.ascontiguousarray(raw, dtype=np.uint16)
+    h, w = raw.shape
+    lv = np.ascontiguousarray(np.asarray(levels, np.float32))
+    bh, bw = lv.shape
+    out = np.empty((h, w), np.float32)
+    wh = np.ascontiguousarray(np.broadcast_to(np.asarray(white, np.float32), (3,)))
+    lib().dsref_normalize_u16_bp(raw, w, h, w, _pat(cfa), lv.ravel(), bw, bh, int(origin[0]), int(origin[1]), wh, out)
     return out
 
 

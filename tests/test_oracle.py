@@ -201,3 +201,39 @@ def test_highlights_untouched_without_clipping(oracle):
     img = np.random.default_rng(3).uniform(0, 0.8, (20, 30, 3)).astype(np.float32)
     out = oracle.reconstruct_highlights(img, np.zeros((20, 30), np.float32), [2, 1, 1.4], [1.0, 1.0, 1.0])
     np.testing.assert_array_equal(out, img)
+
+
+def _norm_bp_numpy(raw, codes, levels, origin, white):
+    """decode.rs:266-306, restated with numpy float32 arithmetic."""
+    h, w = raw.shape
+    lv = np.asarray(levels, np.float32)
+    bh, bw = lv.shape
+    yy, xx = np.mgrid[0:h, 0:w]
+    b = lv[(yy + origin[1]) % bh, (xx + origin[0]) % bw]
+    c = np.asarray(codes, np.int64).reshape(2, 2)[yy % 2, xx % 2]
+    wc = np.asarray(white, np.float32)[c]
+    return ((raw.astype(np.float32) - b) / np.maximum(wc - b, np.float32(1.0))).astype(np.float32)
+
+
+@pytest.mark.parametrize("levels,origin", [([[512.0]], (0, 0)), ([[510.0, 514.0], [511.0, 517.5]], (0, 0)),
+                                           ([[510.0, 514.0], [511.0, 517.5]], (1, 3)),
+                                           ([[500, 501, 502, 503], [504, 505, 506, 507.25]], (5, 2))])
+def test_oracle_black_pattern(oracle, levels, origin):
+    """The per-site black level of load_raw (black_at, decode.rs:266-270) in
+    the oracle against a numpy restatement, bit for bit; a 1x1 pattern is the
+    scalar black; a frame cropped at `origin` equals the crop of the frame
+    normalised from the sensor origin."""
+    rng = np.random.default_rng(len(levels) * 7 + origin[0])
+    raw = rng.integers(0, 16384, (37, 53), dtype=np.uint16)
+    raw[0, :5] = [0, 1, 16383, 500, 517]  # below, at and above black; white
+    white = [16383.0, 15000.0, 16000.0]
+    codes = [1, 0, 2, 1]  # GRBG
+    got = oracle.normalize_u16_bp(raw, codes, levels, origin, white)
+    np.testing.assert_array_equal(got, _norm_bp_numpy(raw, codes, levels, origin, white))
+    if np.asarray(levels).size == 1:
+        np.testing.assert_array_equal(got, oracle.normalize_u16(raw, codes, float(levels[0][0]), white))
+    full = oracle.normalize_u16_bp(raw, codes, levels, (0, 0), white)
+    ox, oy = 2, 4  # crop: the pattern shifts with the crop origin (CfaPattern::shifted)
+    shifted = [codes[((oy + r) % 2) * 2 + (ox + q) % 2] for r in range(2) for q in range(2)]
+    crop = oracle.normalize_u16_bp(raw[oy:, ox:], shifted, levels, (ox, oy), white)
+    np.testing.assert_array_equal(crop, full[oy:, ox:])
