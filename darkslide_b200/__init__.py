@@ -296,7 +296,10 @@ def apply_orientation(img: "Image3", orientation: int, ctx: Context | None = Non
 class BatchFrame:
     """One frame of develop_batch: a CUDA uint16 tensor (h, w), its CFA
     pattern, levels, white balance and NLM strength; `out` (h, w, 3) and
-    optional `clip` (h, w) float32 CUDA tensors receive the result."""
+    optional `clip` (h, w) float32 CUDA tensors receive the result.
+    `black_pattern` (optional, (bh, bw) up to 4 x 4) gives per-site black
+    levels at uncropped coordinates, `black_origin` the frame's crop origin
+    (load_raw's black_at); without it the scalar `black` applies."""
     raw: object
     pattern: "CfaPattern"
     black: float
@@ -305,6 +308,8 @@ class BatchFrame:
     h_param: float
     out: object
     clip: object = None
+    black_pattern: object = None
+    black_origin: tuple = (0, 0)
 
 
 def develop_batch(frames, search: int, patch: int, ctx: Context | None = None, sync: bool = True) -> None:
@@ -318,6 +323,7 @@ def develop_batch(frames, search: int, patch: int, ctx: Context | None = None, s
     cx = ctx or default_context(dev.index or 0)
     cx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
     arr = (_lib.Frame * len(frames))()
+    keep = []  # black patterns, alive for the call
     for d, f in zip(arr, frames):
         h, w = f.raw.shape
         d.raw = f.raw.data_ptr()
@@ -330,6 +336,14 @@ def develop_batch(frames, search: int, patch: int, ctx: Context | None = None, s
         d.h_param = float(f.h_param)
         d.out_rgb = f.out.data_ptr()
         d.out_clip = f.clip.data_ptr() if f.clip is not None else None
+        if f.black_pattern is not None:
+            bp = np.ascontiguousarray(np.asarray(f.black_pattern, np.float32))
+            if bp.ndim != 2:
+                raise DsgpuError(_lib.DSGPU_ERR_ARG, "develop_batch", "black_pattern must be a (bh, bw) array")
+            keep.append(bp)
+            d.black_pattern = bp.ctypes.data
+            d.black_h, d.black_w = bp.shape
+            d.black_x0, d.black_y0 = int(f.black_origin[0]), int(f.black_origin[1])
     flags = 0 if sync else _lib.DSGPU_ASYNC
     cx.check(lib().dsgpu_rcd_nlm_batch(cx.handle, arr, len(frames), int(search), int(patch), flags),
              "dsgpu_rcd_nlm_batch")

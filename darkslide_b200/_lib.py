@@ -72,6 +72,11 @@ class Frame(ctypes.Structure):
         ("h_param", ctypes.c_float),
         ("out_rgb", ctypes.c_void_p),
         ("out_clip", ctypes.c_void_p),
+        ("black_pattern", ctypes.c_void_p),
+        ("black_w", ctypes.c_int),
+        ("black_h", ctypes.c_int),
+        ("black_x0", ctypes.c_int),
+        ("black_y0", ctypes.c_int),
     ]
 
 

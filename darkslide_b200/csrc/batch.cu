@@ -138,7 +138,15 @@ void describe(ds_batch_frame& d, const dsgpu_frame& fr, ds_pat pat, int shape, i
   d.src.data = fr.raw;
   d.src.pitch = fr.pitch_elems;
   d.src.black = fr.black;
-  d.src.bw = d.src.bh = d.src.bx0 = d.src.by0 = 0;  // one black level per frame
+  d.src.bw = d.src.bh = d.src.bx0 = d.src.by0 = 0;  // the scalar black level, unless the frame has a pattern
+  for (int i = 0; i < DS_BLACK_MAX * DS_BLACK_MAX; i++) d.src.bpat[i] = 0.f;
+  if (fr.black_pattern) {
+    d.src.bw = fr.black_w;
+    d.src.bh = fr.black_h;
+    d.src.bx0 = fr.black_x0 % fr.black_w;
+    d.src.by0 = fr.black_y0 % fr.black_h;
+    for (int i = 0; i < fr.black_w * fr.black_h; i++) d.src.bpat[i] = fr.black_pattern[i];
+  }
   for (int c = 0; c < 3; c++) {
     d.src.white[c] = fr.white[c];
     d.mul[c] = fr.mul[c];
@@ -168,6 +176,13 @@ int check_frame(const dsgpu_frame& f, ds_pat* pat) {
   if (f.w < 16 || f.h < 16) return DSGPU_ERR_UNSUPPORTED;  // the reference's MHC case: one-frame calls
   if (f.w > DSGPU_MAX_DIM || f.h > DSGPU_MAX_DIM) return DSGPU_ERR_SIZE;
   if (f.pitch_elems < (size_t)f.w) return DSGPU_ERR_ARG;
+  if (f.black_pattern) {
+    if (f.black_w < 1 || f.black_h < 1 || f.black_w > DS_BLACK_MAX || f.black_h > DS_BLACK_MAX || f.black_x0 < 0 ||
+        f.black_y0 < 0)
+      return DSGPU_ERR_ARG;
+    for (int i = 0; i < f.black_w * f.black_h; i++)
+      if (!(f.black_pattern[i] == f.black_pattern[i])) return DSGPU_ERR_ARG;  // NaN
+  }
   pat->packed = 0;
   for (int i = 0; i < 4; i++) {
     if (f.cfa[i] > 2) return DSGPU_ERR_CFA;

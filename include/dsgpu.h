@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define DSGPU_ABI_VERSION 1
+#define DSGPU_ABI_VERSION 2
 
 /* status codes */
 #define DSGPU_OK 0
@@ -118,8 +118,9 @@ int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s);
  * is set, every u16 entry point of this context (dsgpu_normalize_u16,
  * dsgpu_develop_u16, dsgpu_develop_u16_cnn) uses it in place of its scalar
  * black argument, in the numerator and in the white - black denominator
- * alike (decode.rs:303). bw = bh = 0 clears it. The batch and the no-alloc
- * entry points take the scalar black only. */
+ * alike (decode.rs:303). bw = bh = 0 clears it. A batch takes its patterns
+ * per frame (dsgpu_frame.black_pattern); the no-alloc entry point takes the
+ * scalar black only. */
 int dsgpu_set_black_pattern(dsgpu_ctx* ctx, const float* levels, int bw, int bh, int origin_x, int origin_y);
 /* CFA normalisation of an integer raw: out = (raw - black) / max(white[c] - black, 1),
  * c the colour of the site; values are not clamped.
@@ -250,6 +251,13 @@ typedef struct dsgpu_frame {
   float h_param;        /* NLM strength of this frame */
   float* out_rgb;       /* device, w*h*3 */
   float* out_clip;      /* device, w*h, or NULL */
+  /* Per-site black levels of this frame (as dsgpu_set_black_pattern, at
+   * uncropped coordinates; the context's own pattern does not apply to a
+   * batch): host pointer to black_w * black_h levels (1..4 each), or NULL
+   * for the scalar black. */
+  const float* black_pattern;
+  int black_w, black_h;
+  int black_x0, black_y0; /* the frame's crop origin */
 } dsgpu_frame;
 #define DSGPU_BATCH_MAX 256
 /* Device pointers only (DSGPU_HOST -> DSGPU_ERR_UNSUPPORTED); search >= 1.

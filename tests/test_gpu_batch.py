@@ -127,3 +127,28 @@ def test_batch_argument_errors(env):
     with pytest.raises(ds.DsgpuError):
         ds.develop_batch(small, 10, 3, ctx=ctx)
     assert ds.autotune_get(100, 100, ctx=ds.Context(0))["rcd_tile"] == (32, 32)  # empty table: the default
+
+
+def test_batch_black_patterns(env):
+    """Per-frame black patterns (dsgpu_frame.black_pattern): each frame of a
+    batch equals the one-frame develop under the same context pattern, bit
+    for bit; a frame without one keeps its scalar black."""
+    torch, dev = env
+    ctx = ds.Context(0)
+    frames = make_frames(torch, dev, CASES[:3], seed=300)
+    pats = [([[500.0, 507.0], [503.0, 519.0]], (1, 0)), None, ([[250, 251, 252, 253], [254, 255, 256, 257]], (3, 1))]
+    for f, p in zip(frames, pats):
+        if p is not None:
+            f.black_pattern, f.black_origin = p
+    ds.develop_batch(frames, 10, 3, ctx=ctx)
+    for f, p in zip(frames, pats):
+        one = ds.Context(0)
+        if p is not None:
+            one.set_black_pattern(*p)
+        rgb, clip = single(f, 10, 3, one)
+        np.testing.assert_array_equal(f.out.cpu().numpy(), rgb)
+        np.testing.assert_array_equal(f.clip.cpu().numpy(), clip)
+    bad = make_frames(torch, dev, CASES[:1], seed=301)
+    bad[0].black_pattern = [[512.0] * 5]  # 5 wide: more than 4
+    with pytest.raises(ds.DsgpuError):
+        ds.develop_batch(bad, 10, 3, ctx=ctx)

@@ -42,7 +42,7 @@ def test_library_exports_every_declared_symbol(L):
 
 
 def test_abi_version_and_strerror(L):
-    assert L.dsgpu_abi_version() == 1
+    assert L.dsgpu_abi_version() == 2
     for code in range(-8, 1):
         assert _lib.strerror(code) != "unknown status"
     assert _lib.strerror(-99) == "unknown status"
