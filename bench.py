@@ -539,6 +539,10 @@ def run_ours(args):
             "value": learned["value"], "ms_per_step": learned["ms_per_step"], "e2e": learned_e2e,
             "speedup_vs_plain": learned["value"] / plain["value"],
             "e2e_speedup_vs_plain": learned_e2e["value"] / plain_e2e["value"],
+            # the denoisers alone: network + residual check + fallback against plain NLM (same frame,
+            # stage events on the launching stream), i.e. without the RCD both paths share
+            "denoise_speedup_vs_plain_nlm": (plain["nlm"][0] / learned["cnn"][0]
+                                             if learned["cnn"][0] > 0 and plain["nlm"][0] > 0 else None),
             "stage_ms_per_step": {"demosaic": learned["demosaic"][0] / args.steps,
                                   "cnn_with_fallback": learned["cnn"][0] / args.steps},
             "gpu_launches": learned["launches"], "fallback_tiles": nf.value, "tiles": tiles, "tau": TAU,
