@@ -37,6 +37,7 @@ DSGPU_STAGE_CNN_HIDDEN = 4
 EXPORTS = [
     "dsgpu_strerror", "dsgpu_abi_version", "dsgpu_create", "dsgpu_destroy", "dsgpu_set_stream",
     "dsgpu_get_stream", "dsgpu_synchronize", "dsgpu_trim", "dsgpu_last_error", "dsgpu_set_black_pattern",
+    "dsgpu_selftest_batch_timeout",
     "dsgpu_normalize_u16",
     "dsgpu_clip_plane", "dsgpu_mhc", "dsgpu_rcd", "dsgpu_demosaic", "dsgpu_box_blur", "dsgpu_nlm",
     "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_estimate_noise", "dsgpu_guided_filter",
@@ -121,6 +122,7 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_last_error.restype = ctypes.c_char_p
             L.dsgpu_normalize_u16.argtypes = [vp, vp, i, i, sz, vp, f, vp, vp, u]
             L.dsgpu_set_black_pattern.argtypes = [vp, vp, i, i, i, i]
+            L.dsgpu_selftest_batch_timeout.argtypes = [vp]
             L.dsgpu_clip_plane.argtypes = [vp, vp, i, i, vp, u]
             L.dsgpu_mhc.argtypes = [vp, vp, i, i, vp, vp, vp, u]
             L.dsgpu_rcd.argtypes = [vp, vp, i, i, vp, vp, vp, u]

@@ -289,6 +289,58 @@ int dsgpu_rcd_nlm_batch(dsgpu_ctx* ctx, const dsgpu_frame* frames, int n, int se
   return DSGPU_OK;
 }
 
+// Failure detection on the device, without a fault: one NLM work item whose
+// frame's demosaic (one RCD tile) is never queued, so the item's bounded wait
+// on the frame's RCD counter can only run out; the kernel then records
+// DSGPU_ERR_TIMEOUT in its status word and returns, and the stream and the
+// context stay usable. The NLM tile body is never reached (its buffers are
+// allocated all the same).
+int dsgpu_selftest_batch_timeout(dsgpu_ctx* ctx) {
+  if (!ctx) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  constexpr int FW = 64, FH = 58;
+  ds_batch_frame f{};
+  f.w = FW;
+  f.h = FH;
+  f.pat.packed = 0u | (1u << 8) | (1u << 16) | (2u << 24);
+  f.mul[0] = f.mul[1] = f.mul[2] = 1.f;
+  f.sigma = 1.f;
+  f.rcd_tiles = 1;  // waited for, never produced
+  f.nlm_tiles_x = 1;
+  f.nlm_tiles_y = 1;
+  const ds_batch_seg seg{1, 0, 0};  // one NLM item of frame 0
+  ds_batch_frame* df = nullptr;
+  ds_batch_seg* ds = nullptr;
+  int* dc = nullptr;
+  unsigned long long* dst = nullptr;
+  float* buf = nullptr;
+  int status = DSGPU_OK, h = 0;
+  cudaError_t e = cudaMalloc(&buf, (size_t)2 * FW * FH * 3 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&df, sizeof(ds_batch_frame));
+  if (e == cudaSuccess) e = cudaMalloc(&ds, sizeof(ds_batch_seg));
+  if (e == cudaSuccess) e = cudaMalloc(&dc, (size_t)ds_batch_ctr_nlm(1) * sizeof(int) + sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&dst, sizeof(unsigned long long));
+  if (e == cudaSuccess) {
+    f.rgb = buf;
+    f.out = buf + (size_t)FW * FH * 3;
+    e = cudaMemcpyAsync(df, &f, sizeof f, cudaMemcpyHostToDevice, ctx->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ds, &seg, sizeof seg, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(dc, 0, (size_t)ds_batch_ctr_nlm(1) * sizeof(int) + sizeof(int), ctx->stream);
+  if (e == cudaSuccess) e = ds_launch_batch_fused(ctx->stream, df, 1, ds, 1, 1, 3, 3, 1, dc, 1, dst);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, dc + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) status = map_cuda(ctx, e, "dsgpu_selftest_batch_timeout");
+  else status = h;
+  cudaFree(dst);
+  cudaFree(dc);
+  cudaFree(ds);
+  cudaFree(df);
+  cudaFree(buf);
+  return status;  // DSGPU_ERR_TIMEOUT when the wait gave up as designed
+}
+
 int dsgpu_batch_frame_ms(dsgpu_ctx* ctx, double* frame_ms, int n) {
   if (!ctx || !frame_ms || n < 0) return DSGPU_ERR_ARG;
   DsBatch* b = ctx->batch;

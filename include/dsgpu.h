@@ -267,6 +267,12 @@ typedef struct dsgpu_frame {
  * frame pointers and levels may change between calls. RCD tile shapes come
  * from the context's autotune table (dsgpu_autotune), else 32 x 32. */
 int dsgpu_rcd_nlm_batch(dsgpu_ctx* ctx, const dsgpu_frame* frames, int n, int search, int patch, unsigned flags);
+/* Failure-detection self-test (no counterpart in the reference): runs the
+ * batched kernel on one NLM work item whose frame's demosaic is never queued,
+ * so the item's bounded wait (2 s of device clock) must give up. Returns
+ * DSGPU_ERR_TIMEOUT when it does, the context staying usable; DSGPU_OK would
+ * mean the wait did not end as designed. Allocates its own small buffers. */
+int dsgpu_selftest_batch_timeout(dsgpu_ctx* ctx);
 /* Completion time of each frame of the last batch, ms after the batch started
  * on the device (measured with the device clock; waits for the batch).
  * Returns the batch's own status when it stopped early (DSGPU_ERR_TIMEOUT). */

@@ -152,3 +152,24 @@ def test_batch_black_patterns(env):
     bad[0].black_pattern = [[512.0] * 5]  # 5 wide: more than 4
     with pytest.raises(ds.DsgpuError):
         ds.develop_batch(bad, 10, 3, ctx=ctx)
+
+
+def test_bounded_wait_reports_timeout(env):
+    """Failure detection without a fault: a work item whose frame's demosaic
+    is never queued waits in vain; its bounded wait (2 s of device clock)
+    gives up, the call returns DSGPU_ERR_TIMEOUT, and the same context then
+    develops a batch correctly."""
+    import time
+
+    torch, dev = env
+    ctx = ds.Context(0)
+    L = _lib.lib()
+    t0 = time.perf_counter()
+    assert L.dsgpu_selftest_batch_timeout(ctx.handle) == _lib.DSGPU_ERR_TIMEOUT
+    dt = time.perf_counter() - t0
+    assert 1.5 < dt < 20.0, dt
+    frames = make_frames(torch, dev, CASES[:2], seed=500)
+    ds.develop_batch(frames, 10, 3, ctx=ctx)
+    for f in frames:
+        rgb, _ = single(f, 10, 3, ctx)
+        np.testing.assert_array_equal(f.out.cpu().numpy(), rgb)
