@@ -7,6 +7,7 @@
     python -m darkslide_b200.profile_case cnn      # the learned stand-in (8 conv layers)
     python -m darkslide_b200.profile_case learned  # u16 -> RCD -> network + NLM fallback (committed weights)
     python -m darkslide_b200.profile_case batch --frames 8 --w 2048 --h 1536   # one batched graph launch
+    python -m darkslide_b200.profile_case mma      # tcgen05 MMA issue rate vs N and commit spacing
 
 Each case does one warm-up call and `--reps` timed calls on cuda:0 and
 prints the mean device time per call (CUDA events).
@@ -25,7 +26,7 @@ from darkslide_b200 import _lib
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise", "cnn", "learned", "batch"])
+    ap.add_argument("case", choices=["nlm", "rcd", "develop", "denoise", "cnn", "learned", "batch", "mma"])
     ap.add_argument("--frames", type=int, default=8, help="batch: frames of w x h")
     ap.add_argument("--w", type=int, default=0)
     ap.add_argument("--h", type=int, default=0)
@@ -34,6 +35,15 @@ def main():
     ap.add_argument("--patch", type=int, default=3)
     ap.add_argument("--fp16", action="store_true", help="NLM's FP16-staging precision variant")
     a = ap.parse_args()
+    if a.case == "mma":  # no frame: the microbenchmark alone
+        ctx = ds.Context(0)
+        commits = [0, 1, 2, 6, 12, 19, 57, 228]
+        print("SM cycles per 128 x N x 16 BF16 tcgen05 MMA (4096 back to back per SM, all SMs)")
+        print("commit every:" + "".join(f"{c:>8}" for c in commits))
+        for n in (48, 96, 144, 256):
+            row = [ctx.measure_tcgen05_mma(n, c) for c in commits]
+            print(f"N = {n:3d}     :" + "".join(f"{v:8.1f}" for v in row))
+        return
     xflags = _lib.DSGPU_FP16_STAGING if a.fp16 else 0
     dev = torch.device("cuda", 0)
     ctx = ds.Context(0)

@@ -109,6 +109,12 @@ unsigned long long dsgpu_launch_count(dsgpu_ctx* ctx);
 int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops_per_s, double* ex2_per_s, double* ffma2_flops_per_s);
 /* BF16 mma.sync (m16n8k16, FP32 accumulate) throughput microbenchmark. */
 int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s);
+/* tcgen05 MMA issue-rate microbenchmark (instrumentation, no counterpart in
+ * the reference): one thread per SM issues 4096 back-to-back 128 x n x 16
+ * BF16 MMAs from shared memory (n in 48, 96, 144, 256), with a
+ * tcgen05.commit after every `commit_every` of them (0, 1, 2, 6, 12, 19, 57
+ * or 228; 0: none); returns the mean SM cycles per MMA. */
+int dsgpu_measure_tcgen05_mma(dsgpu_ctx* ctx, int n, int commit_every, double* cycles_per_mma);
 
 /* Per-site black levels, as load_raw's black_at takes them from the raw's
  * black-level record (decode.rs:266-270): a bw x bh pattern (1..4 each, row
