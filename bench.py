@@ -48,7 +48,7 @@ BLACK, WHITE = 512, 16383
 GAIN, READ_SIGMA = 0.5, 6.0
 SEARCH, PATCH = 10, 3
 WB = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
-CPU_SAMPLE = (1536, 1024)  # oracle crop (w, h) of the same frame for the CPU baseline
+CPU_SAMPLE = (2048, 2048)  # oracle crop (w, h) of the same frame for the CPU legs
 WEIGHTS = os.path.join(ROOT, "darkslide_b200", "weights", "cnn_nlm.bin")
 TAU = 3.0                  # residual check of the learned path: NLM on tiles removing > TAU x sigma
 QUALITY_CROP = 2048        # central crop for PSNR against the noise-free scene
@@ -147,35 +147,60 @@ class Clocks:
                 "power_w_max": max(power) if power else None}
 
 
-def cpu_baseline(threads: int | None = None, repeats: int = 3) -> dict:
-    """The oracle (a C++ restatement of the reference's CPU path, OpenMP over
-    all host threads) on a crop of the same frame; returns Mpix/s."""
+def _oracle():
+    """The CPU oracle (oracle/libdsref.so), built on first use. The CPU legs
+    load nothing else: their input comes from the oracle's own copy of the
+    scene generator, so the GPU library is never mapped by them."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import dsref
-    import darkslide_b200 as ds
 
     dsref.build()
-    if threads:
-        dsref.set_threads(threads)
+    return dsref
+
+
+def cpu_sample():
+    """The CPU legs' bounded sample of the workload: the central
+    CPU_SAMPLE crop of the bench frame (same seed, levels and noise), its CFA
+    codes shifted to the crop origin as load_raw shifts them."""
+    dsref = _oracle()
     cw, ch = CPU_SAMPLE
     x0, y0 = (W - cw) // 2 & ~1, (H - ch) // 2 & ~1
-    sc = ds.Scene(seed=1, w=W, h=H, pattern=ds.RGGB, black=BLACK, white=WHITE, gain=GAIN, read_sigma=READ_SIGMA)
-    raw = sc.render_host(x0, y0, cw, ch)
+    rggb = np.array([0, 1, 1, 2], np.uint8)
+    raw = dsref.scene_render(1, W, H, rggb, BLACK, WHITE, GAIN, READ_SIGMA, x0, y0, cw, ch)
+    return raw, rggb  # x0, y0 even: the crop keeps the RGGB phase
+
+
+def cpu_step(dsref, raw, pat, nt: int) -> float:
+    """One pass of the reference's path over the sample (normalise, RCD,
+    clip plane, NLM on each channel); returns seconds."""
     white = np.full(3, WHITE, np.float32)
-    pat = ds.RGGB.shifted(x0, y0).codes()
-    times = []
+    t0 = time.perf_counter()
+    cfa = dsref.normalize_u16(raw, pat, BLACK, white)
+    rgb = dsref.rcd(cfa, pat, WB)
+    dsref.clip_plane(cfa)
+    dsref.nlm_rgb(rgb, h_param(), SEARCH, PATCH, nthreads=nt)
+    return time.perf_counter() - t0
+
+
+def cpu_sample_text() -> str:
+    cw, ch = CPU_SAMPLE
+    return (f"central {cw}x{ch} crop ({cw * ch / 1e6:.2f} MP) of the 6000x4000 bench frame, same seed and noise, "
+            "through the oracle (C++ restatement of the reference CPU path, OpenMP over all host threads; the "
+            "Rust reference cannot be built here): normalise + RCD + clip plane + NLM x3")
+
+
+def cpu_baseline(threads: int | None = None, repeats: int = 3) -> dict:
+    """The oracle timed on the bounded sample; returns Mpix/s of sensor pixels."""
+    dsref = _oracle()
+    if threads:
+        dsref.set_threads(threads)
+    raw, pat = cpu_sample()
     nt = dsref.threads()
-    for _ in range(repeats):
-        t0 = time.perf_counter()
-        cfa = dsref.normalize_u16(raw, pat, BLACK, white)
-        rgb = dsref.rcd(cfa, pat, WB)
-        dsref.clip_plane(cfa)
-        dsref.nlm_rgb(rgb, h_param(), SEARCH, PATCH, nthreads=nt)
-        times.append(time.perf_counter() - t0)
+    times = [cpu_step(dsref, raw, pat, nt) for _ in range(repeats)]
     t = statistics.median(times)
+    cw, ch = CPU_SAMPLE
     return {"value": cw * ch / t / 1e6, "unit": "Mpix/s", "cores": nt, "kind": "port",
-            "sample": f"{cw}x{ch} crop of the 6000x4000 frame (normalise+RCD+clip+NLM x3), median of {repeats}, "
-                      f"{t:.2f} s each", "seconds": t}
+            "sample": f"{cpu_sample_text()}; median of {repeats}, {t:.2f} s each", "seconds": t}
 
 
 def read_traffic() -> dict:
@@ -202,18 +227,20 @@ def dist_env():
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU path (the oracle port) on the
+    host cores, same metric, unit and config as ours; each step is one pass
+    over the bounded sample. Loads only oracle/libdsref.so."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import dsref
-
-    dsref.build()
+    dsref = _oracle()
+    raw, pat = cpu_sample()
+    nt = dsref.threads()
     times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(repeats=1)
+        t = cpu_step(dsref, raw, pat, nt)
         if i >= args.warmup:
-            times.append(r["seconds"])
+            times.append(t)
     t = sum(times) / len(times)
     cw, ch = CPU_SAMPLE
     v = cw * ch / t / 1e6
@@ -222,9 +249,9 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args.gpus),
-        "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": dsref.threads(), "kind": "port",
-                         "sample": f"each step: {cw}x{ch} crop of the 6000x4000 frame through the oracle "
-                                   "(C++ restatement of the reference CPU path; the Rust reference cannot be built here)"},
+        "sample": f"each step: {cpu_sample_text()}",
+        "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": nt, "kind": "port",
+                         "sample": f"each step: {cpu_sample_text()}"},
         "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -504,14 +531,10 @@ def run_ours(args):
             "algorithmic": f"{updates:.4g} exp per launch (W*H*3*(2S+1)^2, one exp per pixel, channel and offset)",
             "peak_source": "ex2.approx throughput microbenchmark on this GPU (dsgpu_measure_peaks)",
             "launch_ms": nlm_launch_ms, "fp32_peak_tflops": fl / 1e12, "fp32x2_peak_tflops": fl2 / 1e12,
-            "binding": {
-                "resource": "shared memory (LSU data pipe) and issue, jointly",
-                "shared_bytes_per_update": 16.5, "shared_pct_of_peak": 73.4, "issue_pct_of_peak": 72.3,
-                "shared_bound_updates_per_s": 128.0 / 16.5 * 148 * 1.965e9,
-                "frac_of_shared_bound": updates / (nlm_launch_ms * 1e-3) / (128.0 / 16.5 * 148 * 1.965e9),
-                "source": "profiles/nlm_tile_kernel_4096x3072_full.md (ncu --set full); bound = 128 B/clk/SM "
-                          "x 148 SMs x 1.965 GHz / 16.5 B per update",
-            },
+            "binding": {k[len("nlm_"):]: v for k, v in traffic.items()
+                        if k.startswith("nlm_") and k != "nlm_bytes_per_launch"} or None,
+            "binding_source": "ncu counters of one launch on 4096x3072x3, from profiles/dram_traffic.txt "
+                              "(shared-memory bytes and issue per (pixel, channel, offset) update)",
         }
         roof_rcd = {
             "kernel": "rcd_tile_kernel<SrcU16>", "bound": "hbm", "achieved": rcd_bytes / (dem_launch_ms * 1e-3) / 1e9,
@@ -588,6 +611,109 @@ def run_ours(args):
     return 0
 
 
+CASES = ("nlm", "rcd", "develop", "denoise", "cnn", "learned", "batch")
+
+
+def run_case(args):
+    """One stage of the path on its own, for profiler captures: one warm-up
+    call, then `--reps` calls timed with CUDA events on the launching stream;
+    prints the mean device time per call. Inputs: the bench scene (6000x4000,
+    or 4096x3072 for `nlm`, or --w/--h), demosaiced first where the stage
+    takes RGB.
+      nlm      dsgpu_nlm on the demosaiced frame, 3 channels, 7x7 / 21x21
+      rcd      dsgpu_demosaic (Full: RCD + clip plane) of the normalised CFA
+      develop  dsgpu_develop_u16 (u16 -> RCD -> NLM)
+      denoise  dsgpu_denoise (enhance::denoise), amount 50
+      cnn      dsgpu_cnn_infer, the 8 conv layers
+      learned  dsgpu_develop_u16_cnn with the committed weights, tau 3
+      batch    dsgpu_rcd_nlm_batch of --frames equal frames, the 4 CFA layouts"""
+    import ctypes
+
+    import torch
+
+    import darkslide_b200 as ds
+    from darkslide_b200 import _lib, cnn
+
+    xflags = _lib.DSGPU_FP16_STAGING if args.fp16 else 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    ctx = ds.Context(0)
+    st = torch.cuda.Stream(dev)
+    ctx.set_stream(st.cuda_stream)
+    L = _lib.lib()
+    vp = ctypes.c_void_p
+    w = args.w or (4096 if args.case == "nlm" else W)
+    h = args.h or (3072 if args.case == "nlm" else H)
+    sc = ds.Scene(seed=1, w=w, h=h, pattern=ds.RGGB, black=BLACK, white=WHITE, gain=GAIN, read_sigma=READ_SIGMA)
+    white = np.full(3, WHITE, np.float32)
+    pat = ds.RGGB.codes()
+    hp = 1.5 * sc.sigma_norm()
+    with torch.cuda.stream(st):
+        raw = sc.render(dev, ctx=ctx)
+        rgb = torch.empty((h, w, 3), dtype=torch.float32, device=dev)
+        out = torch.empty((h, w, 3), dtype=torch.float32, device=dev)
+        clip = torch.empty((h, w), dtype=torch.float32, device=dev)
+        cfa = ds.normalize_u16(raw, ds.RGGB, BLACK, white, ctx=ctx).data
+    st.synchronize()
+    net = None
+    if args.case in ("cnn", "learned"):
+        net = cnn.ResidualCNN(ctx)
+        if args.case == "learned":
+            net.load(WEIGHTS)
+    frames = None
+    if args.case == "batch":
+        pats = [ds.RGGB, ds.BGGR, ds.GRBG, ds.GBRG]
+        with torch.cuda.stream(st):
+            frames = [ds.BatchFrame(raw, pats[k % 4], BLACK, white, WB, hp,
+                                    torch.empty((h, w, 3), dtype=torch.float32, device=dev))
+                      for k in range(args.frames)]
+        st.synchronize()
+    if args.case in ("nlm", "denoise", "cnn"):  # these stages take the demosaiced frame
+        ctx.check(L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(WB.ctypes.data),
+                                   _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(0), 0), "dsgpu_demosaic")
+    A = _lib.DSGPU_ASYNC
+
+    def call():
+        c = args.case
+        if c == "batch":
+            with torch.cuda.stream(st):
+                ds.develop_batch(frames, args.search, args.patch, ctx=ctx, sync=False)
+            return
+        if c == "nlm":
+            r = L.dsgpu_nlm(ctx.handle, vp(rgb.data_ptr()), w, h, 3, float(hp), args.search, args.patch,
+                            vp(out.data_ptr()), A | xflags)
+        elif c == "rcd":
+            r = L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(WB.ctypes.data),
+                                 _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(clip.data_ptr()), A)
+        elif c == "cnn":
+            r = L.dsgpu_cnn_infer(ctx.handle, net.handle, vp(rgb.data_ptr()), w, h, 0.5, vp(out.data_ptr()), A)
+        elif c == "learned":
+            r = L.dsgpu_develop_u16_cnn(ctx.handle, net.handle, vp(raw.data_ptr()), w, h, w, vp(pat.ctypes.data),
+                                        float(BLACK), vp(white.ctypes.data), vp(WB.ctypes.data), float(hp),
+                                        args.search, args.patch, float(TAU), vp(out.data_ptr()), vp(0), A)
+        elif c == "denoise":
+            r = L.dsgpu_denoise(ctx.handle, vp(rgb.data_ptr()), w, h, 50.0, vp(out.data_ptr()), A)
+        else:
+            r = L.dsgpu_develop_u16(ctx.handle, vp(raw.data_ptr()), w, h, w, vp(pat.ctypes.data), float(BLACK),
+                                    vp(white.ctypes.data), vp(WB.ctypes.data), float(hp), args.search, args.patch,
+                                    vp(out.data_ptr()), vp(0), A | xflags)
+        ctx.check(r, c)
+
+    call()
+    st.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.reps):
+        call()
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.reps
+    px = w * h * (args.frames if args.case == "batch" else 1)
+    print(json.dumps({"case": args.case, "w": w, "h": h, "ms_per_call": ms, "mpix_per_s": px / ms / 1e3,
+                      "reps": args.reps, "fp16_staging": bool(args.fp16)}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,7 +722,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-frame batched workload")
+    ap.add_argument("--case", choices=CASES, help="time one stage alone (profiler captures); see run_case")
+    ap.add_argument("--w", type=int, default=0, help="--case: frame width")
+    ap.add_argument("--h", type=int, default=0, help="--case: frame height")
+    ap.add_argument("--reps", type=int, default=2, help="--case: timed calls")
+    ap.add_argument("--frames", type=int, default=8, help="--case batch: frames per batch")
+    ap.add_argument("--search", type=int, default=SEARCH, help="--case: NLM search radius")
+    ap.add_argument("--patch", type=int, default=PATCH, help="--case: NLM patch radius")
+    ap.add_argument("--fp16", action="store_true", help="--case nlm/develop: the FP16-staging variant")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

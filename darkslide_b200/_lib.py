@@ -32,6 +32,7 @@ DSGPU_STAGE_NLM = 1
 DSGPU_STAGE_COPY = 2
 DSGPU_STAGE_CNN = 3
 DSGPU_STAGE_CNN_HIDDEN = 4
+DSGPU_NOALLOC_MAX_PIXELS = 1 << 20
 
 # every symbol include/dsgpu.h and include/dsgpu_scene.h declare
 EXPORTS = [
@@ -44,7 +45,7 @@ EXPORTS = [
     "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_cnn_param_count", "dsgpu_cnn_create", "dsgpu_cnn_destroy",
     "dsgpu_cnn_state", "dsgpu_cnn_gradients", "dsgpu_cnn_train_step", "dsgpu_cnn_infer", "dsgpu_cnn_denoise",
     "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_cnn_set_loss", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
-    "dsgpu_measure_mma_sync", "dsgpu_measure_tcgen05_mma",
+    "dsgpu_measure_mma_sync",
     "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render", "dsgpu_scene_render_window",
     "dsgpu_cfa_clip_levels", "dsgpu_reconstruct_highlights", "dsgpu_apply_orientation", "dsgpu_rcd_nlm_batch", "dsgpu_batch_frame_ms", "dsgpu_autotune", "dsgpu_autotune_get", "dsgpu_autotune_set",
 ]
@@ -145,7 +146,6 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_cnn_denoise.argtypes = [vp, vp, vp, i, i, f, i, i, f, vp, ctypes.POINTER(i), u]
             L.dsgpu_develop_u16_cnn.argtypes = [vp, vp, vp, i, i, sz, vp, f, vp, vp, f, i, i, f, vp, vp, u]
             L.dsgpu_measure_mma_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
-            L.dsgpu_measure_tcgen05_mma.argtypes = [vp, i, i, ctypes.POINTER(ctypes.c_double)]
             L.dsgpu_cnn_set_engine.argtypes = [vp, vp, i]
             L.dsgpu_cnn_set_clip.argtypes = [vp, vp, f]
             L.dsgpu_cnn_set_loss.argtypes = [vp, vp, i]
@@ -244,14 +244,6 @@ class Context:
         f = ctypes.c_double()
         self.check(lib().dsgpu_measure_mma_sync(self.handle, ctypes.byref(f)), "dsgpu_measure_mma_sync")
         return f.value
-
-    def measure_tcgen05_mma(self, n: int, commit_every: int = 0) -> float:
-        """SM cycles per 128 x n x 16 BF16 tcgen05 MMA, back to back, with a
-        commit after every `commit_every` MMAs (0: none)."""
-        c = ctypes.c_double()
-        self.check(lib().dsgpu_measure_tcgen05_mma(self.handle, int(n), int(commit_every), ctypes.byref(c)),
-                   "dsgpu_measure_tcgen05_mma")
-        return c.value
 
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and _lib is not None:

@@ -21,7 +21,6 @@ cudaError_t ds_measure_peaks(cudaStream_t st, int device, double* ffma_flops, do
                              double* ffma2_flops);
 
 cudaError_t ds_measure_mma_sync(cudaStream_t st, int device, double* flops);
-cudaError_t ds_measure_tcgen05_mma(cudaStream_t st, int device, int n, int commit_every, double* cycles_per_mma);
 struct DsCnn;
 size_t ds_cnn_param_count();
 cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out);
@@ -503,17 +502,6 @@ int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s) {
   if (!ctx || !bf16_flops_per_s) return DSGPU_ERR_ARG;
   DeviceGuard g(ctx->device);
   DS_TRY(ds_measure_mma_sync(ctx->stream, ctx->device, bf16_flops_per_s));
-  ctx->launches += 2;
-  return DSGPU_OK;
-}
-
-int dsgpu_measure_tcgen05_mma(dsgpu_ctx* ctx, int n, int commit_every, double* cycles_per_mma) {
-  if (!ctx || !cycles_per_mma || (n != 48 && n != 96 && n != 144 && n != 256)) return DSGPU_ERR_ARG;
-  if (commit_every != 0 && commit_every != 1 && commit_every != 2 && commit_every != 6 && commit_every != 12 &&
-      commit_every != 19 && commit_every != 57 && commit_every != 228)
-    return DSGPU_ERR_ARG;
-  DeviceGuard g(ctx->device);
-  DS_TRY(ds_measure_tcgen05_mma(ctx->stream, ctx->device, n, commit_every, cycles_per_mma));
   ctx->launches += 2;
   return DSGPU_OK;
 }

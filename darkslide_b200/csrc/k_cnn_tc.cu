@@ -558,122 +558,3 @@ cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b
   return e;
 }
 
-// ----------------------------------------------------------- MMA issue-rate microbenchmark
-// One thread per SM issues TC_MB_R back-to-back 128 x N x 16 BF16 MMAs from shared
-// memory (no-swizzle K-major operands, A views stepping 16 bytes like the conv's
-// kx-shifted views, the same TMEM accumulator), with a tcgen05.commit to an
-// otherwise unused mbarrier after every `commit_every` MMAs (0: none), then one
-// commit it waits on (bounded). Each CTA reports SM cycles per MMA. This is the
-// measurement behind the conv kernel's tile choices: an MMA costs the same for
-// every N up to 144, and interleaved commits slow the stream.
-namespace {
-constexpr int TC_MB_R = 4096;
-constexpr size_t TC_MB_SMEM = 160 * 1024;  // one CTA per SM; operands live in the first 64 KB
-
-// The trip count is a kernel argument on purpose: the same loop with a
-// compile-time trip count of 4096 measured 115 cycles per MMA instead of 76
-// (the issue rate depends on how the compiler lays out the issuing loop).
-template <int N, int C>
-__global__ void __launch_bounds__(128, 1) mma_issue_kernel(int r, unsigned long long* out) {
-  extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ unsigned tslot;
-  __shared__ __align__(8) unsigned long long done_bar, spare_bar;
-  const int tid = threadIdx.x;
-  for (int i = tid; i < 96 * 1024 / 16; i += 128) reinterpret_cast<uint4*>(sm)[i] = make_uint4(0u, 0u, 0u, 0u);
-  if (tid < 32) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tslot)),
-                 "r"(TC_TMEM_COLS));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  if (tid == 0) {
-    mbar_init(smem_u32(&done_bar), 1);
-    mbar_init(smem_u32(&spare_bar), 1u << 19);  // never completes a phase: commits only count
-    asm volatile("fence.mbarrier_init.release.cluster;");
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const unsigned tmem = tslot;
-  if (tid == 0) {
-    const unsigned abase = smem_u32(sm), bbase = smem_u32(sm + 48 * 1024);
-    const unsigned long long t0 = clock64();
-    for (int i = 0; i < r; i++) {
-      // A: 9 views 272 bytes apart, second K half 13056 bytes on (< 18 KB in all);
-      // B: 3 views 768 bytes apart, second K half 2304 bytes on (< 8 KB from bbase for N <= 256)
-      const unsigned long long a = umma_desc(abase + (unsigned)((i % 9) * 272), 13056, 128);
-      const unsigned long long b = umma_desc(bbase + (unsigned)((i % 3) * 768), 2304, 128);
-      asm volatile(
-          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-          "l"(a), "l"(b), "r"(umma_idesc(TC_M, N)), "r"(i > 0 ? 1 : 0));
-      if (C && i % C == C - 1) mma_commit(smem_u32(&spare_bar));
-    }
-    mma_commit(smem_u32(&done_bar));
-    const unsigned long long g0 = globaltimer_ns();
-    while (!mbar_test(smem_u32(&done_bar), 0) && globaltimer_ns() - g0 < TC_WAIT_NS) {
-    }
-    const bool ok = mbar_test(smem_u32(&done_bar), 0);
-    out[blockIdx.x] = ok ? clock64() - t0 : 0ull;
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (tid < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
-}
-
-template <int N, int C>
-cudaError_t launch_mma_issue(cudaStream_t st, int sms, unsigned long long* out) {
-  cudaError_t e = cudaFuncSetAttribute(mma_issue_kernel<N, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TC_MB_SMEM);
-  if (e != cudaSuccess) return e;
-  mma_issue_kernel<N, C><<<sms, 128, TC_MB_SMEM, st>>>(TC_MB_R, out);
-  return cudaGetLastError();
-}
-
-template <int N>
-cudaError_t launch_mma_issue_c(cudaStream_t st, int c, int sms, unsigned long long* out) {
-  switch (c) {
-    case 0: return launch_mma_issue<N, 0>(st, sms, out);
-    case 1: return launch_mma_issue<N, 1>(st, sms, out);
-    case 2: return launch_mma_issue<N, 2>(st, sms, out);
-    case 6: return launch_mma_issue<N, 6>(st, sms, out);
-    case 12: return launch_mma_issue<N, 12>(st, sms, out);
-    case 19: return launch_mma_issue<N, 19>(st, sms, out);
-    case 57: return launch_mma_issue<N, 57>(st, sms, out);
-    case 228: return launch_mma_issue<N, 228>(st, sms, out);
-    default: return cudaErrorInvalidValue;
-  }
-}
-}  // namespace
-
-// SM cycles per MMA, averaged over all SMs (n in {48, 96, 144, 256}; commit
-// spacing in {0, 1, 2, 6, 12, 19, 57, 228}).
-cudaError_t ds_measure_tcgen05_mma(cudaStream_t st, int device, int n, int commit_every, double* cycles_per_mma) {
-  int sms = 0;
-  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  if (e != cudaSuccess) return e;
-  unsigned long long* d = nullptr;
-  if ((e = cudaMallocAsync(&d, sizeof(unsigned long long) * sms, st)) != cudaSuccess) return e;
-  std::vector<unsigned long long> h(sms);
-  for (int rep = 0; rep < 2 && e == cudaSuccess; rep++) {  // the first launch warms up
-    switch (n) {
-      case 48: e = launch_mma_issue_c<48>(st, commit_every, sms, d); break;
-      case 96: e = launch_mma_issue_c<96>(st, commit_every, sms, d); break;
-      case 144: e = launch_mma_issue_c<144>(st, commit_every, sms, d); break;
-      case 256: e = launch_mma_issue_c<256>(st, commit_every, sms, d); break;
-      default: e = cudaErrorInvalidValue;
-    }
-  }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * sms, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFreeAsync(d, st);
-  if (e != cudaSuccess) return e;
-  double sum = 0.0;
-  for (int i = 0; i < sms; i++) {
-    if (h[i] == 0ull) return cudaErrorLaunchTimeout;  // a CTA's final wait did not complete
-    sum += (double)h[i];
-  }
-  *cycles_per_mma = sum / sms / TC_MB_R;
-  return cudaSuccess;
-}

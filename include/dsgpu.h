@@ -109,12 +109,6 @@ unsigned long long dsgpu_launch_count(dsgpu_ctx* ctx);
 int dsgpu_measure_peaks(dsgpu_ctx* ctx, double* ffma_flops_per_s, double* ex2_per_s, double* ffma2_flops_per_s);
 /* BF16 mma.sync (m16n8k16, FP32 accumulate) throughput microbenchmark. */
 int dsgpu_measure_mma_sync(dsgpu_ctx* ctx, double* bf16_flops_per_s);
-/* tcgen05 MMA issue-rate microbenchmark (instrumentation, no counterpart in
- * the reference): one thread per SM issues 4096 back-to-back 128 x n x 16
- * BF16 MMAs from shared memory (n in 48, 96, 144, 256), with a
- * tcgen05.commit after every `commit_every` of them (0, 1, 2, 6, 12, 19, 57
- * or 228; 0: none); returns the mean SM cycles per MMA. */
-int dsgpu_measure_tcgen05_mma(dsgpu_ctx* ctx, int n, int commit_every, double* cycles_per_mma);
 
 /* Per-site black levels, as load_raw's black_at takes them from the raw's
  * black-level record (decode.rs:266-270): a bw x bh pattern (1..4 each, row
@@ -223,11 +217,17 @@ int dsgpu_develop_u16(dsgpu_ctx* ctx, const uint16_t* raw, int w, int h, size_t 
  *  - All pointers are device memory of the current device; DSGPU_HOST is
  *    rejected (DSGPU_ERR_ARG). Work goes on `cuda_stream` (NULL: the legacy
  *    default stream); the call synchronises it unless DSGPU_ASYNC is given.
+ *  - Flags: DSGPU_ASYNC and DSGPU_FP16_STAGING act as in dsgpu_develop_u16
+ *    (the output is bit-identical to it with the same flags);
+ *    DSGPU_HIGHLIGHTS needs scratch this call does not have
+ *    (DSGPU_ERR_UNSUPPORTED); any other bit is DSGPU_ERR_ARG.
+ *  - There is no context, so no per-site black pattern
+ *    (dsgpu_set_black_pattern) applies: every site uses the scalar `black`.
  *  - Frames above DSGPU_NOALLOC_MAX_PIXELS (w*h) are rejected with
  *    DSGPU_ERR_SIZE.
  *  - The first call on a device looks up the array's device address (once per
- *    device, with that device current); make that first call before any
- *    stream capture.
+ *    device and CUDA context, with that device current); make that first
+ *    call before any stream capture.
  *  - Every call shares the array and it keeps the last call's contents (each
  *    call overwrites what it reads). Calls that overlap on the GPU race on it:
  *    serialise them. */

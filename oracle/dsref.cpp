@@ -38,6 +38,12 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+
+// The seeded synthetic mosaic generator of the library (host half of a
+// header shared with the device renderer), so that the CPU legs of the
+// benchmark and the tests can make their inputs without loading the GPU
+// library. It is input generation, not part of the restated path.
+#include "../darkslide_b200/csrc/scene.h"
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -818,6 +824,29 @@ void dsref_reconstruct_highlights(float* img, const float* clip, int w, int h, c
 
 void dsref_denoise_f32(const float* img, int w, int h, float amount, int nthreads, float* out, float* sigma) {
   denoise(img, w, h, amount, nthreads, out, sigma);
+}
+
+// The seeded synthetic mosaic (the library's scene generator; no counterpart
+// in the reference): the cw x ch window at (x0, y0) of the w x h frame.
+void dsref_scene_render(uint64_t seed, int w, int h, const uint8_t cfa[4], int black, int white, float gain,
+                        float read_sigma, int x0, int y0, int cw, int ch, uint16_t* out) {
+  ds_scene s;
+  ds_scene_init(&s, seed, w, h, cfa, black, white, gain, read_sigma);
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < ch; y++)
+    for (long x = 0; x < cw; x++) out[y * cw + x] = ds_scene_pixel(&s, x0 + (int)x, y0 + (int)y);
+}
+
+// Noise-free scene values (RGB, before white balance) of the same window.
+void dsref_scene_truth(uint64_t seed, int w, int h, const uint8_t cfa[4], int black, int white, float gain,
+                       float read_sigma, int x0, int y0, int cw, int ch, float* out) {
+  ds_scene s;
+  ds_scene_init(&s, seed, w, h, cfa, black, white, gain, read_sigma);
+#pragma omp parallel for schedule(static)
+  for (long y = 0; y < ch; y++)
+    for (long x = 0; x < cw; x++)
+      for (int c = 0; c < 3; c++)
+        out[(y * cw + x) * 3 + c] = ds_mul(ds_scene_value(&s, x0 + (int)x, y0 + (int)y, c), s.ch_gain[c]);
 }
 
 }  // extern "C"

@@ -63,6 +63,9 @@ def lib():
         L.dsref_oklab_to_prophoto.argtypes = [_f32p, i, _f32p]
         L.dsref_guided_filter_f32.argtypes = [_f32p, _f32p, i, i, i, f, _f32p]
         L.dsref_denoise_f32.argtypes = [_f32p, i, i, f, i, _f32p, _f32p]
+        u64 = ctypes.c_uint64
+        L.dsref_scene_render.argtypes = [u64, i, i, _u8p, i, i, f, f, i, i, i, i, _u16p]
+        L.dsref_scene_truth.argtypes = [u64, i, i, _u8p, i, i, f, f, i, i, i, i, _f32p]
         _lib = L
     return _lib
 
@@ -270,3 +273,28 @@ def apply_orientation(img: np.ndarray, o: int) -> np.ndarray:
     src = {2: (w - 1 - x, y), 3: (w - 1 - x, h - 1 - y), 4: (x, h - 1 - y), 5: (y, x), 6: (y, h - 1 - x),
            7: (w - 1 - y, h - 1 - x), 8: (w - 1 - y, x)}.get(o, (x, y))
     return img[src[1], src[0]]
+
+
+def scene_render(seed: int, w: int, h: int, cfa, black: int, white: int, gain: float, read_sigma: float,
+                 x0: int = 0, y0: int = 0, cw: int | None = None, ch: int | None = None) -> np.ndarray:
+    """The seeded synthetic mosaic (the library's scene generator, compiled
+    into this library from the same header): the cw x ch window at (x0, y0)
+    of the w x h frame, u16. Equal to darkslide_b200.Scene(...).render_host."""
+    cw = w - x0 if cw is None else cw
+    ch = h - y0 if ch is None else ch
+    out = np.empty((ch, cw), np.uint16)
+    lib().dsref_scene_render(int(seed), w, h, _pat(cfa), int(black), int(white), float(gain), float(read_sigma),
+                             x0, y0, cw, ch, out)
+    return out
+
+
+def scene_truth(seed: int, w: int, h: int, cfa, black: int, white: int, gain: float, read_sigma: float,
+                x0: int = 0, y0: int = 0, cw: int | None = None, ch: int | None = None) -> np.ndarray:
+    """Noise-free RGB of the same scene window (channel gains applied, no
+    white balance); equal to darkslide_b200.Scene(...).truth_host."""
+    cw = w - x0 if cw is None else cw
+    ch = h - y0 if ch is None else ch
+    out = np.empty((ch, cw, 3), np.float32)
+    lib().dsref_scene_truth(int(seed), w, h, _pat(cfa), int(black), int(white), float(gain), float(read_sigma),
+                            x0, y0, cw, ch, out)
+    return out

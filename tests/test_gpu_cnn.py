@@ -365,21 +365,3 @@ def test_learned_develop_composes_and_rejects(torch_dev):
     assert call(40, 40, codes=np.array([0, 1, 3, 2], np.uint8)) == _lib.DSGPU_ERR_CFA
     assert call(40, 40, rawp=vp(0)) == _lib.DSGPU_ERR_ARG
     assert call(0, 0) == _lib.DSGPU_OK  # empty: nothing to do
-
-
-def test_tcgen05_mma_microbenchmark(torch_dev):
-    """The MMA issue-rate microbenchmark behind the conv kernel's design runs
-    and returns plausible cycle counts (a 128 x 256 x 16 MMA cannot beat the
-    math rate, 128 cycles at 4096 MACs per cycle and SM); bad shapes are
-    rejected."""
-    from darkslide_b200 import _lib
-
-    ctx = ds.Context(0)
-    c144 = ctx.measure_tcgen05_mma(144, 0)
-    c256 = ctx.measure_tcgen05_mma(256, 0)
-    assert 40.0 < c144 < 400.0 and 120.0 < c256 < 600.0, (c144, c256)
-    assert ctx.measure_tcgen05_mma(48, 6) > 0.0
-    L = _lib.lib()
-    out = __import__("ctypes").c_double()
-    for n, c in [(40, 0), (0, 0), (272, 0), (144, 5), (144, -1)]:
-        assert L.dsgpu_measure_tcgen05_mma(ctx.handle, n, c, __import__("ctypes").byref(out)) == _lib.DSGPU_ERR_ARG

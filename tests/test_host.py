@@ -75,6 +75,27 @@ def test_scene_host_render_is_deterministic_and_croppable(L):
     assert not np.array_equal(a, ds.Scene(seed=6, w=96, h=64, black=256, white=4095).render_host())
 
 
+def test_oracle_scene_copy_equals_library_scene(L):
+    """The oracle's copy of the scene generator (what the benchmark's CPU legs
+    render their input with, so that they never load the GPU library) gives
+    the library's mosaic and noise-free scene exactly."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import dsref
+
+    for seed, w, h, pat, black, white, g, s in [(1, 6000, 4000, ds.RGGB, 512, 16383, 0.5, 6.0),
+                                                (9, 301, 203, ds.GRBG, 256, 4095, 0.25, 12.0)]:
+        sc = ds.Scene(seed=seed, w=w, h=h, pattern=pat, black=black, white=white, gain=g, read_sigma=s)
+        x0, y0 = (w - 96) // 2, (h - 64) // 2
+        np.testing.assert_array_equal(
+            sc.render_host(x0, y0, 96, 64),
+            dsref.scene_render(seed, w, h, pat.codes(), black, white, g, s, x0, y0, 96, 64))
+        np.testing.assert_array_equal(
+            sc.truth_host(x0, y0, 40, 30),
+            dsref.scene_truth(seed, w, h, pat.codes(), black, white, g, s, x0, y0, 40, 30))
+
+
 def test_scene_noise_statistics(L):
     """Poisson-Gaussian noise: var(DN) ~ signal/g + sigma_read^2 on flat-ish areas."""
     sc = ds.Scene(seed=1, w=512, h=512, pattern=ds.RGGB, black=512, white=16383, gain=0.5, read_sigma=6)
