@@ -576,15 +576,16 @@ __global__ void hl_apply_kernel(float* __restrict__ img, const float* __restrict
 }
 
 // One RCD tile of a batch frame (local tile index), with the frame's tile shape.
+template <int NT>
 __device__ __noinline__ void rcd_batch_tile(const ds_batch_frame& F, int local, float* smem) {
   const int ty = local / F.rcd_tiles_x, tx = local - ty * F.rcd_tiles_x;
   const SrcU16 src{F.src};
   switch (F.rcd_shape) {
-    case 0: rcd_tile<SrcU16, 32, 32>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-    case 1: rcd_tile<SrcU16, 64, 16>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-    case 2: rcd_tile<SrcU16, 48, 24>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-    case 3: rcd_tile<SrcU16, 24, 48>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-    default: rcd_tile<SrcU16, 16, 64>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    case 0: rcd_tile<SrcU16, 32, 32, NT>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    case 1: rcd_tile<SrcU16, 64, 16, NT>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    case 2: rcd_tile<SrcU16, 48, 24, NT>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    case 3: rcd_tile<SrcU16, 24, 48, NT>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
+    default: rcd_tile<SrcU16, 16, 64, NT>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
   }
 }
 
@@ -605,7 +606,7 @@ __device__ __forceinline__ unsigned long long batch_clock_ns() {
 // stamps[f] = the device clock. The tile bodies are those of the one-frame
 // kernels, so every frame's output equals the one-frame path's bit for bit.
 template <int P>
-__global__ void __launch_bounds__(RCD_THREADS, 2) batch_fused_kernel(const ds_batch_frame* __restrict__ frames,
+__global__ void __launch_bounds__(nlmk::NLM_THREADS, 1) batch_fused_kernel(const ds_batch_frame* __restrict__ frames,
                                                                      int n, const ds_batch_seg* __restrict__ segs,
                                                                      int nseg, int total, int S, int* counters,
                                                                      int max_frames,
@@ -631,7 +632,7 @@ __global__ void __launch_bounds__(RCD_THREADS, 2) batch_fused_kernel(const ds_ba
     const ds_batch_frame& F = frames[sg.frame];
     const int local = t - sg.start;
     if (sg.kind == 0) {
-      rcd_batch_tile(F, local, smem);  // out of line: keeps the NLM body's registers to itself
+      rcd_batch_tile<nlmk::NLM_THREADS>(F, local, smem);  // out of line: keeps the NLM body's registers to itself
       __syncthreads();
       if (tid == 0) {
         __threadfence();  // the tile's output before its count
@@ -677,7 +678,7 @@ cudaError_t launch_batch_fused_p(cudaStream_t st, const ds_batch_frame* frames, 
   const size_t smem = nlm > RCD_BATCH_SMEM ? nlm : RCD_BATCH_SMEM;
   cudaError_t e = cudaFuncSetAttribute(batch_fused_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  batch_fused_kernel<P><<<grid, RCD_THREADS, smem, st>>>(frames, n, segs, nseg, total, S, counters, max_frames,
+  batch_fused_kernel<P><<<grid, nlmk::NLM_THREADS, smem, st>>>(frames, n, segs, nseg, total, S, counters, max_frames,
                                                          stamps);
   return cudaGetLastError();
 }
@@ -912,7 +913,6 @@ cudaError_t ds_launch_batch_fused(cudaStream_t st, const ds_batch_frame* frames,
                                   int max_frames, unsigned long long* stamps) {
   if (n <= 0 || total_items <= 0) return cudaSuccess;
   if (search <= 0 || search > DSGPU_NLM_MAX_SEARCH) return cudaErrorInvalidValue;
-  static_assert(nlmk::NLM_THREADS == RCD_THREADS, "one block size for both tile bodies");
   switch (patch) {
     case 0: return launch_batch_fused_p<0>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);
     case 1: return launch_batch_fused_p<1>(st, frames, n, segs, nseg, total_items, search, grid, counters, max_frames, stamps);

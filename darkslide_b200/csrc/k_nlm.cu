@@ -7,24 +7,28 @@
 // (:58) and accumulates weight*sample and weight (:59-60); the result is
 // a/max(s,1e-12) (:71).
 //
-// B200 design. The kernel is bound by shared-memory bandwidth (one 128-byte
-// wavefront per clock per SM) long before the ex2 unit (16/clock/SM), so the
-// layout minimises shared bytes per (pixel, channel, offset) update:
-//  - one CTA owns a 64-wide tile of one channel, TY = 64 - 2P rows tall, so
-//    that the horizontal box sums it needs cover exactly 64 rows;
+// B200 design. Per (pixel, channel, offset) update the kernel needs one ex2
+// and ~8 FP32 operations; what binds is the shared-memory traffic of the
+// separable box sums (one 128-byte wavefront per clock per SM), so the
+// layout minimises shared bytes per update:
+//  - one CTA (512 threads, one per SM) owns a 64-wide tile of one channel,
+//    TY = 64 - 2P rows tall, so that the horizontal box sums it needs cover
+//    exactly 64 rows; the three channels of a tile are adjacent in launch
+//    order, so the interleaved RGB lines they all read come from L2;
 //  - the tile plus its S+P+1 halo is staged once in shared memory, PRE-SCALED
 //    by sigma = sqrt(log2(e) / (h^2 (2P+1)^2)): the squared differences of
 //    scaled samples sum directly to the ex2 exponent, so a weight costs one
 //    ex2 and no multiply;
-//  - offsets are processed in 2x2 blocks {dx0, dx0+1} x {dy0, dy0+1}:
-//    phase A: thread t owns H row t%64 (a 16-wide segment, its 22 centre
-//      samples kept in registers for the whole kernel) and forms the
-//      horizontal running sums for the block's offsets from one 23-sample
-//      load of each shifted row (so one load serves both dx);
-//    phase B: thread t owns one column and a quarter of the tile's rows,
-//      sums 2P+1 H rows as a running vertical sum, and accumulates; the
-//      shifted sample of row r at dy0+1 is the one of row r+1 at dy0, so one
-//      column load serves both dy;
+//  - offsets are processed in blocks of 4 dx x 2 dy (8 planes of H):
+//    phase A: thread t owns H row t%64, a 16-wide segment and one dy of the
+//      block (its 22 centre samples kept in registers for the whole kernel)
+//      and forms the horizontal running sums of all four dx from ONE
+//      25-sample load of the shifted row;
+//    phase B: thread t owns one column, a quarter of the tile's rows and two
+//      of the four dx, sums 2P+1 H rows as a running vertical sum, and
+//      accumulates; the shifted sample of row r at dy0+1 is the one of row
+//      r+1 at dy0, so one column load serves both dy. The two dx halves of a
+//      pixel's sums meet once, at the end;
 //  - all shared pitches are odd, so a warp's 32 rows (phase A) or 32 columns
 //    (phase B) hit 32 distinct banks.
 // Clamped edges: the staged copy is loaded at clamped coordinates, so the
@@ -42,21 +46,25 @@ namespace {
 
 using namespace nlmk;
 
+// grid: (tiles_x * C, tile rows); block x = tile_x * C + channel, so the C
+// channels of a tile run side by side
 template <int P, bool F16>
-__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
+__global__ void __launch_bounds__(NLM_THREADS, 1) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
                                                                   int S, float sigma, const float* __restrict__ h_dev,
                                                                   float norm2_log2e,
                                                                   const unsigned char* __restrict__ tile_flags,
                                                                   float* __restrict__ out, int ty0) {
   const int ty = blockIdx.y + ty0;  // tile row (a launch may cover a band of tile rows)
+  const int tx = blockIdx.x / C, ch = blockIdx.x - tx * C;
+  const int tiles_x = gridDim.x / C;
   // tile-list mode (the learned path's fallback): only flagged tiles run
-  if (tile_flags && !tile_flags[ty * gridDim.x + blockIdx.x]) return;
+  if (tile_flags && !tile_flags[ty * tiles_x + tx]) return;
   if (h_dev) {  // strength computed on the device (enhance.rs:40 floor included)
     const float hh = *h_dev;
     sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
   }
   extern __shared__ float4 smem4[];
-  nlm_tile<P, F16>(in, W, H, C, S, sigma, out, blockIdx.x, ty, blockIdx.z, reinterpret_cast<float*>(smem4));
+  nlm_tile<P, F16>(in, W, H, C, S, sigma, out, tx, ty, ch, reinterpret_cast<float*>(smem4));
 }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -71,7 +79,7 @@ __global__ void stamp_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
 // last tile of frame f is done, stamps[f] = the device clock (ns), so the
 // host can report per-frame completion times.
 template <int P>
-__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
+__global__ void __launch_bounds__(NLM_THREADS, 1) nlm_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
                                                                    int total, int S, unsigned* __restrict__ done,
                                                                    unsigned long long* __restrict__ stamps) {
   extern __shared__ float4 smem4[];
@@ -121,7 +129,7 @@ cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, 
   cudaError_t e =
       cudaFuncSetAttribute(nlm_tile_kernel<P, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((w + TX - 1) / TX, ty1 - ty0, C);
+  dim3 grid((w + TX - 1) / TX * C, ty1 - ty0);
   nlm_tile_kernel<P, F16><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags, out,
                                                             ty0);
   return cudaGetLastError();

@@ -11,11 +11,15 @@
 namespace {
 namespace nlmk {
 
-constexpr int NLM_THREADS = 256;
-constexpr int TX = 64;   // tile width
-constexpr int HRW = 64;  // H rows per offset (TY + 2P)
-constexpr int SEG = 16;  // phase-A segment width
-constexpr int HP = TX + 1;  // odd H pitch
+constexpr int NLM_THREADS = 512;
+constexpr int TX = 64;      // tile width
+constexpr int HRW = 64;     // H rows per offset (TY + 2P)
+constexpr int SEG = 16;     // phase-A segment width
+constexpr int NI = 4;       // dx per block (one shifted-row load serves all four)
+constexpr int NJ = 2;       // dy per block (one shifted-column load serves both)
+constexpr int NPLANE = NI * NJ;
+constexpr int HP = TX + 1;  // odd H pitch: conflict-free row stores and column loads
+constexpr int HBR = HRW + 4;  // H rows allocated: phase B of the last quarter reads up to row 66
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -24,8 +28,6 @@ __device__ __forceinline__ float ex2(float x) {
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-
-constexpr int HBR = HRW + 4;  // H rows allocated: phase B of the last quarter reads past row 63
 
 // Plane pitch: odd and fixed per P (sized for the largest search radius) so
 // that every shared address offset is a compile-time constant.
@@ -52,7 +54,7 @@ size_t nlm_plane_bytes(int S, int P, bool f16) {
 }
 
 size_t nlm_smem_bytes(int S, int P, bool f16 = false) {
-  return nlm_plane_bytes(S, P, f16) + (size_t)4 * HBR * HP * sizeof(float);
+  return nlm_plane_bytes(S, P, f16) + (size_t)NPLANE * HBR * HP * sizeof(float);
 }
 
 __device__ __forceinline__ float ldp(const float* p) { return *p; }
@@ -61,25 +63,37 @@ __device__ __forceinline__ void stp(float* p, float v) { *p = v; }
 __device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v); }
 
 // One 64 x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
-// image; smem holds nlm_smem_bytes(S, P, F16) bytes.
+// image, by NLM_THREADS threads; smem holds nlm_smem_bytes(S, P, F16) bytes.
+//
+// Offsets are taken in blocks of up to NI dx x NJ dy. Phase A (thread =
+// H row, 16-wide segment and one dy of the block) forms the horizontal box
+// sums of every dx of the block from ONE load of the shifted row; phase B
+// (thread = column, quarter of the tile's rows and one half of the block's
+// dx) sums them vertically, weights and accumulates. A pixel's sums are
+// split between the two dx halves and added once at the end.
+//
 // F16 (the precision variant): the pre-scaled plane is staged in half
 // precision, centred on the tile's centre sample (NLM weights depend only on
 // differences, so the offset costs nothing there and keeps the half-precision
 // error of the staged values small; it is added back to the result), while
 // distances, weights and sums stay in FP32 and the weight sum (the
 // normalisation) is accumulated with Kahan compensation.
-template <int P, bool F16 = false>
-__device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
-                                         float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
+//
+// XIN: every patch window of the tile's columns lies inside the image (no
+// column clamping in phase A). The two cases are separate code so that the
+// border case's per-element clamping does not cost the interior registers.
+template <int P, bool F16, bool XIN>
+__device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
+                                              float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
   using T = typename std::conditional<F16, __half, float>::type;
   constexpr int TY = HRW - 2 * P;
-  constexpr int DW = SEG + 2 * P;  // differences per phase-A segment
-  constexpr int RB = (TY + 3) / 4; // phase-B rows per thread (a quarter of the tile)
+  constexpr int DW = SEG + 2 * P;   // differences per phase-A segment
+  constexpr int RB = (TY + 3) / 4;  // phase-B rows per thread (a quarter of the tile)
   constexpr int PP = nlm_pitch(P);
   const NlmGeom g = nlm_geom(S, P);
   T* PL = reinterpret_cast<T*>(smem);  // scaled plane, pitch PP
   float* HB = reinterpret_cast<float*>(reinterpret_cast<char*>(smem) +
-                                       ((size_t)PP * g.PHA * sizeof(T) + 15) / 16 * 16);  // 4 offsets x HBR rows x HP
+                                       ((size_t)PP * g.PHA * sizeof(T) + 15) / 16 * 16);  // NPLANE x HBR rows x HP
 
   const int X0 = tile_x * TX, Y0 = tile_y * TY;
   const int tid = threadIdx.x;
@@ -95,21 +109,22 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
   }
   for (int i = tid; i < (g.PHA - g.PH) * PP; i += NLM_THREADS) stp(&PL[g.PH * PP + i], 0.f);
 
-  // ---- phase-A role: H row `arow` (tile row arow - P), segment at ax0
+  // ---- phase-A role: H row `arow` (tile row arow - P), segment at ax0, dy index aj
   const int arow = tid & (HRW - 1);
-  const int ax0 = (tid >> 6) * SEG;
+  const int ax0 = ((tid >> 6) & 3) * SEG;
+  const int aj = tid >> 8;
   const int aprow = clampi(Y0 + arow - P, 0, H - 1) - oy0;  // plane row of the clamped H row
-  const bool xin = (X0 - P >= 0) && (X0 + TX + P <= W);
   const int acol0 = ax0 - P + g.R;  // plane column of difference 0 (interior tiles)
-  // ---- phase-B role: column bcol, rows [brow0, brow0 + RB) (clipped to TY)
+  // ---- phase-B role: column bcol, rows [brow0, brow0 + RB) (clipped to TY), dx half bk
   const int bcol = tid & (TX - 1);
-  const int brow0 = (tid >> 6) * RB;
+  const int brow0 = ((tid >> 6) & 3) * RB;
+  const int bk = tid >> 8;
 
   __syncthreads();
   float pv[DW];  // centre samples of this thread's phase-A segment
 #pragma unroll
   for (int k = 0; k < DW; k++) {
-    const int col = xin ? acol0 + k : clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
+    const int col = XIN ? acol0 + k : clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
     pv[k] = ldp(&PL[aprow * PP + col]);
   }
   float a[RB], s[RB], cs[F16 ? RB : 1];  // cs: Kahan compensation of s (F16)
@@ -120,64 +135,63 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
     if (F16) cs[r] = 0.f;
   }
 
-  // One 2x2 block of offsets {dx0, dx0+1} x {dy0, dy0+NJ-1}.
-  auto block = [&](int dx0, int dy0, auto nj_tag) {
-    constexpr int NJ = decltype(nj_tag)::value;
+  // One block of offsets {dx0 .. dx0+BI-1} x {dy0 .. dy0+BJ-1}; plane (i, j)
+  // of the block is HB + (j * NI + i) * HBR * HP.
+  auto block = [&](int dx0, int dy0, auto ni_tag, auto nj_tag) {
+    constexpr int BI = decltype(ni_tag)::value;
+    constexpr int BJ = decltype(nj_tag)::value;
     // phase A: horizontal sums, stored NEGATED (-sum d^2) so that phase B's
     // vertical sum is the ex2 argument itself
+    if (aj < BJ) {
+      const T* qrow = PL + (aprow + dy0 + aj) * PP + dx0;
+      float q[DW + BI - 1];
+      if constexpr (XIN) {
 #pragma unroll
-    for (int j = 0; j < NJ; j++) {
-      const T* qrow = PL + (aprow + dy0 + j) * PP + dx0;
-      float d0[DW], d1[DW];
-      if (xin) {
-        float q[DW + 1];
-#pragma unroll
-        for (int k = 0; k <= DW; k++) q[k] = ldp(&qrow[acol0 + k]);
-#pragma unroll
-        for (int k = 0; k < DW; k++) {
-          d0[k] = pv[k] - q[k];
-          d1[k] = pv[k] - q[k + 1];
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < DW; k++) {
-          const int col = clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
-          d0[k] = pv[k] - ldp(&qrow[col]);
-          d1[k] = pv[k] - ldp(&qrow[col + 1]);
-        }
+        for (int m = 0; m < DW + BI - 1; m++) q[m] = ldp(&qrow[acol0 + m]);
       }
-      float h0 = 0.f, h1 = 0.f;
+      float* Hrow = HB + (size_t)aj * NI * (HBR * HP) + arow * HP + ax0;
 #pragma unroll
-      for (int k = 0; k <= 2 * P; k++) {
-        h0 = fmaf(-d0[k], d0[k], h0);
-        h1 = fmaf(-d1[k], d1[k], h1);
-      }
-      float* H0 = HB + (j * 2 + 0) * (HBR * HP) + arow * HP + ax0;
-      float* H1 = HB + (j * 2 + 1) * (HBR * HP) + arow * HP + ax0;
-      H0[0] = h0;
-      H1[0] = h1;
+      for (int i = 0; i < BI; i++) {
+        // difference k of plane i; computed where it enters the window and
+        // again where it leaves (cheaper than keeping 22 of them live)
+        auto dif = [&](int k) {
+          if constexpr (XIN) {
+            return pv[k] - q[k + i];
+          } else {
+            const int col = clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
+            return pv[k] - ldp(&qrow[col + i]);
+          }
+        };
+        float h = 0.f;
 #pragma unroll
-      for (int k = 1; k < SEG; k++) {
-        h0 = fmaf(-d0[k + 2 * P], d0[k + 2 * P], h0);
-        h0 = fmaf(d0[k - 1], d0[k - 1], h0);
-        h1 = fmaf(-d1[k + 2 * P], d1[k + 2 * P], h1);
-        h1 = fmaf(d1[k - 1], d1[k - 1], h1);
-        H0[k] = h0;
-        H1[k] = h1;
+        for (int k = 0; k <= 2 * P; k++) {
+          const float d = dif(k);
+          h = fmaf(-d, d, h);
+        }
+        float* Hi = Hrow + i * (HBR * HP);
+        Hi[0] = h;
+#pragma unroll
+        for (int k = 1; k < SEG; k++) {
+          const float de = dif(k + 2 * P), dl = dif(k - 1);
+          h = fmaf(-de, de, h);
+          h = fmaf(dl, dl, h);
+          Hi[k] = h;
+        }
       }
     }
     __syncthreads();
-    // phase B: vertical sums, weights, accumulation for (dx0 + i, dy0 + j)
+    // phase B: vertical sums, weights, accumulation for dx0 + i (i = bk, bk + 2)
 #pragma unroll
-    for (int i = 0; i < 2; i++) {
-      if (dx0 + i <= S) {  // false only for the dx tail of an odd search width
+    for (int ii = 0; ii < 2; ii++) {
+      const int i = bk + 2 * ii;
+      if (i < BI) {
         const T* qc = PL + (brow0 + g.R + dy0) * PP + bcol + g.R + dx0 + i;
-        float qv[RB + NJ - 1];
+        float qv[RB + BJ - 1];
 #pragma unroll
-        for (int r = 0; r < RB + NJ - 1; r++) qv[r] = ldp(&qc[r * PP]);
+        for (int r = 0; r < RB + BJ - 1; r++) qv[r] = ldp(&qc[r * PP]);
 #pragma unroll
-        for (int j = 0; j < NJ; j++) {
-          const float* hc = HB + (j * 2 + i) * (HBR * HP) + brow0 * HP + bcol;
+        for (int j = 0; j < BJ; j++) {
+          const float* hc = HB + (j * NI + i) * (HBR * HP) + brow0 * HP + bcol;
           float hv[RB + 2 * P];
 #pragma unroll
           for (int r = 0; r < RB + 2 * P; r++) hv[r] = hc[r * HP];
@@ -204,22 +218,64 @@ __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, in
     __syncthreads();
   };
 
+  // blocks of NI dx x NJ dy, then the dx tail (fewer than NI columns of
+  // offsets) and the dy tail (one row of offsets when 2S+1 is odd)
+  const int n_off = 2 * S + 1;
+  const int dx_main = n_off / NI * NI;  // dx in [-S, -S + dx_main) go in full blocks
+  const int dx_tail = n_off - dx_main;
+  auto row_of_blocks = [&](int dy0, auto nj_tag) {
+    for (int dx0 = -S; dx0 < -S + dx_main; dx0 += NI) block(dx0, dy0, std::integral_constant<int, NI>{}, nj_tag);
+    const int dxt = -S + dx_main;
+    switch (dx_tail) {
+      case 1: block(dxt, dy0, std::integral_constant<int, 1>{}, nj_tag); break;
+      case 2: block(dxt, dy0, std::integral_constant<int, 2>{}, nj_tag); break;
+      case 3: block(dxt, dy0, std::integral_constant<int, 3>{}, nj_tag); break;
+      default: break;
+    }
+  };
   int dy0 = -S;
-  for (; dy0 + 1 <= S; dy0 += 2)
-    for (int dx0 = -S; dx0 <= S; dx0 += 2) block(dx0, dy0, std::integral_constant<int, 2>{});
-  if (dy0 <= S)  // the dy tail of an odd search width
-    for (int dx0 = -S; dx0 <= S; dx0 += 2) block(dx0, dy0, std::integral_constant<int, 1>{});
+  for (; dy0 + NJ - 1 <= S; dy0 += NJ) row_of_blocks(dy0, std::integral_constant<int, NJ>{});
+  if (dy0 <= S) row_of_blocks(dy0, std::integral_constant<int, 1>{});  // the dy tail of an odd search width
 
-  const float inv_sigma = 1.0f / sigma;
+  // the two dx halves of each pixel's sums: half 1 hands its sums over
+  // through shared memory (the H planes are free now), half 0 adds and writes
+  float* XA = HB;
+  float* XS = HB + TX * 4 * RB;
+  float* XC = HB + 2 * TX * 4 * RB;
+  const int slot = ((tid >> 6) & 3) * RB * TX + bcol;  // (quarter, row r) x column
+  if (bk == 1) {
 #pragma unroll
-  for (int r = 0; r < RB; r++) {
-    const int y = brow0 + r;
-    const int gx = X0 + bcol, gy = Y0 + y;
-    if (y < TY && gx < W && gy < H) {
-      const float o = __fdiv_rn(a[r] * inv_sigma, fmaxf(F16 ? s[r] - cs[r] : s[r], 1e-12f));
-      out[((size_t)gy * W + gx) * C + ch] = F16 ? o + off : o;
+    for (int r = 0; r < RB; r++) {
+      XA[slot + r * TX] = a[r];
+      XS[slot + r * TX] = s[r];
+      if (F16) XC[slot + r * TX] = cs[r];
     }
   }
+  __syncthreads();
+  if (bk == 0) {
+    const float inv_sigma = 1.0f / sigma;
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      const int y = brow0 + r;
+      const int gx = X0 + bcol, gy = Y0 + y;
+      if (y < TY && gx < W && gy < H) {
+        const float at = a[r] + XA[slot + r * TX];
+        const float st = F16 ? (s[r] - cs[r]) + (XS[slot + r * TX] - XC[slot + r * TX]) : s[r] + XS[slot + r * TX];
+        const float o = __fdiv_rn(at * inv_sigma, fmaxf(st, 1e-12f));
+        out[((size_t)gy * W + gx) * C + ch] = F16 ? o + off : o;
+      }
+    }
+  }
+}
+
+template <int P, bool F16 = false>
+__device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
+                                         float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
+  const int X0 = tile_x * TX;
+  if (X0 - P >= 0 && X0 + TX + P <= W)
+    nlm_tile_body<P, F16, true>(in, W, H, C, S, sigma, out, tile_x, tile_y, ch, smem);
+  else
+    nlm_tile_body<P, F16, false>(in, W, H, C, S, sigma, out, tile_x, tile_y, ch, smem);
 }
 
 }  // namespace nlmk
