@@ -44,7 +44,8 @@ EXPORTS = [
     "dsgpu_develop_u16", "dsgpu_develop_u16_noalloc", "dsgpu_estimate_noise", "dsgpu_guided_filter",
     "dsgpu_oklab_matrices", "dsgpu_denoise", "dsgpu_cnn_param_count", "dsgpu_cnn_create", "dsgpu_cnn_destroy",
     "dsgpu_cnn_state", "dsgpu_cnn_gradients", "dsgpu_cnn_train_step", "dsgpu_cnn_infer", "dsgpu_cnn_denoise",
-    "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_cnn_set_loss", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
+    "dsgpu_develop_u16_cnn", "dsgpu_cnn_set_engine", "dsgpu_cnn_set_clip", "dsgpu_cnn_set_loss",
+    "dsgpu_cnn_set_judge", "dsgpu_cnn_judge_stats", "dsgpu_cnn_judge_tile", "dsgpu_profile", "dsgpu_stage_ms", "dsgpu_launch_count", "dsgpu_measure_peaks",
     "dsgpu_measure_mma_sync",
     "dsgpu_scene_render_host", "dsgpu_scene_truth_host", "dsgpu_scene_render", "dsgpu_scene_render_window",
     "dsgpu_cfa_clip_levels", "dsgpu_reconstruct_highlights", "dsgpu_apply_orientation", "dsgpu_rcd_nlm_batch", "dsgpu_batch_frame_ms", "dsgpu_autotune", "dsgpu_autotune_get", "dsgpu_autotune_set",
@@ -147,6 +148,10 @@ def lib() -> ctypes.CDLL:
             L.dsgpu_develop_u16_cnn.argtypes = [vp, vp, vp, i, i, sz, vp, f, vp, vp, f, i, i, f, vp, vp, u]
             L.dsgpu_measure_mma_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
             L.dsgpu_cnn_set_engine.argtypes = [vp, vp, i]
+            L.dsgpu_cnn_set_judge.argtypes = [vp, vp, f, f, u]
+            L.dsgpu_cnn_judge_stats.argtypes = [vp, vp, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(f),
+                                                ctypes.POINTER(f)]
+            L.dsgpu_cnn_judge_tile.argtypes = [u, f, i]
             L.dsgpu_cnn_set_clip.argtypes = [vp, vp, f]
             L.dsgpu_cnn_set_loss.argtypes = [vp, vp, i]
             L.dsgpu_profile.argtypes = [vp, i]

@@ -205,6 +205,22 @@ class ResidualCNN:
         img = Image3(w, h, rgb)
         return (img, Plane(w, h, clip)) if with_clip else img
 
+    def set_judge(self, fraction: float, limit: float = 0.5, seed: int = 0) -> None:
+        """Judge mode (dsgpu_cnn_set_judge): plain NLM recomputes a seeded
+        `fraction` of the NLM tiles and a sampled tile keeps NLM's result when
+        the network's RMS error against it exceeds `limit` x sigma. 0: off."""
+        self.ctx.check(lib().dsgpu_cnn_set_judge(self.ctx.handle, self.handle, float(fraction), float(limit),
+                                                 int(seed) & 0xFFFFFFFF), "dsgpu_cnn_set_judge")
+
+    def judge_stats(self) -> dict:
+        """The judge's record of the last call: sampled tiles, tiles that kept
+        NLM, max and RMS error of the network against NLM (over sigma)."""
+        j, f = ctypes.c_int(), ctypes.c_int()
+        mx, rms = ctypes.c_float(), ctypes.c_float()
+        self.ctx.check(lib().dsgpu_cnn_judge_stats(self.ctx.handle, self.handle, ctypes.byref(j), ctypes.byref(f),
+                                                   ctypes.byref(mx), ctypes.byref(rms)), "dsgpu_cnn_judge_stats")
+        return {"judged": j.value, "failed": f.value, "max_rms_over_sigma": mx.value, "rms_over_sigma": rms.value}
+
     def set_clip(self, max_norm: float) -> None:
         """Clip the global gradient norm to max_norm in train_step (0: off)."""
         self.ctx.check(lib().dsgpu_cnn_set_clip(self.ctx.handle, self.handle, float(max_norm)), "dsgpu_cnn_set_clip")

@@ -42,6 +42,13 @@ cudaError_t ds_cnn_denoise(DsCnn* net, cudaStream_t st, const float* rgb, int w,
                            int patch, float tau, float strength_scale, float* out, unsigned char* flags_scratch,
                            unsigned* count_dev);
 cudaError_t ds_cnn_reserve(DsCnn* net, int w, int h);
+void ds_cnn_set_judge(DsCnn* net, float fraction, float limit, unsigned seed);
+bool ds_cnn_judge_on(const DsCnn* net);
+int ds_cnn_judge_tile(unsigned seed, float fraction, int t);
+cudaError_t ds_cnn_reserve_judge(DsCnn* net, int w, int h, int patch);
+cudaError_t ds_cnn_judge_reset(DsCnn* net, cudaStream_t st);
+cudaError_t ds_cnn_judge_stats(DsCnn* net, cudaStream_t st, int* judged, int* failed, float* max_rms,
+                               float* mean_rms);
 int ds_cnn_halo_rows();
 cudaError_t ds_cnn_denoise_band(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, int r0, int r1, int halo,
                                 float h_param, int search, int patch, float tau, float strength_scale, float* out,
@@ -1007,6 +1014,25 @@ int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* c, int tensor_core_gen5) {
   return DSGPU_OK;
 }
 
+int dsgpu_cnn_set_judge(dsgpu_ctx* ctx, dsgpu_cnn* c, float fraction, float limit, unsigned seed) {
+  if (!ctx || !c || !(fraction >= 0.f && fraction <= 1.f) || !(limit >= 0.f)) return DSGPU_ERR_ARG;
+  ds_cnn_set_judge(c->net, fraction, limit, seed);
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_judge_stats(dsgpu_ctx* ctx, dsgpu_cnn* c, int* judged, int* failed, float* max_rms_over_sigma,
+                          float* rms_over_sigma) {
+  if (!ctx || !c || !judged || !failed || !max_rms_over_sigma || !rms_over_sigma) return DSGPU_ERR_ARG;
+  DeviceGuard g(ctx->device);
+  DS_TRY(ds_cnn_judge_stats(c->net, ctx->stream, judged, failed, max_rms_over_sigma, rms_over_sigma));
+  return DSGPU_OK;
+}
+
+int dsgpu_cnn_judge_tile(unsigned seed, float fraction, int tile_index) {
+  if (tile_index < 0 || !(fraction >= 0.f && fraction <= 1.f)) return DSGPU_ERR_ARG;
+  return ds_cnn_judge_tile(seed, fraction, tile_index);
+}
+
 // Scratch for the fallback: the tile flags (one byte per NLM tile) + u32 count
 static int fallback_scratch(dsgpu_ctx* ctx, int w, int h, int patch, unsigned char** flags, unsigned** count) {
   int tx, ty, tw, th;
@@ -1042,7 +1068,7 @@ int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* in_rgb, int w, 
                           DSGPU_CNN_STRENGTH_SCALE, (float*)dout, fl, cnt));
     hidden.done = true;
   }
-  ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0);
+  ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0) + (ds_cnn_judge_on(c->net) ? 3 : 0);
   if (!(flags & DSGPU_ASYNC)) DS_CHECK(ds_cnn_take_status(c->net, ctx->stream));
   if (fallback_tiles) {
     unsigned hc = 0;
@@ -1101,6 +1127,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
   if (out_clip) DS_CHECK(scratch(ctx, S_OUT2, n * sizeof(float), &dclip));
   DS_CHECK(fallback_scratch(ctx, w, h, patch, &fl, &cnt));
   DS_TRY(ds_cnn_reserve(net, w, max_rows));
+  DS_TRY(ds_cnn_reserve_judge(net, w, h, patch));
   if (!ctx->copy) DS_TRY(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
   PipelineDrain drain_guard(ctx);
   while (ctx->band_ev.size() < CHUNKS + BANDS + 1) {
@@ -1117,6 +1144,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
     ca = nullptr;
   }
   DS_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned), ctx->stream));
+  if (ds_cnn_judge_on(net)) DS_TRY(ds_cnn_judge_reset(net, ctx->stream));
   // the copy stream starts after whatever the context stream already holds
   DS_TRY(cudaEventRecord(start_ev, ctx->stream));
   DS_TRY(cudaStreamWaitEvent(ctx->copy, start_ev, 0));
@@ -1152,7 +1180,7 @@ static int develop_cnn_pipelined(dsgpu_ctx* ctx, DsCnn* net, const uint16_t* raw
     }
     DS_TRY(ds_cnn_denoise_band(net, ctx->stream, (const float*)mid, w, h, r0, r1, halo, h_param, search, patch, tau,
                                DSGPU_CNN_STRENGTH_SCALE, (float*)drgb, (float*)band, fl, cnt));
-    ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0);
+    ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0) + (ds_cnn_judge_on(net) ? 3 : 0);
     DS_TRY(cudaEventRecord(band_ev[b], ctx->stream));
     DS_TRY(cudaStreamWaitEvent(ctx->copy, band_ev[b], 0));
     DS_TRY(cudaMemcpyAsync(out_rgb + (size_t)r0 * row, static_cast<float*>(drgb) + (size_t)r0 * row,
@@ -1206,7 +1234,7 @@ int dsgpu_develop_u16_cnn(dsgpu_ctx* ctx, dsgpu_cnn* c, const uint16_t* raw, int
     DS_TRY(ds_cnn_denoise(c->net, ctx->stream, (const float*)mid, w, h, h_param, search, patch, tau,
                           DSGPU_CNN_STRENGTH_SCALE, (float*)drgb, fl, cnt));
     hidden.done = true;
-    ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0);
+    ctx->launches += 1 + 8 + (tau > 0.f ? 2 : 0) + (ds_cnn_judge_on(c->net) ? 3 : 0);
   }
   DS_CHECK(finish(ctx, flags, out_rgb, drgb, n * 3 * sizeof(float), out_clip, dclip, n * sizeof(float)));
   return (flags & DSGPU_ASYNC) ? DSGPU_OK : ds_cnn_take_status(c->net, ctx->stream);

@@ -18,6 +18,7 @@
 //                 fixed order (deterministic)
 #include <cuda_bf16.h>
 
+#include <cstring>
 #include <vector>
 
 #include "internal.cuh"
@@ -493,6 +494,96 @@ __global__ void residual_check_kernel(const float* __restrict__ in, const float*
   (void)n;
 }
 
+// Judge mode (plain NLM as the judge of the network's error). Tile t of the
+// NLM tile grid is judged when a 32-bit mix of (seed, t) is below
+// fraction * 2^32, so the sample depends only on the seed and the tile grid
+// (the same tiles whether the frame runs whole or in bands).
+__host__ __device__ __forceinline__ unsigned judge_mix(unsigned seed, unsigned t) {
+  unsigned x = seed * 0x9E3779B9u ^ (t + 0x7F4A7C15u);
+  x ^= x >> 16;
+  x *= 0x85EBCA6Bu;
+  x ^= x >> 13;
+  x *= 0xC2B2AE35u;
+  x ^= x >> 16;
+  return x;
+}
+
+// One CTA per tile of tile rows [ty0, ty0 + gridDim.y): marks the judged
+// tiles and saves the network's output there (NLM overwrites it next).
+__global__ void judge_save_kernel(const float* __restrict__ out, int w, int h, int tile_w, int tile_h,
+                                  unsigned seed, unsigned long long thr, float* __restrict__ save,
+                                  unsigned char* __restrict__ jflags, unsigned* __restrict__ stats, int ty0) {
+  const int ty = blockIdx.y + ty0;
+  const int t = ty * gridDim.x + blockIdx.x;
+  const bool sel = (unsigned long long)judge_mix(seed, (unsigned)t) < thr;
+  if (threadIdx.x == 0) {
+    jflags[t] = sel ? 1 : 0;
+    if (sel) atomicAdd(&stats[0], 1u);
+  }
+  if (!sel) return;
+  const int x0 = blockIdx.x * tile_w, y0 = ty * tile_h;
+  const int tw = min(tile_w, w - x0), th = min(tile_h, h - y0);
+  for (int i = threadIdx.x; i < tw * th * 3; i += blockDim.x) {
+    const int y = y0 + i / (tw * 3), r = i - (y - y0) * tw * 3;
+    const size_t p = ((size_t)y * w + x0) * 3 + r;
+    save[p] = out[p];
+  }
+}
+
+// After NLM has rewritten the judged tiles: per judged tile, the RMS of the
+// network's output against NLM's, over sigma. The tile keeps NLM's result
+// when that exceeds the limit, when the network's output is not finite, or
+// when the residual check already failed it; otherwise the network's output
+// goes back. Judged tiles are settled here, so their residual flag is
+// cleared (the fallback pass skips them).
+__global__ void judge_decide_kernel(const float* __restrict__ save, float* __restrict__ out, int w, int h,
+                                    int tile_w, int tile_h, const unsigned char* __restrict__ jflags,
+                                    unsigned char* __restrict__ rflags, float inv_sigma2, float limit2,
+                                    unsigned* __restrict__ stats, int ty0) {
+  __shared__ float red[CNN_THREADS];
+  __shared__ int bad, keep_nlm;
+  const int ty = blockIdx.y + ty0;
+  const int t = ty * gridDim.x + blockIdx.x;
+  if (!jflags[t]) return;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  const int x0 = blockIdx.x * tile_w, y0 = ty * tile_h;
+  const int tw = min(tile_w, w - x0), th = min(tile_h, h - y0);
+  float acc = 0.f;
+  for (int i = threadIdx.x; i < tw * th * 3; i += CNN_THREADS) {
+    const int y = y0 + i / (tw * 3), r = i - (y - y0) * tw * 3;
+    const size_t p = ((size_t)y * w + x0) * 3 + r;
+    const float a = save[p];
+    if (!isfinite(a)) bad = 1;
+    const float d = a - out[p];
+    acc += d * d;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int k = CNN_THREADS / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const float e2 = red[0] / (float)(3 * tw * th) * inv_sigma2;  // (rms / sigma)^2
+    const int fail = bad || rflags[t] || !(e2 <= limit2);
+    keep_nlm = fail;
+    rflags[t] = 0;
+    if (fail) atomicAdd(&stats[1], 1u);
+    if (isfinite(e2)) {
+      atomicMax(&stats[2], __float_as_uint(e2));  // non-negative floats order as their bits
+      atomicAdd(reinterpret_cast<float*>(&stats[3]), e2);
+    }
+  }
+  __syncthreads();
+  if (keep_nlm) return;
+  for (int i = threadIdx.x; i < tw * th * 3; i += CNN_THREADS) {
+    const int y = y0 + i / (tw * 3), r = i - (y - y0) * tw * 3;
+    const size_t p = ((size_t)y * w + x0) * 3 + r;
+    out[p] = save[p];
+  }
+}
+
 // ------------------------------------------------------------------ host side
 
 template <int CIN, int COUT, int EPI, int D>
@@ -601,6 +692,15 @@ struct DsCnn {
   // inference buffers (grown on demand)
   bf16 *ia = nullptr, *ib = nullptr;
   size_t infer_px = 0;
+  // judge mode: plain NLM recomputes a seeded sample of the NLM tiles and
+  // judges the network's output there (fraction 0: off)
+  float judge_frac = 0.f, judge_limit = 0.f;
+  unsigned judge_seed = 0;
+  float* judge_save = nullptr;            // the network's output on the judged tiles (frame layout)
+  size_t judge_px = 0;
+  unsigned char* judge_flags = nullptr;   // one byte per NLM tile: judged
+  size_t judge_tiles = 0;
+  unsigned* judge_stats = nullptr;        // judged, failed, max (rms/sigma)^2 bits, sum (rms/sigma)^2 bits
   std::vector<void*> allocs;
 
   void* alloc(size_t bytes, cudaError_t& e) {
@@ -611,6 +711,8 @@ struct DsCnn {
   }
   ~DsCnn() {
     for (void* p : allocs) cudaFree(p);
+    if (judge_save) cudaFree(judge_save);
+    if (judge_flags) cudaFree(judge_flags);
   }
 };
 
@@ -668,6 +770,8 @@ cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out) {
   }
   if (e == cudaSuccess) net->err = (int*)net->alloc(sizeof(int), e);
   if (e == cudaSuccess) net->gsq = (float*)net->alloc(sizeof(float), e);
+  if (e == cudaSuccess) net->judge_stats = (unsigned*)net->alloc(4 * sizeof(unsigned), e);
+  if (e == cudaSuccess) e = cudaMemset(net->judge_stats, 0, 4 * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(net->err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(net->m, 0, pb);
   if (e == cudaSuccess) e = cudaMemset(net->v, 0, pb);
@@ -874,31 +978,133 @@ int ds_cnn_take_status(DsCnn* net, cudaStream_t st) {
   return h;
 }
 
+// ---- judge mode, host side
+void ds_cnn_set_judge(DsCnn* net, float fraction, float limit, unsigned seed) {
+  net->judge_frac = fraction > 0.f ? (fraction < 1.f ? fraction : 1.f) : 0.f;
+  net->judge_limit = limit;
+  net->judge_seed = seed;
+}
+
+bool ds_cnn_judge_on(const DsCnn* net) { return net->judge_frac > 0.f; }
+
+// whether tile t is judged under (seed, fraction)
+int ds_cnn_judge_tile(unsigned seed, float fraction, int t) {
+  const unsigned long long thr = (unsigned long long)((double)fraction * 4294967296.0);
+  return (unsigned long long)judge_mix(seed, (unsigned)t) < thr ? 1 : 0;
+}
+
+// Grows the judge buffers to a w x h frame (cudaFree synchronises the
+// device, so a band pipeline reserves before its first launch).
+cudaError_t ds_cnn_reserve_judge(DsCnn* net, int w, int h, int patch) {
+  if (!ds_cnn_judge_on(net)) return cudaSuccess;
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  const size_t px = (size_t)w * h, tiles = (size_t)tx * ty;
+  cudaError_t e = cudaSuccess;
+  if (net->judge_px < px) {
+    if (net->judge_save) cudaFree(net->judge_save);
+    net->judge_save = nullptr;
+    net->judge_px = 0;
+    if ((e = cudaMalloc(&net->judge_save, px * 3 * sizeof(float))) != cudaSuccess) return e;
+    net->judge_px = px;
+  }
+  if (net->judge_tiles < tiles) {
+    if (net->judge_flags) cudaFree(net->judge_flags);
+    net->judge_flags = nullptr;
+    net->judge_tiles = 0;
+    if ((e = cudaMalloc(&net->judge_flags, tiles)) != cudaSuccess) return e;
+    net->judge_tiles = tiles;
+  }
+  return e;
+}
+
+cudaError_t ds_cnn_judge_reset(DsCnn* net, cudaStream_t st) {
+  return cudaMemsetAsync(net->judge_stats, 0, 4 * sizeof(unsigned), st);
+}
+
+// judged tiles, failed tiles, max and RMS over the judged tiles of (rms / sigma), of the last call
+cudaError_t ds_cnn_judge_stats(DsCnn* net, cudaStream_t st, int* judged, int* failed, float* max_rms,
+                               float* mean_rms) {
+  unsigned hs[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(hs, net->judge_stats, sizeof(hs), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  float mx, sum;
+  memcpy(&mx, &hs[2], 4);
+  memcpy(&sum, &hs[3], 4);
+  *judged = (int)hs[0];
+  *failed = (int)hs[1];
+  *max_rms = sqrtf(mx);
+  *mean_rms = hs[0] ? sqrtf(sum / (float)hs[0]) : 0.f;
+  return cudaSuccess;
+}
+
+namespace {
+// Residual check, judge and fallback on the NLM tile rows [t0, t1), the
+// network's output already in `out`.
+cudaError_t check_judge_fallback(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float h_param,
+                                 int search, int patch, float tau, float* out, unsigned char* rflags,
+                                 unsigned* count_dev, int t0, int t1) {
+  const bool judge = ds_cnn_judge_on(net);
+  if (tau <= 0.f && !judge) return cudaSuccess;  // no fallback
+  int tx, ty, tw, th;
+  ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
+  const float sigma = h_param / 1.5f;
+  cudaError_t e;
+  if (tau > 0.f) {
+    residual_check_kernel<<<dim3(tx, t1 - t0), CNN_THREADS, 0, st>>>(rgb, out, w, h, tw, th,
+                                                                     tau * tau * sigma * sigma, rflags, count_dev, t0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  } else if ((e = cudaMemsetAsync(rflags + (size_t)t0 * tx, 0, (size_t)(t1 - t0) * tx, st)) != cudaSuccess) {
+    return e;
+  }
+  if (judge) {
+    if (net->judge_px < (size_t)w * h || net->judge_tiles < (size_t)tx * ty) return cudaErrorInvalidValue;
+    const unsigned long long thr = (unsigned long long)((double)net->judge_frac * 4294967296.0);
+    judge_save_kernel<<<dim3(tx, t1 - t0), CNN_THREADS, 0, st>>>(out, w, h, tw, th, net->judge_seed, thr,
+                                                                 net->judge_save, net->judge_flags, net->judge_stats,
+                                                                 t0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = ds_launch_nlm_tiles_rows(st, rgb, w, h, 3, h_param, search, patch, net->judge_flags, t0, t1, out)) !=
+        cudaSuccess)
+      return e;
+    const float s2 = sigma * sigma > 1e-30f ? sigma * sigma : 1e-30f;
+    judge_decide_kernel<<<dim3(tx, t1 - t0), CNN_THREADS, 0, st>>>(net->judge_save, out, w, h, tw, th,
+                                                                   net->judge_flags, rflags, 1.0f / s2,
+                                                                   net->judge_limit * net->judge_limit,
+                                                                   net->judge_stats, t0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (tau <= 0.f) return cudaSuccess;
+  return ds_launch_nlm_tiles_rows(st, rgb, w, h, 3, h_param, search, patch, rflags, t0, t1, out);
+}
+}  // namespace
+
 // The learned stand-in with its fallback: CNN, residual check per NLM tile,
+// (judge mode) NLM on a seeded sample of tiles judging the network there,
 // NLM on the flagged tiles (written over the CNN output). flags_scratch holds
-// the tile flags followed by a u32 count; *fallback_count_dev receives it.
+// the tile flags followed by a u32 count; *count_dev receives it.
 cudaError_t ds_cnn_denoise(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, float h_param, int search,
                            int patch, float tau, float strength_scale, float* out, unsigned char* flags_scratch,
                            unsigned* count_dev) {
-  cudaError_t e = ds_cnn_infer(net, st, rgb, w, h, h_param * strength_scale, out);
+  cudaError_t e = ds_cnn_reserve_judge(net, w, h, patch);
   if (e != cudaSuccess) return e;
-  if (tau <= 0.f) return cudaSuccess;  // no fallback
+  if ((e = ds_cnn_infer(net, st, rgb, w, h, h_param * strength_scale, out)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(count_dev, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
+  if (ds_cnn_judge_on(net) && (e = ds_cnn_judge_reset(net, st)) != cudaSuccess) return e;
   int tx, ty, tw, th;
   ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
-  if ((e = cudaMemsetAsync(count_dev, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
-  const float sigma = h_param / 1.5f;
-  residual_check_kernel<<<dim3(tx, ty), CNN_THREADS, 0, st>>>(rgb, out, w, h, tw, th, tau * tau * sigma * sigma,
-                                                              flags_scratch, count_dev, 0);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  return ds_launch_nlm_tiles(st, rgb, w, h, 3, h_param, search, patch, flags_scratch, out);
+  return check_judge_fallback(net, st, rgb, w, h, h_param, search, patch, tau, out, flags_scratch, count_dev, 0, ty);
 }
 
 // The same for output rows [r0, r1) only, r0 a multiple of the NLM tile
 // height: the network runs on rows [r0 - halo, r1 + halo) (clipped to the
 // frame) into band_out, whose rows [r0, r1) are exact when halo covers the
 // receptive field (35 rows, plus 1 for the input's local mean); they are
-// copied into out, then the residual check and the NLM fallback run on the
-// NLM tile rows of the band. count_dev must be zeroed before the first band.
+// copied into out, then the residual check, the judge and the NLM fallback
+// run on the NLM tile rows of the band. count_dev (and, in judge mode, the
+// judge statistics: ds_cnn_judge_reset) must be zeroed before the first band,
+// and the judge buffers reserved for the whole frame (ds_cnn_reserve_judge).
 cudaError_t ds_cnn_denoise_band(DsCnn* net, cudaStream_t st, const float* rgb, int w, int h, int r0, int r1, int halo,
                                 float h_param, int search, int patch, float tau, float strength_scale, float* out,
                                 float* band_out, unsigned char* flags_scratch, unsigned* count_dev) {
@@ -909,14 +1115,8 @@ cudaError_t ds_cnn_denoise_band(DsCnn* net, cudaStream_t st, const float* rgb, i
   if ((e = cudaMemcpyAsync(out + (size_t)r0 * row, band_out + (size_t)(r0 - a0) * row,
                            (size_t)(r1 - r0) * row * sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
-  if (tau <= 0.f) return cudaSuccess;
   int tx, ty, tw, th;
   ds_nlm_tile_grid(w, h, patch, &tx, &ty, &tw, &th);
   const int t0 = r0 / th, t1 = (r1 + th - 1) / th;
-  const float sigma = h_param / 1.5f;
-  residual_check_kernel<<<dim3(tx, t1 - t0), CNN_THREADS, 0, st>>>(rgb, out, w, h, tw, th,
-                                                                   tau * tau * sigma * sigma, flags_scratch,
-                                                                   count_dev, t0);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  return ds_launch_nlm_tiles_rows(st, rgb, w, h, 3, h_param, search, patch, flags_scratch, t0, t1, out);
+  return check_judge_fallback(net, st, rgb, w, h, h_param, search, patch, tau, out, flags_scratch, count_dev, t0, t1);
 }

@@ -349,6 +349,26 @@ int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* net, int tensor_core_gen5);
  * *fallback_tiles (may be NULL) receives the number of tiles recomputed. */
 int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, int h, float h_param,
                       int search, int patch, float tau, float* out_rgb, int* fallback_tiles, unsigned flags);
+/* Judge mode of the learned path (plain GPU NLM as the judge of the
+ * network's error; no counterpart in the reference): plain NLM recomputes a
+ * seeded sample of the NLM tiles, and on each sampled tile the network's
+ * output is compared with it. A sampled tile keeps the NLM result when the
+ * RMS of (network - NLM) over the tile exceeds limit * sigma (sigma = h / 1.5,
+ * the noise level the strength implies), when the network's output is not
+ * finite, or when the residual check failed it; otherwise it keeps the
+ * network's output. Tile t (row-major in the NLM tile grid) is sampled when
+ * dsgpu_cnn_judge_tile(seed, fraction, t) is 1, so the sample is the same
+ * for device-buffer and band-pipelined (DSGPU_HOST) calls. fraction in
+ * [0, 1]; 0 (the default) turns the judge off. Applies to dsgpu_cnn_denoise
+ * and dsgpu_develop_u16_cnn; its cost is NLM on `fraction` of the tiles. */
+int dsgpu_cnn_set_judge(dsgpu_ctx* ctx, dsgpu_cnn* net, float fraction, float limit, unsigned seed);
+/* The judge's record of the last call: tiles sampled, tiles that kept NLM,
+ * and the largest and the root-mean-square (over the sampled tiles) of the
+ * network's per-tile RMS error against NLM, in units of sigma. */
+int dsgpu_cnn_judge_stats(dsgpu_ctx* ctx, dsgpu_cnn* net, int* judged, int* failed, float* max_rms_over_sigma,
+                          float* rms_over_sigma);
+/* 1 when tile `tile_index` is in the judge's sample for (seed, fraction), else 0. */
+int dsgpu_cnn_judge_tile(unsigned seed, float fraction, int tile_index);
 /* u16 raw -> normalise -> RCD -> learned denoise with NLM fallback (the
  * learned counterpart of dsgpu_develop_u16; w or h < 16 gives
  * DSGPU_ERR_UNSUPPORTED, search < 1 DSGPU_ERR_ARG). With DSGPU_HOST the call

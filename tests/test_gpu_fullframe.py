@@ -1,0 +1,66 @@
+"""Whole-frame parity at camera size.
+
+The plain path's camera-size workload: a 6000x4000 RGGB 14-bit mosaic (black
+512, white 16383) of the seeded scene at the three noise levels (read noise
+DN, conversion gain e/DN) = (2, 0.25), (6, 0.5), (12, 1.0); NLM 7x7 patch,
+21x21 search, h = 1.5 x the noise sigma at mid grey. Every pixel of
+dsgpu_develop_u16's output is compared with the f32 oracle run on the same
+raw: normalise + RCD + clip plane must match bit for bit, NLM within
+NLM_TOL_FULL. The oracle costs tens of seconds of host time per frame.
+"""
+import numpy as np
+import pytest
+
+import darkslide_b200 as ds
+
+pytestmark = pytest.mark.gpu
+
+W, H = 6000, 4000
+BLACK, WHITE = 512, 16383
+S, P = 10, 3
+WB = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
+LEVELS = [(2.0, 0.25), (6.0, 0.5), (12.0, 1.0)]
+# the NLM bound against the f32 oracle over the whole frame (the reference's
+# own bound is 1e-3)
+NLM_TOL_FULL = 2e-4
+
+
+@pytest.fixture(scope="module")
+def dev():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from darkslide_b200 import build
+
+    build.build()
+    return torch.device("cuda", 0)
+
+
+@pytest.mark.parametrize("level", LEVELS, ids=lambda v: f"read{v[0]:g}_g{v[1]:g}")
+def test_whole_24mp_frame_against_oracle(dev, oracle, level):
+    import torch
+
+    read, gain = level
+    sc = ds.Scene(seed=24, w=W, h=H, pattern=ds.RGGB, black=BLACK, white=WHITE, gain=gain, read_sigma=read)
+    raw_t = sc.render(dev)
+    white = np.full(3, WHITE, np.float32)
+    hp = 1.5 * sc.sigma_norm()
+    out, clip = ds.develop_u16(raw_t, ds.RGGB, BLACK, white, WB, hp, S, P, with_clip=True)
+    torch.cuda.synchronize()
+    got = out.data.cpu().numpy()
+    got_clip = clip.data.cpu().numpy()
+    dem = ds.develop_u16(raw_t, ds.RGGB, BLACK, white, WB, hp, 0, P).data.cpu().numpy()  # search 0: the demosaic
+    raw = raw_t.cpu().numpy()
+
+    cfa = oracle.normalize_u16(raw, ds.RGGB.codes(), BLACK, white)
+    rgb = oracle.rcd(cfa, ds.RGGB.codes(), WB)
+    np.testing.assert_array_equal(got_clip, oracle.clip_plane(cfa))
+    np.testing.assert_array_equal(dem, rgb)
+    exp = oracle.nlm_rgb(rgb, hp, S, P)
+    err = np.abs(got.astype(np.float64) - exp)
+    mse = float(np.mean(err * err))
+    print(f"\n24MP RGGB read {read:g} DN gain {gain:g}: NLM max-abs {err.max():.3e}, "
+          f"mean-abs {err.mean():.3e}, PSNR vs f32 oracle {10 * np.log10(1 / max(mse, 1e-30)):.1f} dB")
+    assert np.isfinite(got).all()
+    assert err.max() <= NLM_TOL_FULL, err.max()

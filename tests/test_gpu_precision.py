@@ -6,11 +6,9 @@ mid grey.
 
 The GPU develops the whole frame; the oracle recomputes a central 512x512
 crop in FP64 from the raw with a margin wider than the RCD + NLM receptive
-field (10 + S + P), and the interior is compared. With DSGPU_PRECISION_FULL=1
-the oracle develops the whole frame in FP64 as well (minutes of host time).
-Max-abs and PSNR (peak 1) are printed (pytest -s) and bounded here."""
-import os
-
+field (10 + S + P), and the interior is compared; then the oracle develops
+the whole frame in FP64 and every pixel is compared. Max-abs and PSNR
+(peak 1) are printed (pytest -s) and bounded here."""
 import numpy as np
 import pytest
 
@@ -68,7 +66,6 @@ def test_crop_512_against_fp64(frame, oracle):
     assert e32[0] <= 1e-3 and e16[0] <= 3e-3, (e32, e16)
 
 
-@pytest.mark.skipif(os.environ.get("DSGPU_PRECISION_FULL") != "1", reason="full-frame FP64 oracle: minutes")
 def test_full_frame_against_fp64(frame, oracle):
     sc, raw, hp, out32, out16 = frame
     ref = oracle64(oracle, raw, hp, ds.BGGR)
