@@ -53,6 +53,8 @@ WEIGHTS = os.path.join(ROOT, "darkslide_b200", "weights", "cnn_nlm.bin")
 TAU = 3.0                  # residual check of the learned path: NLM on tiles removing > TAU x sigma
 QUALITY_CROP = 2048        # central crop for PSNR against the noise-free scene
 QUALITY_BOUND_DB = 0.1     # allowed PSNR loss of the learned path against plain NLM
+JUDGE_FRACTION = 1.0 / 16  # judge mode: share of the NLM tiles plain NLM recomputes to judge the network
+JUDGE_LIMIT = 0.5          # judge mode: a judged tile keeps NLM when the network's RMS error exceeds this x sigma
 
 
 def workload_config(n_gpus: int) -> dict:
@@ -187,6 +189,39 @@ def cpu_sample_text() -> str:
     return (f"central {cw}x{ch} crop ({cw * ch / 1e6:.2f} MP) of the 6000x4000 bench frame, same seed and noise, "
             "through the oracle (C++ restatement of the reference CPU path, OpenMP over all host threads; the "
             "Rust reference cannot be built here): normalise + RCD + clip plane + NLM x3")
+
+
+FP64_CROP = 256  # central crop on which the FP64 oracle checks the quality claim
+
+
+def cpu_fp64_quality(q_plain, q_learned, qx: int, qy: int) -> dict:
+    """The CPU leg's check of the quality claim: the FP64 oracle (RCD + NLM in
+    double precision, oracle/dsref.cpp) on the central FP64_CROP x FP64_CROP
+    crop of the bench frame (64 px of margin on every side), and the PSNR
+    against the noise-free scene of it, of plain GPU NLM and of the learned
+    path (q_plain / q_learned: the GPU outputs on the QUALITY_CROP crop at
+    (qx, qy))."""
+    dsref = _oracle()
+    c, m = FP64_CROP, 64
+    x0, y0 = (W - c) // 2 & ~1, (H - c) // 2 & ~1
+    rggb = np.array([0, 1, 1, 2], np.uint8)
+    raw = dsref.scene_render(1, W, H, rggb, BLACK, WHITE, GAIN, READ_SIGMA, x0 - m, y0 - m, c + 2 * m, c + 2 * m)
+    t0 = time.perf_counter()
+    cfa = dsref.normalize_u16(raw, rggb, BLACK, np.full(3, WHITE, np.float32))
+    ref = dsref.nlm_rgb(dsref.rcd(cfa, rggb, WB, fp64=True), h_param(), SEARCH, PATCH, fp64=True)[m:m + c, m:m + c]
+    secs = time.perf_counter() - t0
+    truth = dsref.scene_truth(1, W, H, rggb, BLACK, WHITE, GAIN, READ_SIGMA, x0, y0, c, c).astype(np.float64) * WB
+    sx, sy = x0 - qx, y0 - qy
+
+    def db(a):
+        return 10.0 * float(np.log10(1.0 / float(np.mean((np.asarray(a, np.float64) - truth) ** 2))))
+
+    gp = q_plain[sy:sy + c, sx:sx + c]
+    gl = q_learned[sy:sy + c, sx:sx + c]
+    p64, pp, pl = db(ref), db(gp), db(gl)
+    return {"crop": f"central {c}x{c} of the bench frame", "psnr_db_vs_truth": {"fp64_oracle": p64, "plain_gpu": pp,
+            "learned": pl}, "learned_loss_db_vs_fp64_oracle": p64 - pl, "plain_gpu_max_abs_vs_fp64": float(
+            np.abs(gp - ref).max()), "oracle_seconds": secs}
 
 
 def cpu_baseline(threads: int | None = None, repeats: int = 3) -> dict:
@@ -468,6 +503,11 @@ def run_ours(args):
 
     plain = device_timed(step_plain)
     learned = device_timed(step_learned)
+    # judge mode (plain NLM on a seeded 1/16 of the tiles judging the network there): its cost
+    net.set_judge(JUDGE_FRACTION, JUDGE_LIMIT, seed=1)
+    learned_judged = device_timed(step_learned)
+    judge = net.judge_stats()
+    net.set_judge(0.0)
     plain_e2e = e2e_timed(step_plain)
     learned_e2e = e2e_timed(step_learned)
 
@@ -573,6 +613,9 @@ def run_ours(args):
             "psnr_loss_db": loss_db, "quality_bound_db": QUALITY_BOUND_DB, "meets_quality_bound": meets,
             "quality_sample": f"central {cw}x{ch} crop of the frame, PSNR against the noise-free scene (x WB); "
                               "plain GPU NLM stands for the FP64 oracle (they agree within 2e-4 max-abs)",
+            "judge": {"fraction": JUDGE_FRACTION, "limit_sigma": JUDGE_LIMIT, "value": learned_judged["value"],
+                      "ms_per_step": learned_judged["ms_per_step"],
+                      "cost_ms_per_step": learned_judged["ms_per_step"] - learned["ms_per_step"], **judge},
             "roofline": roof_conv, "weights": "darkslide_b200/weights/cnn_nlm.bin", "dtype": "bf16 (fp32 accumulate)",
             "clocks": learned["clocks"],
         }
@@ -600,6 +643,7 @@ def run_ours(args):
         }
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}
+            learned_info["quality_vs_fp64_oracle"] = cpu_fp64_quality(q_plain, q_learned, qx, qy)
         if batched is not None:
             line["batched"] = batched
         print(json.dumps(line), flush=True)
