@@ -11,10 +11,12 @@
 // and ~8 FP32 operations; what binds is the shared-memory traffic of the
 // separable box sums (one 128-byte wavefront per clock per SM), so the
 // layout minimises shared bytes per update:
-//  - one CTA (512 threads, one per SM) owns a 64-wide tile of one channel,
-//    TY = 64 - 2P rows tall, so that the horizontal box sums it needs cover
-//    exactly 64 rows; the three channels of a tile are adjacent in launch
-//    order, so the interleaved RGB lines they all read come from L2;
+//  - one CTA (256 threads, two per SM, so that one CTA's row phase, heavy on
+//    shared stores, overlaps the other's column phase, heavy on ex2) owns a
+//    32-wide tile of one channel, TY = 64 - 2P rows tall, so that the
+//    horizontal box sums it needs cover exactly 64 rows; the three channels
+//    of a tile are adjacent in launch order, so the interleaved RGB lines
+//    they all read come from L2;
 //  - the tile plus its S+P+1 halo is staged once in shared memory, PRE-SCALED
 //    by sigma = sqrt(log2(e) / (h^2 (2P+1)^2)): the squared differences of
 //    scaled samples sum directly to the ex2 exponent, so a weight costs one
@@ -49,7 +51,7 @@ using namespace nlmk;
 // grid: (tiles_x * C, tile rows); block x = tile_x * C + channel, so the C
 // channels of a tile run side by side
 template <int P, bool F16>
-__global__ void __launch_bounds__(NLM_THREADS, 1) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
+__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
                                                                   int S, float sigma, const float* __restrict__ h_dev,
                                                                   float norm2_log2e,
                                                                   const unsigned char* __restrict__ tile_flags,
@@ -79,7 +81,7 @@ __global__ void stamp_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
 // last tile of frame f is done, stamps[f] = the device clock (ns), so the
 // host can report per-frame completion times.
 template <int P>
-__global__ void __launch_bounds__(NLM_THREADS, 1) nlm_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
+__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
                                                                    int total, int S, unsigned* __restrict__ done,
                                                                    unsigned long long* __restrict__ stamps) {
   extern __shared__ float4 smem4[];

@@ -11,8 +11,8 @@
 namespace {
 namespace nlmk {
 
-constexpr int NLM_THREADS = 512;
-constexpr int TX = 64;      // tile width
+constexpr int NLM_THREADS = 256;  // two CTAs per SM: one's row phase overlaps the other's column phase
+constexpr int TX = 32;      // tile width
 constexpr int HRW = 64;     // H rows per offset (TY + 2P)
 constexpr int SEG = 16;     // phase-A segment width
 constexpr int NI = 4;       // dx per block (one shifted-row load serves all four)
@@ -62,7 +62,7 @@ __device__ __forceinline__ float ldp(const __half* p) { return __half2float(*p);
 __device__ __forceinline__ void stp(float* p, float v) { *p = v; }
 __device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v); }
 
-// One 64 x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
+// One TX x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
 // image, by NLM_THREADS threads; smem holds nlm_smem_bytes(S, P, F16) bytes.
 //
 // Offsets are taken in blocks of up to NI dx x NJ dy. Phase A (thread =
@@ -111,14 +111,14 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
 
   // ---- phase-A role: H row `arow` (tile row arow - P), segment at ax0, dy index aj
   const int arow = tid & (HRW - 1);
-  const int ax0 = ((tid >> 6) & 3) * SEG;
-  const int aj = tid >> 8;
+  const int ax0 = ((tid >> 6) & (TX / SEG - 1)) * SEG;
+  const int aj = tid / (HRW * (TX / SEG));
   const int aprow = clampi(Y0 + arow - P, 0, H - 1) - oy0;  // plane row of the clamped H row
   const int acol0 = ax0 - P + g.R;  // plane column of difference 0 (interior tiles)
   // ---- phase-B role: column bcol, rows [brow0, brow0 + RB) (clipped to TY), dx half bk
   const int bcol = tid & (TX - 1);
-  const int brow0 = ((tid >> 6) & 3) * RB;
-  const int bk = tid >> 8;
+  const int brow0 = ((tid / TX) & 3) * RB;
+  const int bk = tid / (4 * TX);
 
   __syncthreads();
   float pv[DW];  // centre samples of this thread's phase-A segment
@@ -242,7 +242,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
   float* XA = HB;
   float* XS = HB + TX * 4 * RB;
   float* XC = HB + 2 * TX * 4 * RB;
-  const int slot = ((tid >> 6) & 3) * RB * TX + bcol;  // (quarter, row r) x column
+  const int slot = ((tid / TX) & 3) * RB * TX + bcol;  // (quarter, row r) x column
   if (bk == 1) {
 #pragma unroll
     for (int r = 0; r < RB; r++) {
