@@ -584,6 +584,41 @@ __global__ void judge_decide_kernel(const float* __restrict__ save, float* __res
   }
 }
 
+// Layout conversions of the tensor-core training engine. A batch of B crops
+// of H x W pixels lives in the tensor-core layout as one frame [C/8][Hp][Wp][8]
+// whose crop b occupies rows b * period .. b * period + H - 1 (period = H +
+// the largest dilation; the rows between crops and the padding are zero);
+// the mma.sync weight-gradient kernels read NHWC [B][H][W][C].
+// NHWC -> tensor-core layout (only the crops' pixels are written).
+template <int C>
+__global__ void nhwc_to_tc_kernel(const bf16* __restrict__ x, int B, int H, int W, int period, int wp, size_t plane,
+                                  bf16* __restrict__ y) {
+  const size_t n = (size_t)B * H * W * (C / 8);
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cb = (int)(i % (C / 8));
+  const size_t p = i / (C / 8);
+  const int b = (int)(p / ((size_t)H * W));
+  const int r = (int)(p - (size_t)b * H * W), py = r / W, px = r - py * W;
+  const uint4 v = reinterpret_cast<const uint4*>(x)[i];
+  reinterpret_cast<uint4*>(y)[(size_t)cb * plane + (size_t)(b * period + py) * wp + px] = v;
+}
+
+// tensor-core layout -> NHWC
+template <int C>
+__global__ void tc_to_nhwc_kernel(const bf16* __restrict__ y, int B, int H, int W, int period, int wp, size_t plane,
+                                  bf16* __restrict__ x) {
+  const size_t n = (size_t)B * H * W * (C / 8);
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cb = (int)(i % (C / 8));
+  const size_t p = i / (C / 8);
+  const int b = (int)(p / ((size_t)H * W));
+  const int r = (int)(p - (size_t)b * H * W), py = r / W, px = r - py * W;
+  reinterpret_cast<uint4*>(x)[i] =
+      reinterpret_cast<const uint4*>(y)[(size_t)cb * plane + (size_t)(b * period + py) * wp + px];
+}
+
 // ------------------------------------------------------------------ host side
 
 template <int CIN, int COUT, int EPI, int D>
@@ -654,12 +689,22 @@ constexpr int cnn_reach() {
   return r;
 }
 
+// the largest dilation: zero rows between the crops of a tensor-core training batch
+constexpr int cnn_max_dil() {
+  int d = 1;
+  for (int l = 0; l < NL; l++) d = LAYERS[l].dil > d ? LAYERS[l].dil : d;
+  return d;
+}
+
 }  // namespace
 
 int ds_cnn_halo_rows() { return cnn_reach(); }
 
 // ----------------------------------------------------------------- network
 
+cudaError_t ds_tc_layer(cudaStream_t st, int kind, int dil, const void* x, int H, int W, const void* wt,
+                        const float* bias, void* y, const float* resid, float* yf, const void* mask, int period,
+                        int valid, int* err);
 cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
                               const void* const* wf, const float* const* bias, const int* dil, const float* rgb,
                               float* out, int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end);
@@ -689,6 +734,12 @@ struct DsCnn {
   float* out = nullptr;
   float *wpart = nullptr, *bpart = nullptr, *lpart = nullptr;
   int wgrid = 0, bgrid = 0;
+  // training on the tensor cores: the batch as one frame of crops (see
+  // nhwc_to_tc_kernel); activations, the output gradient and the ping-pong
+  // data gradients in the tensor-core layout
+  bf16* tact[NL] = {};
+  bf16 *tg[2] = {}, *tdy8 = nullptr;
+  int t_period = 0, t_wp = 0, t_hp = 0;
   // inference buffers (grown on demand)
   bf16 *ia = nullptr, *ib = nullptr;
   size_t infer_px = 0;
@@ -767,6 +818,18 @@ cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out) {
     if (e == cudaSuccess) net->wpart = (float*)net->alloc((size_t)net->wgrid * 9 * 48 * 48 * sizeof(float), e);
     if (e == cudaSuccess) net->bpart = (float*)net->alloc((size_t)net->bgrid * 48 * sizeof(float), e);
     if (e == cudaSuccess) net->lpart = (float*)net->alloc((size_t)1024 * sizeof(float), e);
+    // the tensor-core engine's batch frame: crops cnn_max_dil() rows apart, zero between them
+    net->t_period = crop + cnn_max_dil();
+    net->t_wp = (crop + 3) / 4 * 4;
+    net->t_hp = (max_batch * net->t_period + 11) / 12 * 12;
+    const size_t tplane = (size_t)net->t_wp * net->t_hp * 16;  // bytes of an 8-channel block
+    for (int l = 0; l < NL && e == cudaSuccess; l++) net->tact[l] = (bf16*)net->alloc(tplane * (l == 0 ? 2 : 6), e);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) net->tg[k] = (bf16*)net->alloc(tplane * 6, e);
+    if (e == cudaSuccess) net->tdy8 = (bf16*)net->alloc(tplane * 2, e);
+    // zero once: the epilogues write every row of the frame, so the padding rows stay zero
+    for (int l = 0; l < NL && e == cudaSuccess; l++) e = cudaMemset(net->tact[l], 0, tplane * (l == 0 ? 2 : 6));
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaMemset(net->tg[k], 0, tplane * 6);
+    if (e == cudaSuccess) e = cudaMemset(net->tdy8, 0, tplane * 2);
   }
   if (e == cudaSuccess) net->err = (int*)net->alloc(sizeof(int), e);
   if (e == cudaSuccess) net->gsq = (float*)net->alloc(sizeof(float), e);
@@ -840,7 +903,37 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
   if (e != cudaSuccess) return e;
   pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, B, H, W, strength_map, strength,
                                                                   net->act[0]);
-  if ((e = forward(net, st, net->act[0], rgb, B, H, W, net->act, net->out)) != cudaSuccess) return e;
+  // the tensor-core engine: forward and data gradients on tcgen05 over the batch frame; the
+  // weight gradients read NHWC copies of its activations and gradients
+  const bool tc = net->use_tc;
+  const int period = net->t_period, HF = B * period, wp = net->t_wp;
+  const size_t tplane = (size_t)wp * ((HF + 11) / 12 * 12);  // pixels of an 8-channel block of the frame
+  auto to_tc = [&](const bf16* x, int C, bf16* y) {
+    const size_t m = n * (C / 8);
+    if (C == 16) nhwc_to_tc_kernel<16><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(x, B, H, W, period, wp, tplane, y);
+    else nhwc_to_tc_kernel<48><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(x, B, H, W, period, wp, tplane, y);
+    return cudaGetLastError();
+  };
+  auto to_nhwc = [&](const bf16* y, bf16* x) {
+    const size_t m = n * 6;
+    tc_to_nhwc_kernel<48><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(y, B, H, W, period, wp, tplane, x);
+    return cudaGetLastError();
+  };
+  if (tc) {
+    if (B > net->max_batch) return cudaErrorInvalidValue;
+    // the two 16-channel frames are written at the crops' pixels only: zero the rest first
+    if ((e = cudaMemsetAsync(net->tact[0], 0, tplane * 2 * 16, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(net->tdy8, 0, tplane * 2 * 16, st)) != cudaSuccess) return e;
+    if ((e = to_tc(net->act[0], 16, net->tact[0])) != cudaSuccess) return e;
+    for (int l = 0; l < NL && e == cudaSuccess; l++) {
+      const int kind = l == 0 ? 0 : (l == NL - 1 ? 2 : 1);
+      e = ds_tc_layer(st, kind, LAYERS[l].dil, net->tact[l], HF, W, net->wf[l], net->bias[l],
+                      l == NL - 1 ? nullptr : net->tact[l + 1], rgb, net->out, nullptr, period, H, net->err);
+    }
+    if (e != cudaSuccess) return e;
+  } else if ((e = forward(net, st, net->act[0], rgb, B, H, W, net->act, net->out)) != cudaSuccess) {
+    return e;
+  }
   const int lgrid = 512;
   mse_kernel<<<lgrid, CNN_THREADS, 0, st>>>(net->out, tgt, n, strength_map, strength, net->relative_loss, net->dy8,
                                             net->lpart);
@@ -854,6 +947,7 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
     reduce_grads_kernel<<<(nreal + 255) / 256, 256, 0, st>>>(net->wpart, net->wgrid, coutw, cinp, net->bpart,
                                                             net->bgrid, cb, L.cout, L.cin, net->grads + net->off[l]);
   };
+  if (tc && (e = to_nhwc(net->tact[7], net->act[7])) != cudaSuccess) return e;
   if ((e = launch_wgrad<48, 16>(st, net->wgrid, LAYERS[7].dil, net->act[7], net->dy8, B, H, W, net->wpart)) !=
       cudaSuccess)
     return e;
@@ -861,15 +955,33 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
   reduce(7, 16, 48, 16);
   bf16* g = net->gA;
   bf16* gnext = net->gB;
-  if ((e = launch_fwd<16, 48, EPI_MASK>(st, grid, LAYERS[7].dil, net->dy8, B, H, W, net->wd[7], nullptr, g,
-                                        net->act[7], nullptr, nullptr)) != cudaSuccess)
+  int tgi = 0;  // tensor-core engine: the data gradient is in net->tg[tgi]
+  if (tc) {
+    if ((e = to_tc(net->dy8, 16, net->tdy8)) != cudaSuccess) return e;
+    if ((e = ds_tc_layer(st, 3, LAYERS[7].dil, net->tdy8, HF, W, net->wd[7], nullptr, net->tg[0], nullptr, nullptr,
+                         net->tact[7], period, H, net->err)) != cudaSuccess)
+      return e;
+  } else if ((e = launch_fwd<16, 48, EPI_MASK>(st, grid, LAYERS[7].dil, net->dy8, B, H, W, net->wd[7], nullptr, g,
+                                               net->act[7], nullptr, nullptr)) != cudaSuccess) {
     return e;
+  }
   for (int l = 6; l >= 1; l--) {  // layers 7..2 (index l): dW from (act[l], g); g_next = dgrad(g) * [act[l] > 0]
+    if (tc) {
+      if ((e = to_nhwc(net->tg[tgi], g)) != cudaSuccess) return e;
+      if ((e = to_nhwc(net->tact[l], net->act[l])) != cudaSuccess) return e;
+    }
     if ((e = launch_wgrad<48, 48>(st, net->wgrid, LAYERS[l].dil, net->act[l], g, B, H, W, net->wpart)) !=
         cudaSuccess)
       return e;
     bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
     reduce(l, 48, 48, 48);
+    if (tc) {
+      if ((e = ds_tc_layer(st, 4, LAYERS[l].dil, net->tg[tgi], HF, W, net->wd[l], nullptr, net->tg[tgi ^ 1], nullptr,
+                           nullptr, net->tact[l], period, H, net->err)) != cudaSuccess)
+        return e;
+      tgi ^= 1;
+      continue;
+    }
     if ((e = launch_fwd<48, 48, EPI_MASK>(st, grid, LAYERS[l].dil, g, B, H, W, net->wd[l], nullptr, gnext,
                                           net->act[l], nullptr, nullptr)) != cudaSuccess)
       return e;
@@ -877,6 +989,7 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
     g = gnext;
     gnext = tmp;
   }
+  if (tc && (e = to_nhwc(net->tg[tgi], g)) != cudaSuccess) return e;
   // layer 1: dW from (packed input, g)
   if ((e = launch_wgrad<16, 48>(st, net->wgrid, LAYERS[0].dil, net->act[0], g, B, H, W, net->wpart)) !=
       cudaSuccess)

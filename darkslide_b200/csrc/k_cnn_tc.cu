@@ -81,7 +81,9 @@ constexpr int TC_TMEM_COLS = 512;                  // accumulator sets at column
 constexpr size_t TC_MIN_SMEM = 120 * 1024;         // keeps one CTA per SM (the TMEM plan assumes it)
 constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
 
-enum { TC_RELU = 0, TC_RESID = 1 };
+// epilogues: bias + ReLU to BF16 (forward); fp32 residual output (the last
+// layer); ReLU mask of the layer below to BF16, no bias (data gradient)
+enum { TC_RELU = 0, TC_RESID = 1, TC_MASK = 2 };
 
 // Shape of a tile of TR output rows: PR staged rows; SLAB bytes per 8-channel
 // block of the staged tile; a ring slot (SUB) holds the 16 channels of one K
@@ -207,7 +209,13 @@ __device__ __forceinline__ void mma_commit(unsigned bar) {
 // wt: [9][COUT_G][CIN] bf16; NK: output channels per ky block (COUT_G padded
 // to a multiple of 16); y: [COUT_G/8][Hp][Wp][8] bf16 (ReLU; padding columns
 // written as zero, padding rows left alone) or yf: [H][W][3] fp32 = resid +
-// conv (residual). DIL: dilation of the taps. A tile is TR output rows
+// conv (residual). EPI TC_MASK: y = conv x [mask > 0], mask a BF16 tensor
+// laid out like y (the ReLU mask of the layer below, for the data gradient).
+// Batches (training): period > 0 means the frame is crops of `valid` rows
+// stacked `period` rows apart; the rows between them (at least the largest
+// dilation) are written as zero, so the next layer reads zero padding there,
+// and the residual output yf / resid are the crops without those rows.
+// DIL: dilation of the taps. A tile is TR output rows
 // DIL apart (y0, y0 + DIL, ...) by 128 pixels; on that subsampled row grid a
 // dilated conv is an undilated one, so the staging and the stacked-tap MMAs
 // are the same for every DIL.
@@ -215,7 +223,8 @@ template <int CIN, int COUT_G, int NK, int EPI, int DIL, int TR>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     conv_tc_kernel(const __grid_constant__ CUtensorMap xmap, int H, int W, const bf16* __restrict__ wt,
                    const float* __restrict__ bias, bf16* __restrict__ y, const float* __restrict__ resid,
-                   float* __restrict__ yf, int* __restrict__ err) {
+                   float* __restrict__ yf, const bf16* __restrict__ mask, int period, int valid,
+                   int* __restrict__ err) {
   static_assert(CIN % 16 == 0 && NK % 16 == 0 && NK >= COUT_G && 3 * NK <= 256, "shapes");
   typedef TcShape<TR, NK> S;
   constexpr int TC_PR = S::PR, TC_SLAB = S::SLAB, TC_SUB = S::SUB, TC_RING = S::RING, NSETS = S::NSETS;
@@ -256,7 +265,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       v = *reinterpret_cast<const uint4*>(wt + ((size_t)(ky * 3 + kx) * COUT_G + co) * CIN + cb * 8);
     *reinterpret_cast<uint4*>(Bs + (size_t)i * 16) = v;
   }
-  for (int i = tid; i < NK; i += TC_THREADS) bias_s[i] = i < COUT_G ? bias[i] : 0.f;
+  for (int i = tid; i < NK; i += TC_THREADS) bias_s[i] = (bias && i < COUT_G) ? bias[i] : 0.f;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TC_TMEM_COLS));
@@ -377,7 +386,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // hands the accumulator set back, then stores: the MMAs of the next tile need not wait for
     // the stores, which matters when a single set holds the tile.
     constexpr int RPW = (TR + 1) / 2;  // output rows per epilogue warp (the second four may hold one fewer)
-    constexpr int PK = EPI == TC_RELU ? COUT_G / 2 : 3;  // per row: BF16 pairs, or the 3 residual floats
+    constexpr int PK = EPI != TC_RESID ? COUT_G / 2 : 3;  // per row: BF16 pairs, or the 3 residual floats
     static_assert(TC_EPI_WARPS == 8, "two epilogue warps per TMEM lane quarter");
     const int quarter = warp & 3, r0 = (warp >> 2) * RPW, rn = TR - r0 < RPW ? TR - r0 : RPW;
     const int Hp = (H + 11) / 12 * 12;
@@ -414,17 +423,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       for (int i = 0; i < RPW; i++) {
         if (i >= rn) break;
         const unsigned col = tbase + (unsigned)((TR - 1 - (r0 + i)) * NK);
-        if (EPI == TC_RELU) {
+        if (EPI != TC_RESID) {
+          const int gy = y0 + (r0 + i) * DIL;
+          // written as zero: padding columns, rows past the frame, rows between batch crops
+          const bool live = in && gy < H && (period == 0 || gy % period < valid);
 #pragma unroll
           for (int c16 = 0; c16 < COUT_G; c16 += 16) {  // 16 columns at a time keeps the registers low
             unsigned u[16];
             tmem_ld16_async(col + c16, u);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            uint4 mk[2] = {make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u)};
+            if (EPI == TC_MASK && live) {
+#pragma unroll
+              for (int h = 0; h < 2; h++)
+                if (c16 + 8 * h < COUT_G)
+                  mk[h] = *reinterpret_cast<const uint4*>(
+                      mask + ((size_t)((c16 + 8 * h) / 8) * plane + (size_t)gy * Wp + px) * 8);
+            }
 #pragma unroll
             for (int c = c16; c < c16 + 16 && c < COUT_G; c += 2) {
-              __nv_bfloat162 o = __floats2bfloat162_rn(
-                  in ? fmaxf(__uint_as_float(u[c - c16]) + bias_s[c], 0.f) : 0.f,
-                  in ? fmaxf(__uint_as_float(u[c - c16 + 1]) + bias_s[c + 1], 0.f) : 0.f);
+              float v0 = __uint_as_float(u[c - c16]), v1 = __uint_as_float(u[c - c16 + 1]);
+              if (EPI == TC_RELU) {
+                v0 = fmaxf(v0 + bias_s[c], 0.f);
+                v1 = fmaxf(v1 + bias_s[c + 1], 0.f);
+              } else {
+                const unsigned mw = reinterpret_cast<const unsigned*>(&mk[(c - c16) / 8])[((c - c16) % 8) / 2];
+                const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162*>(&mw);
+                v0 = __bfloat162float(m.x) > 0.f ? v0 : 0.f;
+                v1 = __bfloat162float(m.y) > 0.f ? v1 : 0.f;
+              }
+              __nv_bfloat162 o = __floats2bfloat162_rn(live ? v0 : 0.f, live ? v1 : 0.f);
               pk[i][c / 2] = *reinterpret_cast<unsigned*>(&o);
             }
           }
@@ -443,14 +471,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (i >= rn) break;
         const int gy = y0 + (r0 + i) * DIL;
         if (gy >= H || px >= Wp) continue;
-        if (EPI == TC_RELU) {
+        if (EPI != TC_RESID) {
           const size_t pix = (size_t)gy * Wp + px;
 #pragma unroll
           for (int c = 0; c < COUT_G; c += 8)
             *reinterpret_cast<uint4*>(y + ((size_t)(c / 8) * plane + pix) * 8) =
                 make_uint4(pk[i][c / 2], pk[i][c / 2 + 1], pk[i][c / 2 + 2], pk[i][c / 2 + 3]);
-        } else if (in) {
-          const size_t pix = (size_t)gy * W + px;
+        } else if (in && (period == 0 || gy % period < valid)) {
+          // a batch's residual output holds the crops without the rows between them
+          const size_t pix = ((size_t)(period ? gy / period * valid + gy % period : gy)) * W + px;
 #pragma unroll
           for (int c = 0; c < 3; c++) yf[pix * 3 + c] = resid[pix * 3 + c] + __uint_as_float(pk[i][c]);
         }
@@ -478,7 +507,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 template <int CIN, int COUT_G, int NK, int EPI, int DIL, int TR>
 cudaError_t launch_tc_d(cudaStream_t st, const bf16* x, int H, int W, const bf16* wt, const float* bias, bf16* y,
-                        const float* resid, float* yf, int* err) {
+                        const float* resid, float* yf, const bf16* mask, int period, int valid, int* err) {
   static_assert(DIL >= 1 && DIL <= TC_PG && 12 % DIL == 0, "the staged row holds a halo of up to 4 pixels");
   typedef TcShape<TR, NK> S;
   constexpr size_t need = (size_t)S::RING * S::SUB + (size_t)3 * (CIN / 8) * 3 * NK * 16 + NK * 4 +
@@ -510,24 +539,48 @@ cudaError_t launch_tc_d(cudaStream_t st, const bf16* x, int H, int W, const bf16
   const int tiles = ((W + TC_M - 1) / TC_M) * ((H + DIL * TR - 1) / (DIL * TR) * DIL);
   const int grid = tiles < sms ? tiles : sms;
   conv_tc_kernel<CIN, COUT_G, NK, EPI, DIL, TR><<<grid, TC_THREADS, smem, st>>>(map, H, W, wt, bias, y, resid, yf,
-                                                                                err);
+                                                                                mask, period, valid, err);
   return cudaGetLastError();
 }
 
 template <int CIN, int COUT_G, int NK, int EPI,
           int TR = (NK <= 16 ? TC_TR_OUTPUT : (CIN >= 48 ? TC_TR_HIDDEN : TC_TR_INPUT))>
 cudaError_t launch_tc(cudaStream_t st, int dil, const bf16* x, int H, int W, const bf16* wt, const float* bias,
-                      bf16* y, const float* resid, float* yf, int* err) {
+                      bf16* y, const float* resid, float* yf, int* err, const bf16* mask = nullptr, int period = 0,
+                      int valid = 0) {
   switch (dil) {
-    case 1: return launch_tc_d<CIN, COUT_G, NK, EPI, 1, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
-    case 2: return launch_tc_d<CIN, COUT_G, NK, EPI, 2, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
-    case 3: return launch_tc_d<CIN, COUT_G, NK, EPI, 3, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
-    case 4: return launch_tc_d<CIN, COUT_G, NK, EPI, 4, TR>(st, x, H, W, wt, bias, y, resid, yf, err);
+    case 1: return launch_tc_d<CIN, COUT_G, NK, EPI, 1, TR>(st, x, H, W, wt, bias, y, resid, yf, mask, period, valid, err);
+    case 2: return launch_tc_d<CIN, COUT_G, NK, EPI, 2, TR>(st, x, H, W, wt, bias, y, resid, yf, mask, period, valid, err);
+    case 3: return launch_tc_d<CIN, COUT_G, NK, EPI, 3, TR>(st, x, H, W, wt, bias, y, resid, yf, mask, period, valid, err);
+    case 4: return launch_tc_d<CIN, COUT_G, NK, EPI, 4, TR>(st, x, H, W, wt, bias, y, resid, yf, mask, period, valid, err);
     default: return cudaErrorInvalidValue;
   }
 }
 
 }  // namespace
+
+// One conv layer of a training batch on the tensor cores (the batch is a frame
+// of crops `valid` rows tall stacked `period` rows apart; see conv_tc_kernel).
+// kind: 0 forward 16 -> 48 (input layer), 1 forward 48 -> 48, 2 forward
+// 48 -> 3 with the residual (yf = resid + conv, both compact crops), 3 data
+// gradient 16 -> 48 (the output layer's), 4 data gradient 48 -> 48; the data
+// gradients apply the ReLU mask `mask` and no bias.
+cudaError_t ds_tc_layer(cudaStream_t st, int kind, int dil, const void* x, int H, int W, const void* wt,
+                        const float* bias, void* y, const float* resid, float* yf, const void* mask, int period,
+                        int valid, int* err) {
+  const bf16* xi = static_cast<const bf16*>(x);
+  const bf16* w = static_cast<const bf16*>(wt);
+  bf16* yo = static_cast<bf16*>(y);
+  const bf16* m = static_cast<const bf16*>(mask);
+  switch (kind) {
+    case 0: return launch_tc<16, 48, 48, TC_RELU>(st, dil, xi, H, W, w, bias, yo, nullptr, nullptr, err, nullptr, period, valid);
+    case 1: return launch_tc<48, 48, 48, TC_RELU>(st, dil, xi, H, W, w, bias, yo, nullptr, nullptr, err, nullptr, period, valid);
+    case 2: return launch_tc<48, 8, 16, TC_RESID>(st, dil, xi, H, W, w, bias, nullptr, resid, yf, err, nullptr, period, valid);
+    case 3: return launch_tc<16, 48, 48, TC_MASK>(st, dil, xi, H, W, w, nullptr, yo, nullptr, nullptr, err, m, period, valid);
+    case 4: return launch_tc<48, 48, 48, TC_MASK>(st, dil, xi, H, W, w, nullptr, yo, nullptr, nullptr, err, m, period, valid);
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 // One image through the 8 layers on the tensor cores. x16: packed input
 // (16 ch, [2][Hp][Wp][8]); a, b: ping-pong activations (48 ch,

@@ -337,9 +337,11 @@ int dsgpu_cnn_set_loss(dsgpu_ctx* ctx, dsgpu_cnn* net, int relative);
 #define DSGPU_CNN_STRENGTH_SCALE 50.0f
 int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, int h, float strength,
                     float* out_rgb, unsigned flags);
-/* Inference engine: 1 (default) tcgen05 tensor cores with TMEM
- * accumulators, 0 the warp-level mma.sync kernels the training uses.
- * A bounded device wait that gives up makes inference return
+/* Engine: 1 (default) the tcgen05 tensor cores with TMEM accumulators for
+ * inference and for training's forward pass and data gradients (the batch
+ * laid out as one frame of crops with zero rows between them; the weight
+ * gradients stay on mma.sync); 0 the warp-level mma.sync kernels
+ * throughout. A bounded device wait that gives up makes the call return
  * DSGPU_ERR_TIMEOUT. */
 int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* net, int tensor_core_gen5);
 /* The learned stand-in for nlm(in, h_param, search, patch) with its per-tile

@@ -52,8 +52,13 @@ def test_forward_matches_fp64(torch_dev):
     assert np.abs(out - ref).max() <= 2e-2 * max(scale, 1e-3)
 
 
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
 @pytest.mark.parametrize("crop", [16, 20])
-def test_gradients_match_fp64(torch_dev, crop):
+def test_gradients_match_fp64(torch_dev, crop, engine):
+    """Per-layer weight and bias gradients of a batch against the FP64
+    reference, on either engine: tcgen05 (forward and data gradients on the
+    5th-generation tensor cores over the batch laid out as one frame of
+    crops, weight gradients on mma.sync) or mma.sync throughout."""
     import cnn_ref as C
     from darkslide_b200 import cnn
 
@@ -61,6 +66,7 @@ def test_gradients_match_fp64(torch_dev, crop):
     p = cnn.init_params(5)
     p[-1299:] = np.random.default_rng(5).normal(0, 0.05, 1299)
     net = cnn.ResidualCNN(max_batch=2, crop=crop, params=p)
+    net.set_engine(engine == "tcgen05")
     rgb, tgt, trgb, ttgt = _batch(torch, dev, 2, crop, 7)
     s = 0.5
     g, loss = net.gradients(trgb, s, ttgt)
@@ -75,7 +81,8 @@ def test_gradients_match_fp64(torch_dev, crop):
             assert cos >= 0.995 and rel <= 5e-2, (i, sl, cos, rel)
 
 
-def test_relative_loss_gradients_match_fp64(torch_dev):
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
+def test_relative_loss_gradients_match_fp64(torch_dev, engine):
     """Loss weighted by 1 / strength^2 with a strength map that differs per crop."""
     import cnn_ref as C
     from darkslide_b200 import cnn
@@ -85,6 +92,7 @@ def test_relative_loss_gradients_match_fp64(torch_dev):
     p = cnn.init_params(6)
     p[-1299:] = np.random.default_rng(6).normal(0, 0.05, 1299)
     net = cnn.ResidualCNN(max_batch=2, crop=crop, params=p)
+    net.set_engine(engine == "tcgen05")
     net.set_loss(True)
     rgb, tgt, trgb, ttgt = _batch(torch, dev, 2, crop, 8)
     smap = np.stack([np.full((crop, crop), 0.3, np.float32), np.full((crop, crop), 1.7, np.float32)])
@@ -156,6 +164,29 @@ def test_adam_gradient_norm_clip(torch_dev):
     exp = p1 - 1e-3 * (m2 / (1 - 0.9 ** 2)) / (np.sqrt(v2 / (1 - 0.999 ** 2)) + 1e-8)
     assert np.abs(p1 - p0).max() > 0
     np.testing.assert_allclose(net.get_params(), exp, rtol=1e-4, atol=1e-7)
+
+
+def test_tensor_core_training_matches_mma_sync(torch_dev):
+    """The two training engines on a batch of 4 crops of 32 (smaller than the
+    batch the network was created for): the same loss and gradients up to
+    BF16 rounding of the activations."""
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    p = cnn.init_params(12)
+    p[-1299:] = np.random.default_rng(12).normal(0, 0.05, 1299)
+    net = cnn.ResidualCNN(max_batch=6, crop=32, params=p)
+    rgb, tgt, trgb, ttgt = _batch(torch, dev, 4, 32, 13)
+    g_tc, l_tc = net.gradients(trgb, 0.4, ttgt)
+    net.set_engine(False)
+    g_ms, l_ms = net.gradients(trgb, 0.4, ttgt)
+    g_tc, g_ms = g_tc.cpu().numpy(), g_ms.cpu().numpy()
+    assert abs(l_tc - l_ms) <= 1e-2 * l_ms
+    for i, (ws, bs, _) in enumerate(cnn.layer_slices()):
+        for sl in (ws, bs):
+            a, b = g_tc[sl], g_ms[sl]
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+            assert cos >= 0.995, (i, sl, cos)
 
 
 def test_training_reduces_loss(torch_dev):
