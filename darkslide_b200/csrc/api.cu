@@ -958,7 +958,7 @@ int dsgpu_cnn_gradients(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* rgb, const fl
     DS_TRY(cudaMemcpyAsync(grads, ds_cnn_grad_ptr(c->net), ds_cnn_param_count() * sizeof(float),
                            cudaMemcpyDeviceToDevice, ctx->stream));
   DS_TRY(cudaStreamSynchronize(ctx->stream));
-  return DSGPU_OK;
+  return ds_cnn_take_status(c->net, ctx->stream);  // a tensor-core kernel's bounded wait may have given up
 }
 
 int dsgpu_cnn_train_step(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* rgb, const float* strength_map, float strength,
@@ -970,7 +970,9 @@ int dsgpu_cnn_train_step(dsgpu_ctx* ctx, dsgpu_cnn* c, const float* rgb, const f
   DS_TRY(ds_cnn_gradients(c->net, ctx->stream, rgb, strength_map, strength, target, batch, loss_sum ? &loss : nullptr));
   DS_TRY(ds_cnn_adam(c->net, ctx->stream, lr));
   if (loss_sum) *loss_sum = loss;
-  return DSGPU_OK;
+  // a tensor-core kernel's bounded wait may have given up (checked when the
+  // loss is read back, which synchronises anyway)
+  return loss_sum ? ds_cnn_take_status(c->net, ctx->stream) : DSGPU_OK;
 }
 
 int dsgpu_cnn_set_clip(dsgpu_ctx* ctx, dsgpu_cnn* c, float max_norm) {
