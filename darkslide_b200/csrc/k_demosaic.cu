@@ -5,7 +5,6 @@
 // product before adding it, so the GPU must not contract a*b+c into FMAs for
 // these kernels to reproduce it bit for bit. Divisions are IEEE (__fdiv_rn).
 #include <cfloat>
-#include <type_traits>
 
 #include "internal.cuh"
 #include "nlm_tile.cuh"
@@ -206,103 +205,30 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   auto C = [&](int k) { return fmaxf(M[k], 0.0f); };  // demosaic.rs:154
   const int w1 = RSX, w2 = 2 * RSX, w3 = 3 * RSX, w4 = 4 * RSX;
 
-  // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, edge-3) of the staged region.
-  // Each gradient is a 7-tap filter along one direction (vertical, horizontal,
-  // diagonal, anti-diagonal), so it is computed by walks along that direction:
-  // a thread takes up to LV (LH) consecutive sites of one line and keeps the
-  // 7-sample window in registers (one shared load per site instead of seven);
-  // the 3x3 lpf walks down columns with a 3x3 window. Every value is the
-  // reference's expression in its order, whatever the walk.
-  {
-    constexpr int NX1 = RSX - 6, NY1 = RSY - 6;  // the stage-1 region, from local (3, 3)
-    constexpr int LV = 10, LH = 9;                // walk lengths (LH odd: the lanes of a row hit distinct banks)
-    constexpr int CV = (NY1 + LV - 1) / LV, CH = (NX1 + LH - 1) / LH;
-    constexpr int ND = NX1 + NY1 - 1;             // diagonal lines
-    constexpr int N_V = NX1 * CV, N_H = NY1 * CH, N_D = ND * CV;
-    constexpr int N_ALL = N_V + N_H + 2 * N_D + N_V;
-    // gradient walk from region site (x, y), n sites, step (UX, UY)
-    auto grad_walk = [&](auto ux_tag, auto uy_tag, int x, int y, int n, float* OUT) {
-      constexpr int UX = decltype(ux_tag)::value, UY = decltype(uy_tag)::value;
-      constexpr int STEP = UY * RSX + UX;
-      const int k0 = (y + 3) * RSX + (x + 3);
-      float c[7];
-#pragma unroll
-      for (int j = 0; j < 6; j++) c[j] = C(k0 + (j - 3) * STEP);
-#pragma unroll
-      for (int t = 0; t < (UY ? LV : LH); t++) {
-        if (t < n) {
-          const int k = k0 + t * STEP;
-          c[6] = C(k + 3 * STEP);
-          const int gx = gx0 + 3 + x + t * UX, gy = gy0 + 3 + y + t * UY;
-          float g = 0.f;
-          if (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3)
-            g = sq((c[0] - c[2] - c[4] + c[6]) - 3.0f * (c[1] + c[5]) + 6.0f * c[3]);
-          OUT[k] = g;
-#pragma unroll
-          for (int j = 0; j < 6; j++) c[j] = c[j + 1];
-        }
-      }
-    };
-    for (int it = tid; it < N_ALL; it += NT) {
-      int i = it;
-      if (i < N_V) {  // bv: down column x
-        const int x = i % NX1, y0 = (i / NX1) * LV;
-        grad_walk(std::integral_constant<int, 0>{}, std::integral_constant<int, 1>{}, x, y0, min(LV, NY1 - y0), BV);
-        continue;
-      }
-      i -= N_V;
-      if (i < N_H) {  // bh: along row y
-        const int y = i / CH, x0 = (i % CH) * LH;
-        grad_walk(std::integral_constant<int, 1>{}, std::integral_constant<int, 0>{}, x0, y, min(LH, NX1 - x0), BH);
-        continue;
-      }
-      i -= N_H;
-      if (i < N_D) {  // bp: along (1, 1), the line x - y = d
-        const int d = i % ND - (NY1 - 1), c0 = (i / ND) * LV;
-        const int ylo = max(c0, -d), yhi = min(min(NY1, NX1 - d), c0 + LV);
-        if (ylo < yhi)
-          grad_walk(std::integral_constant<int, 1>{}, std::integral_constant<int, 1>{}, ylo + d, ylo, yhi - ylo, BP);
-        continue;
-      }
-      i -= N_D;
-      if (i < N_D) {  // bq: along (-1, 1), the line x + y = e
-        const int e = i % ND, c0 = (i / ND) * LV;
-        const int ylo = max(c0, e - NX1 + 1), yhi = min(min(NY1, e + 1), c0 + LV);
-        if (ylo < yhi)
-          grad_walk(std::integral_constant<int, -1>{}, std::integral_constant<int, 1>{}, e - ylo, ylo, yhi - ylo, BQ);
-        continue;
-      }
-      i -= N_D;
-      {  // lpf at R/B sites: down column x with a 3x3 window
-        const int x = i % NX1, y0 = (i / NX1) * LV, n = min(LV, NY1 - y0);
-        const int k0 = (y0 + 3) * RSX + (x + 3);
-        float r[3][3];
-#pragma unroll
-        for (int a = 0; a < 2; a++)
-#pragma unroll
-          for (int b = 0; b < 3; b++) r[a][b] = C(k0 + (a - 1) * w1 + (b - 1));
-        const int gx = gx0 + 3 + x;
-#pragma unroll
-        for (int t = 0; t < LV; t++) {
-          if (t < n) {
-            const int k = k0 + t * w1;
-#pragma unroll
-            for (int b = 0; b < 3; b++) r[2][b] = C(k + w1 + (b - 1));
-            const int gy = gy0 + 3 + y0 + t;
-            float lp = 0.f;
-            if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2 && pat.at(gx, gy) != 1)
-              lp = r[1][1] + 0.5f * (r[0][1] + r[2][1] + r[1][0] + r[1][2]) +
-                   0.25f * (r[0][0] + r[0][2] + r[2][0] + r[2][2]);
-            LP[k] = lp;
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-              r[0][b] = r[1][b];
-              r[1][b] = r[2][b];
-            }
-          }
-        }
-      }
+  // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, edge-3) of the staged region
+  for (int i = tid; i < (RSX - 6) * (RSY - 6); i += NT) {
+    const int ly = 3 + i / (RSX - 6), lx = 3 + i % (RSX - 6);
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    const int k = ly * RSX + lx;
+    float bv = 0.f, bh = 0.f, bp = 0.f, bq = 0.f, lp = 0.f;
+    if (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3) {
+      const float c0 = C(k);
+      bv = sq((C(k - w3) - C(k - w1) - C(k + w1) + C(k + w3)) - 3.0f * (C(k - w2) + C(k + w2)) + 6.0f * c0);
+      bh = sq((C(k - 3) - C(k - 1) - C(k + 1) + C(k + 3)) - 3.0f * (C(k - 2) + C(k + 2)) + 6.0f * c0);
+      bp = sq((C(k - w3 - 3) - C(k - w1 - 1) - C(k + w1 + 1) + C(k + w3 + 3)) - 3.0f * (C(k - w2 - 2) + C(k + w2 + 2)) +
+              6.0f * c0);
+      bq = sq((C(k - w3 + 3) - C(k - w1 + 1) - C(k + w1 - 1) + C(k + w3 - 3)) - 3.0f * (C(k - w2 + 2) + C(k + w2 - 2)) +
+              6.0f * c0);
     }
+    if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2 && pat.at(gx, gy) != 1) {
+      lp = C(k) + 0.5f * (C(k - w1) + C(k + w1) + C(k - 1) + C(k + 1)) +
+           0.25f * (C(k - w1 - 1) + C(k - w1 + 1) + C(k + w1 - 1) + C(k + w1 + 1));
+    }
+    BV[k] = bv;
+    BH[k] = bh;
+    BP[k] = bp;
+    BQ[k] = bq;
+    LP[k] = lp;
   }
   __syncthreads();
 
