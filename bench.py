@@ -191,7 +191,7 @@ def cpu_sample_text() -> str:
             "Rust reference cannot be built here): normalise + RCD + clip plane + NLM x3")
 
 
-FP64_CROP = 256  # central crop on which the FP64 oracle checks the quality claim
+FP64_CROP = 1024  # central crop on which the FP64 oracle checks the quality claim
 
 
 def cpu_fp64_quality(q_plain, q_learned, qx: int, qy: int) -> dict:

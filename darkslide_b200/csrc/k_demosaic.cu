@@ -168,13 +168,18 @@ __device__ __forceinline__ float sq(float v) { return v * v; }
 // rcd_smem(TXT, TYT) bytes. The value at every site depends only on the
 // frame and the site's global coordinates, so any tiling gives the same
 // output bit for bit.
-template <class Src, int TXT, int TYT, int NT = RCD_THREADS>
-__device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
+// RING: some site of the tile's stage regions lies in the frame's 4-site
+// border ring, where RCD falls back to MHC, which reads data*mul WITHOUT
+// max(0) (demosaic.rs:93-98). Other tiles never need the unclamped value, so
+// their staged plane holds c = max(data*mul, 0) (demosaic.rs:154) directly
+// and the passes skip a max per read.
+template <class Src, int TXT, int TYT, int NT, bool RING>
+__device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
                                          float* __restrict__ out_rgb, float* __restrict__ out_clip, int tile_x,
                                          int tile_y, float* smem) {
   static_assert(TXT % 2 == 0 && TYT % 2 == 0, "tile sides must be even");
   constexpr int RSX = TXT + 2 * RH, RSY = TYT + 2 * RH, RA = RSX * RSY;
-  float* M = smem;  // data*mul (clamped-site load), not max(0)
+  float* M = smem;  // data*mul (clamped-site load): not max(0) in RING tiles, max(0) otherwise
   float* BV = M + RA;   // bv, later g
   float* BH = BV + RA;  // bh, later r after 4.3
   float* BP = BH + RA;  // bp, later b after 4.3
@@ -197,12 +202,13 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
     const int gx = clampi(gx0 + lx, 0, W - 1), gy = clampi(gy0 + ly, 0, H - 1);
     const int col = pat.at(gx, gy);
     const float v = src.load(gx, gy, col);
-    M[i] = v * (col == 0 ? m0 : (col == 1 ? m1 : m2));
+    const float vm = v * (col == 0 ? m0 : (col == 1 ? m1 : m2));
+    M[i] = RING ? vm : fmaxf(vm, 0.0f);
     CL[i] = v >= 0.995f ? 1 : 0;
   }
   __syncthreads();
 
-  auto C = [&](int k) { return fmaxf(M[k], 0.0f); };  // demosaic.rs:154
+  auto C = [&](int k) { return RING ? fmaxf(M[k], 0.0f) : M[k]; };  // demosaic.rs:154
   const int w1 = RSX, w2 = 2 * RSX, w3 = 3 * RSX, w4 = 4 * RSX;
 
   // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, edge-3) of the staged region
@@ -415,6 +421,22 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
     o[2] = B43[k];
     if (out_clip) out_clip[(size_t)gy * W + gx] = clip_at(k);
   }
+}
+
+// One TXT x TYT output tile; see rcd_tile_body. A tile needs the ring code
+// when its stage-3 region (the widest one that can fall back to MHC: local
+// sites [5, edge - 5)) reaches the border ring [0, 4) or [W - 4, W).
+template <class Src, int TXT, int TYT, int NT = RCD_THREADS>
+__device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
+                                         float* __restrict__ out_rgb, float* __restrict__ out_clip, int tile_x,
+                                         int tile_y, float* smem) {
+  constexpr int RSX = TXT + 2 * RH, RSY = TYT + 2 * RH;
+  const int gx0 = tile_x * TXT - RH, gy0 = tile_y * TYT - RH;
+  const bool ring = gx0 + 5 < 4 || gx0 + RSX - 5 > W - 4 || gy0 + 5 < 4 || gy0 + RSY - 5 > H - 4;
+  if (ring)
+    rcd_tile_body<Src, TXT, TYT, NT, true>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
+  else
+    rcd_tile_body<Src, TXT, TYT, NT, false>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
 }
 
 template <class Src>
