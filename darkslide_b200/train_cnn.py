@@ -96,7 +96,9 @@ def psnr(a, b, peak=1.0):
 
 def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=64, mix=8, warmup=500,
           clip_factor=3.0, seed=0, out=None, resume=None, log_every=200, verbose=True, dataset=200000,
-          relative=False, scenes="any"):
+          relative=False, scenes="any", engine="tcgen05"):
+    """engine: "tcgen05" (forward and data gradients on the 5th-generation
+    tensor cores, weight gradients on mma.sync) or "mma.sync" throughout."""
     import torch
 
     dev = torch.device("cuda", 0)
@@ -104,6 +106,7 @@ def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=
     ctx = ds.Context(0)
     stream = torch.cuda.Stream(dev)
     net = cnn.ResidualCNN(ctx, max_batch=batch, crop=crop, seed=seed)
+    net.set_engine(engine == "tcgen05")
     if resume:
         net.load(resume)
     net.set_loss(relative)
@@ -236,10 +239,11 @@ def main():
     ap.add_argument("--out", default=None)
     ap.add_argument("--resume", default=None)
     ap.add_argument("--eval", type=int, default=4)
+    ap.add_argument("--engine", default="tcgen05", choices=["tcgen05", "mma.sync"])
     a = ap.parse_args()
     net, losses, secs = train(a.crops, a.batch, a.crop, a.lr, frame=a.frame, mix=a.mix, warmup=a.warmup,
                               clip_factor=a.clip, seed=a.seed, out=a.out, resume=a.resume, dataset=a.dataset,
-                              relative=a.relative_loss, scenes=a.scenes)
+                              relative=a.relative_loss, scenes=a.scenes, engine=a.engine)
     print(f"trained {a.crops} crop visits of a {a.dataset}-crop set in {secs:.1f} s", flush=True)
     if a.eval:
         evaluate(net, a.eval)
