@@ -583,6 +583,16 @@ def run_ours(args):
             "algorithmic": "14 B/px (u16 in, 3xf32 out)", "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)",
             "launch_ms": dem_launch_ms,
         }
+        rcd_inst = traffic.get("rcd_warp_instructions_per_launch")
+        if rcd_inst:  # what binds RCD: instruction issue (4 warp instructions / clock / SM) and shared memory
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            issue_peak = 4.0 * sms * 1.965e9 / 1e12  # warp instructions per second at the rated clock, x1e12
+            achieved_inst = rcd_inst / (dem_launch_ms * 1e-3) / 1e12
+            roof_rcd["instruction_roof"] = {
+                "achieved": achieved_inst, "peak": issue_peak, "unit": "Twarp-inst/s", "frac": achieved_inst / issue_peak,
+                "instructions_per_launch": rcd_inst,
+                "source": "smsp__inst_executed.sum of one launch at 6000x4000, profiles/dram_traffic.txt; peak = 4 warp "
+                          "instructions per clock per SM at 1965 MHz"}
         # learned path: the hidden conv layer (48 -> 48, 3x3) on the tensor cores
         hid_ms, hid_n = learned["cnn_hidden"]
         conv_ms = hid_ms / max(6 * hid_n, 1)
