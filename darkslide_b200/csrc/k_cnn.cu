@@ -253,23 +253,58 @@ __global__ void __launch_bounds__(CNN_THREADS) conv_wgrad_kernel(const bf16* __r
   }
 }
 
-// Per-CTA channel sums of dY (bias gradient partials).
+// Per-CTA channel sums of dY (bias gradient partials). Each thread reads one
+// 16-byte group of 8 channels of a pixel per load, so a warp's loads cover
+// whole pixel rows; the CTA's pixel lanes are summed in a fixed order.
 template <int C>
-__global__ void bias_grad_kernel(const bf16* __restrict__ dy, size_t n, float* __restrict__ part) {
-  __shared__ float s[CNN_THREADS];
-  const int ch = threadIdx.x % C;
-  const int lanes = (CNN_THREADS / C) * C;  // threads that take part
-  float acc = 0.f;
-  if ((int)threadIdx.x < lanes)
-    for (size_t p = blockIdx.x * (size_t)(lanes / C) + threadIdx.x / C; p < n; p += (size_t)gridDim.x * (lanes / C))
-      acc += __bfloat162float(dy[p * C + ch]);
-  s[threadIdx.x] = (int)threadIdx.x < lanes ? acc : 0.f;
-  __syncthreads();
-  if ((int)threadIdx.x < C) {
-    float t = 0.f;
-    for (int i = threadIdx.x; i < lanes; i += C) t += s[i];
-    part[(size_t)blockIdx.x * C + threadIdx.x] = t;
+__global__ void __launch_bounds__(CNN_THREADS) bias_grad_kernel(const bf16* __restrict__ dy, size_t n,
+                                                                float* __restrict__ part) {
+  constexpr int G = C / 8;             // 8-channel groups per pixel
+  constexpr int PL = CNN_THREADS / G;  // pixel lanes per CTA
+  __shared__ float s[PL * C];
+  const int t = threadIdx.x;
+  if (t < PL * G) {
+    const int gi = t % G, pl = t / G;
+    float acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[j] = 0.f;
+    const uint4* src = reinterpret_cast<const uint4*>(dy) + gi;
+    const size_t stride = (size_t)gridDim.x * PL;
+#pragma unroll 4
+    for (size_t p = (size_t)blockIdx.x * PL + pl; p < n; p += stride) {
+      const uint4 v = __ldg(src + p * G);
+      const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float2 f = __bfloat1622float2(h2[q]);
+        acc[2 * q] += f.x;
+        acc[2 * q + 1] += f.y;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[pl * C + gi * 8 + j] = acc[j];
   }
+  __syncthreads();
+  if (t < C) {
+    float sum = 0.f;
+    for (int pl = 0; pl < PL; pl++) sum += s[pl * C + t];
+    part[(size_t)blockIdx.x * C + t] = sum;
+  }
+}
+
+// sum of p[k * stride], k < n, in eight interleaved partial sums (eight
+// loads in flight per thread) added in a fixed order
+__device__ __forceinline__ float sum_strided(const float* __restrict__ p, size_t stride, int n) {
+  float a[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) a[j] = 0.f;
+  int k = 0;
+  for (; k + 8 <= n; k += 8) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] += p[(size_t)(k + j) * stride];
+  }
+  for (; k < n; k++) a[0] += p[(size_t)k * stride];
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
 }
 
 // grads[layer] (real shape [9][cout][cin] then [cout]) from the partials
@@ -281,14 +316,9 @@ __global__ void reduce_grads_kernel(const float* __restrict__ wpart, int nw, int
   if (i < nwreal) {
     const int tap = i / (cout * cin), r = i - tap * cout * cin, co = r / cin, ci = r - co * cin;
     const size_t off = ((size_t)tap * coutw + co) * cinp + ci, stride = (size_t)9 * coutw * cinp;
-    float s = 0.f;
-    for (int k = 0; k < nw; k++) s += wpart[k * stride + off];
-    gw[i] = s;
+    gw[i] = sum_strided(wpart + off, stride, nw);
   } else if (i < nwreal + cout) {
-    const int co = i - nwreal;
-    float s = 0.f;
-    for (int k = 0; k < nb; k++) s += bpart[(size_t)k * cb + co];
-    gw[i] = s;
+    gw[i] = sum_strided(bpart + (i - nwreal), (size_t)cb, nb);
   }
 }
 
@@ -394,21 +424,25 @@ __global__ void mse_kernel(const float* __restrict__ out, const float* __restric
 }
 
 // Sum of squares of the n gradients into *out (one CTA, fixed order: deterministic).
-__global__ void grad_sqsum_kernel(const float* __restrict__ gr, int n, float* __restrict__ out) {
-  __shared__ float s[1024];
+// Per-CTA partial sums of squared gradients (SQ_BLOCKS CTAs).
+constexpr int SQ_BLOCKS = 64;
+__global__ void __launch_bounds__(CNN_THREADS) grad_sqsum_kernel(const float* __restrict__ gr, int n,
+                                                                 float* __restrict__ part) {
+  __shared__ float s[CNN_THREADS];
   float acc = 0.f;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += gr[i] * gr[i];
+  for (int i = blockIdx.x * CNN_THREADS + threadIdx.x; i < n; i += gridDim.x * CNN_THREADS) acc += gr[i] * gr[i];
   s[threadIdx.x] = acc;
   __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+  for (int k = CNN_THREADS / 2; k > 0; k >>= 1) {
     if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
     __syncthreads();
   }
-  if (threadIdx.x == 0) *out = s[0];
+  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
 }
 
 // Adam; with clip > 0 the gradient is first scaled by min(1, clip / |g|)
-// (global L2 norm from grad_sqsum_kernel).
+// (global L2 norm: the SQ_BLOCKS partials of grad_sqsum_kernel, added in a
+// fixed order by every thread).
 __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ gr, float* __restrict__ m,
                             float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1,
                             float c2, const float* __restrict__ gsq, float clip) {
@@ -416,7 +450,9 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ gr,
   if (i >= n) return;
   float gi = gr[i];
   if (clip > 0.f) {
-    const float norm = sqrtf(*gsq);
+    float sq = 0.f;
+    for (int b = 0; b < SQ_BLOCKS; b++) sq += gsq[b];
+    const float norm = sqrtf(sq);
     if (norm > clip) gi *= clip / norm;
   }
   const float mi = b1 * m[i] + (1.f - b1) * gi;
@@ -725,7 +761,7 @@ struct DsCnn {
   float clip = 0.f;      // global gradient-norm clip of the Adam step (0: off)
   int relative_loss = 0; // 1: squared errors weighted by 1 / strength^2
   cudaEvent_t mark_a = nullptr, mark_b = nullptr;  // profiling: around the hidden layers of inference
-  float* gsq = nullptr;  // device: sum of squared gradients
+  float* gsq = nullptr;  // device: SQ_BLOCKS partial sums of squared gradients
   // training buffers (max_batch crops of crop x crop)
   bf16* act[NL] = {};   // act[0] = packed input (16 ch), act[l] = output of layer l (48 ch), l = 1..7
   bf16* gA = nullptr;   // gradient ping
@@ -814,7 +850,7 @@ cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
     net->wgrid = sms * 2;
-    net->bgrid = sms;
+    net->bgrid = sms * 4;
     if (e == cudaSuccess) net->wpart = (float*)net->alloc((size_t)net->wgrid * 9 * 48 * 48 * sizeof(float), e);
     if (e == cudaSuccess) net->bpart = (float*)net->alloc((size_t)net->bgrid * 48 * sizeof(float), e);
     if (e == cudaSuccess) net->lpart = (float*)net->alloc((size_t)1024 * sizeof(float), e);
@@ -832,7 +868,7 @@ cudaError_t ds_cnn_create(int max_batch, int crop, DsCnn** out) {
     if (e == cudaSuccess) e = cudaMemset(net->tdy8, 0, tplane * 2);
   }
   if (e == cudaSuccess) net->err = (int*)net->alloc(sizeof(int), e);
-  if (e == cudaSuccess) net->gsq = (float*)net->alloc(sizeof(float), e);
+  if (e == cudaSuccess) net->gsq = (float*)net->alloc(SQ_BLOCKS * sizeof(float), e);
   if (e == cudaSuccess) net->judge_stats = (unsigned*)net->alloc(4 * sizeof(unsigned), e);
   if (e == cudaSuccess) e = cudaMemset(net->judge_stats, 0, 4 * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(net->err, 0, sizeof(int));
@@ -1013,7 +1049,7 @@ cudaError_t ds_cnn_adam(DsCnn* net, cudaStream_t st, float lr) {
   net->step++;
   net->packed = false;
   const float c1 = 1.0f - (float)pow(b1, (double)net->step), c2 = 1.0f - (float)pow(b2, (double)net->step);
-  if (net->clip > 0.f) grad_sqsum_kernel<<<1, 1024, 0, st>>>(net->grads, net->n_params, net->gsq);
+  if (net->clip > 0.f) grad_sqsum_kernel<<<SQ_BLOCKS, CNN_THREADS, 0, st>>>(net->grads, net->n_params, net->gsq);
   adam_kernel<<<(net->n_params + 255) / 256, 256, 0, st>>>(net->params, net->grads, net->m, net->v, net->n_params, lr,
                                                            b1, b2, eps, c1, c2, net->gsq, net->clip);
   return cudaGetLastError();

@@ -137,8 +137,9 @@ def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=
         take = [pool.pop() for _ in range(batch)]
         xb = torch.stack([r[y:y + crop, x:x + crop] for (r, _, _, y, x) in take]).contiguous()
         tb = torch.stack([t[y:y + crop, x:x + crop] for (_, t, _, y, x) in take]).contiguous()
-        smap = torch.stack([torch.full((crop, crop), hp * cnn.STRENGTH_SCALE, device=dev)
-                            for (_, _, hp, _, _) in take]).contiguous()
+        hps = np.array([hp * cnn.STRENGTH_SCALE for (_, _, hp, _, _) in take], np.float32)
+        smap = torch.from_numpy(hps).pin_memory().to(dev, non_blocking=True)
+        smap = smap.view(batch, 1, 1).expand(batch, crop, crop).contiguous()
         return xb, tb, smap
 
     with torch.cuda.stream(stream):
