@@ -173,7 +173,10 @@ __device__ __forceinline__ float sq(float v) { return v * v; }
 // max(0) (demosaic.rs:93-98). Other tiles never need the unclamped value, so
 // their staged plane holds c = max(data*mul, 0) (demosaic.rs:154) directly
 // and the passes skip a max per read.
-template <class Src, int TXT, int TYT, int NT, bool RING>
+// FULL (implies !RING): the whole staged region lies inside the frame, so no
+// load is clamped and every stage's border rule holds at every site the tile
+// computes; the tile skips those tests.
+template <class Src, int TXT, int TYT, int NT, bool RING, bool FULL = false>
 __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
                                          float* __restrict__ out_rgb, float* __restrict__ out_clip, int tile_x,
                                          int tile_y, float* smem) {
@@ -199,7 +202,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
   // stage 0: load with clamped coordinates
   for (int i = tid; i < RA; i += NT) {
     const int ly = i / RSX, lx = i - ly * RSX;
-    const int gx = clampi(gx0 + lx, 0, W - 1), gy = clampi(gy0 + ly, 0, H - 1);
+    const int gx = FULL ? gx0 + lx : clampi(gx0 + lx, 0, W - 1), gy = FULL ? gy0 + ly : clampi(gy0 + ly, 0, H - 1);
     const int col = pat.at(gx, gy);
     const float v = src.load(gx, gy, col);
     const float vm = v * (col == 0 ? m0 : (col == 1 ? m1 : m2));
@@ -217,7 +220,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RSX + lx;
     float bv = 0.f, bh = 0.f, bp = 0.f, bq = 0.f, lp = 0.f;
-    if (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3) {
+    if (FULL || (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3)) {
       const float c0 = C(k);
       bv = sq((C(k - w3) - C(k - w1) - C(k + w1) + C(k + w3)) - 3.0f * (C(k - w2) + C(k + w2)) + 6.0f * c0);
       bh = sq((C(k - 3) - C(k - 1) - C(k + 1) + C(k + 3)) - 3.0f * (C(k - 2) + C(k + 2)) + 6.0f * c0);
@@ -226,7 +229,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
       bq = sq((C(k - w3 + 3) - C(k - w1 + 1) - C(k + w1 - 1) + C(k + w3 - 3)) - 3.0f * (C(k - w2 + 2) + C(k + w2 - 2)) +
               6.0f * c0);
     }
-    if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2 && pat.at(gx, gy) != 1) {
+    if ((FULL || (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2)) && pat.at(gx, gy) != 1) {
       lp = C(k) + 0.5f * (C(k - w1) + C(k + w1) + C(k - 1) + C(k + 1)) +
            0.25f * (C(k - w1 - 1) + C(k - w1 + 1) + C(k + w1 - 1) + C(k + w1 + 1));
     }
@@ -244,7 +247,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RSX + lx;
     float vh = 0.5f, pq = 0.5f;
-    if (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4) {
+    if (FULL || (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4)) {
       const float vs = fmaxf(BV[k - w1] + BV[k] + BV[k + w1], eps);
       const float hs = fmaxf(BH[k - 1] + BH[k] + BH[k + 1], eps);
       vh = __fdiv_rn(vs, vs + hs);
@@ -276,7 +279,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
     const bool g_here = pat.at(gx, gy) == 1;
     return lx0 + ((g_here == want_g) ? 0 : 1);
   };
-  auto inner = [&](int gx, int gy) { return gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4; };
+  auto inner = [&](int gx, int gy) { return FULL || (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4); };
 
   // stage 3: green (:203-214 init, :222-245 step 3) on [5, edge-5): (RSY-10)
   // rows x (RSX-10)/2 sites of each class
@@ -356,7 +359,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
     R43[k] = r;
     B43[k] = b;
   }
-  for (int i = tid; i < S4Y * S4H; i += NT) {  // green sites of the ring
+  for (int i = tid; i < (RING ? S4Y * S4H : 0); i += NT) {  // green sites of the ring (RING tiles only)
     const int ly = 7 + i / S4H, lx = col_start(ly, 7, true) + 2 * (i % S4H);
     if (lx >= RSX - 7) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
@@ -381,7 +384,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
     const int ly = RH + i / TH, lx = col_start(ly, RH, true) + 2 * (i % TH);
     if (lx >= RH + TXT) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
-    if (gx >= W || gy >= H) continue;
+    if (!FULL && (gx >= W || gy >= H)) continue;
     const int k = ly * RSX + lx;
     float r = R43[k], b = B43[k];
     const float g = G[k];
@@ -413,7 +416,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
     const int ly = RH + i / TH, lx = col_start(ly, RH, false) + 2 * (i % TH);
     if (lx >= RH + TXT) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
-    if (gx >= W || gy >= H) continue;
+    if (!FULL && (gx >= W || gy >= H)) continue;
     const int k = ly * RSX + lx;
     float* o = out_rgb + ((size_t)gy * W + gx) * 3;
     o[0] = R43[k];
@@ -433,7 +436,10 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   constexpr int RSX = TXT + 2 * RH, RSY = TYT + 2 * RH;
   const int gx0 = tile_x * TXT - RH, gy0 = tile_y * TYT - RH;
   const bool ring = gx0 + 5 < 4 || gx0 + RSX - 5 > W - 4 || gy0 + 5 < 4 || gy0 + RSY - 5 > H - 4;
-  if (ring)
+  const bool full = gx0 >= 0 && gx0 + RSX <= W && gy0 >= 0 && gy0 + RSY <= H;
+  if (full)
+    rcd_tile_body<Src, TXT, TYT, NT, false, true>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
+  else if (ring)
     rcd_tile_body<Src, TXT, TYT, NT, true>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
   else
     rcd_tile_body<Src, TXT, TYT, NT, false>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
