@@ -92,7 +92,7 @@ cudaError_t ds_launch_rcd_f32(cudaStream_t st, ds_src_f32 src, int w, int h, ds_
                               float* out_rgb, float* out_clip);
 cudaError_t ds_launch_rcd_u16(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, const float mul[3],
                               float* out_rgb, float* out_clip);
-constexpr int DS_RCD_TILE = 24;  // rows of a tile row of the one-frame RCD kernel (tiles are 32 x 24)
+constexpr int DS_RCD_TILE = 40;  // rows of a tile row of the one-frame RCD kernel (tiles are 64 x 40)
 constexpr int DS_RCD_HALO = 10;  // rows (and columns) of input beyond a tile that RCD reads
 cudaError_t ds_launch_rcd_u16_rows(cudaStream_t st, ds_src_u16 src, int w, int h, ds_pat pat, const float mul[3],
                                    float* out_rgb, float* out_clip, int ty0, int ty1);

@@ -134,19 +134,19 @@ __global__ void superpixel_kernel(const float* __restrict__ cfa, int w, int h, d
 // read c at +-3. So the tile loads a 10-sample halo (local stage regions
 // along x: m [0,52), b* and lpf [3,49), vh/pq [4,48), g [5,47), r43/b43
 // [7,45), output [10,42)).
-// Tile of the one-frame kernel: 32 x 24. Its 74 KB of shared memory let three
-// CTAs share an SM, which measured 14% faster at 24 MP than 32 x 32 tiles (two
-// CTAs, 89 KB each); larger tiles (fewer halo sites, one CTA per SM) were
-// slower still. Every tiling gives the same output bit for bit.
-constexpr int RTX = 32, RTY = DS_RCD_TILE;
+// Tile of the one-frame kernel: 64 x 40. The passes keep five planes live at
+// once (stages 1 and 2 run in two halves, and two passes write in place from
+// registers), so a 64 x 40 tile (84 x 60 sites with its halo, 2.0 computed
+// sites per output pixel against 3.0 for 32 x 24) takes 103 KB and two CTAs
+// share an SM. Every tiling gives the same output bit for bit.
+constexpr int RTX = 64, RTY = DS_RCD_TILE;
 constexpr int RH = 10;  // halo
 constexpr int RCD_THREADS = 256;  // the batch kernels' block (shared with the NLM tile body)
-// The one-frame kernel's block: 512 threads, three CTAs per SM (40 registers
-// each): 5% faster than 256 (more warps to hide shared-memory latency).
+// The one-frame kernel's block: 512 threads, two CTAs per SM.
 constexpr int RCD_THREADS_1F = 512;
-// shared bytes of a TX x TY tile: 8 stage arrays of (TX+20) x (TY+20) floats + the clip bytes
-__host__ __device__ constexpr size_t rcd_smem(int tx, int ty) {
-  return (size_t)8 * (tx + 2 * RH) * (ty + 2 * RH) * sizeof(float) + (size_t)(tx + 2 * RH) * (ty + 2 * RH);
+// shared bytes of a TX x TY tile: npl stage planes of (TX+20) x (TY+20) floats + the clip bytes
+__host__ __device__ constexpr size_t rcd_smem(int tx, int ty, int npl = 5) {
+  return (size_t)npl * (tx + 2 * RH) * (ty + 2 * RH) * sizeof(float) + (size_t)(tx + 2 * RH) * (ty + 2 * RH);
 }
 constexpr size_t RCD_SMEM = rcd_smem(RTX, RTY);
 
@@ -176,24 +176,38 @@ __device__ __forceinline__ float sq(float v) { return v * v; }
 // FULL (implies !RING): the whole staged region lies inside the frame, so no
 // load is clamped and every stage's border rule holds at every site the tile
 // computes; the tile skips those tests.
-template <class Src, int TXT, int TYT, int NT, bool RING, bool FULL = false>
+template <class Src, int TXT, int TYT, int NT, int NPL, bool RING, bool FULL = false>
 __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
                                          float* __restrict__ out_rgb, float* __restrict__ out_clip, int tile_x,
                                          int tile_y, float* smem) {
   static_assert(TXT % 2 == 0 && TYT % 2 == 0, "tile sides must be even");
   constexpr int RSX = TXT + 2 * RH, RSY = TYT + 2 * RH, RA = RSX * RSY;
-  float* M = smem;  // data*mul (clamped-site load): not max(0) in RING tiles, max(0) otherwise
-  float* BV = M + RA;   // bv, later g
-  float* BH = BV + RA;  // bh, later r after 4.3
-  float* BP = BH + RA;  // bp, later b after 4.3
-  float* BQ = BP + RA;
-  float* LP = BQ + RA;
+  // NPL = 5 stage planes, reused as the passes retire them:
+  //   M   data*mul (clamped-site load; max(0) outside RING tiles) ... later b after 4.3
+  //   LP  lpf ................................................... later r after 4.3
+  //   VH  vh
+  //   X   bv, then bp, then pq
+  //   Y   bh, then bq, then g
+  // pq and b replace planes that their own pass still reads, so each thread
+  // holds its sites' values in registers until every thread is done reading.
+  // NPL = 7 (the batch kernels' 256-thread tiles, whose shared memory is
+  // sized by the NLM tile anyway) gives pq and b planes of their own and
+  // writes them directly.
+  static_assert(NPL == 5 || NPL == 7, "five or seven planes");
+  float* M = smem;
+  float* LP = M + RA;
   float* VH = LP + RA;
-  float* PQ = VH + RA;
-  uint8_t* CL = reinterpret_cast<uint8_t*>(PQ + RA);  // [v >= CLIP]
-  float* G = BV;
-  float* R43 = BH;
-  float* B43 = BP;
+  float* X = VH + RA;
+  float* Y = X + RA;
+  uint8_t* CL = reinterpret_cast<uint8_t*>(smem + NPL * RA);  // [v >= CLIP]
+  float* BV = X;
+  float* BH = Y;
+  float* BP = X;
+  float* BQ = Y;
+  float* PQ = NPL == 5 ? X : Y + RA;
+  float* G = Y;
+  float* R43 = LP;
+  float* B43 = NPL == 5 ? M : Y + 2 * RA;
 
   const int tid = threadIdx.x;
   const int gx0 = tile_x * TXT - RH, gy0 = tile_y * TYT - RH;  // global site of local (0,0)
@@ -214,20 +228,22 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
   auto C = [&](int k) { return RING ? fmaxf(M[k], 0.0f) : M[k]; };  // demosaic.rs:154
   const int w1 = RSX, w2 = 2 * RSX, w3 = 3 * RSX, w4 = 4 * RSX;
 
-  // stage 1: bv, bh, bp, bq (:160-172, :251-260) and lpf (:188-201) on [3, edge-3) of the staged region
-  for (int i = tid; i < (RSX - 6) * (RSY - 6); i += NT) {
-    const int ly = 3 + i / (RSX - 6), lx = 3 + i % (RSX - 6);
+  // The passes' regions (local sites): stage 1 [3, edge - 3), stage 2 [4, edge - 4).
+  constexpr int S1X = RSX - 6, S1N = S1X * (RSY - 6);
+  constexpr int S2X = RSX - 8, S2N = S2X * (RSY - 8);
+  auto grad7 = [&](int k, int s1, int s2, int s3, float c6) {  // (:160-172, :251-260) along the step s1
+    return sq((C(k - s3) - C(k - s1) - C(k + s1) + C(k + s3)) - 3.0f * (C(k - s2) + C(k + s2)) + c6);
+  };
+  // stage 1a: bv, bh (:160-172) and lpf (:188-201)
+  for (int i = tid; i < S1N; i += NT) {
+    const int ly = 3 + i / S1X, lx = 3 + i % S1X;
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RSX + lx;
-    float bv = 0.f, bh = 0.f, bp = 0.f, bq = 0.f, lp = 0.f;
+    float bv = 0.f, bh = 0.f, lp = 0.f;
     if (FULL || (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3)) {
-      const float c0 = C(k);
-      bv = sq((C(k - w3) - C(k - w1) - C(k + w1) + C(k + w3)) - 3.0f * (C(k - w2) + C(k + w2)) + 6.0f * c0);
-      bh = sq((C(k - 3) - C(k - 1) - C(k + 1) + C(k + 3)) - 3.0f * (C(k - 2) + C(k + 2)) + 6.0f * c0);
-      bp = sq((C(k - w3 - 3) - C(k - w1 - 1) - C(k + w1 + 1) + C(k + w3 + 3)) - 3.0f * (C(k - w2 - 2) + C(k + w2 + 2)) +
-              6.0f * c0);
-      bq = sq((C(k - w3 + 3) - C(k - w1 + 1) - C(k + w1 - 1) + C(k + w3 - 3)) - 3.0f * (C(k - w2 + 2) + C(k + w2 - 2)) +
-              6.0f * c0);
+      const float c6 = 6.0f * C(k);
+      bv = grad7(k, w1, w2, w3, c6);
+      bh = grad7(k, 1, 2, 3, c6);
     }
     if ((FULL || (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2)) && pat.at(gx, gy) != 1) {
       lp = C(k) + 0.5f * (C(k - w1) + C(k + w1) + C(k - 1) + C(k + 1)) +
@@ -235,28 +251,75 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
     }
     BV[k] = bv;
     BH[k] = bh;
-    BP[k] = bp;
-    BQ[k] = bq;
     LP[k] = lp;
   }
   __syncthreads();
 
-  // stage 2: vh (:173-184) and pq (:261-272) on [4, edge-4)
-  for (int i = tid; i < (RSX - 8) * (RSY - 8); i += NT) {
-    const int ly = 4 + i / (RSX - 8), lx = 4 + i % (RSX - 8);
+  // stage 2a: vh (:173-184) on [4, edge-4)
+  for (int i = tid; i < S2N; i += NT) {
+    const int ly = 4 + i / S2X, lx = 4 + i % S2X;
     const int gx = gx0 + lx, gy = gy0 + ly;
     const int k = ly * RSX + lx;
-    float vh = 0.5f, pq = 0.5f;
+    float vh = 0.5f;
     if (FULL || (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4)) {
       const float vs = fmaxf(BV[k - w1] + BV[k] + BV[k + w1], eps);
       const float hs = fmaxf(BH[k - 1] + BH[k] + BH[k + 1], eps);
       vh = __fdiv_rn(vs, vs + hs);
-      const float ps = fmaxf(BP[k - w1 - 1] + BP[k] + BP[k + w1 + 1], eps);
-      const float qs = fmaxf(BQ[k - w1 + 1] + BQ[k] + BQ[k + w1 - 1], eps);
-      pq = __fdiv_rn(ps, ps + qs);
     }
     VH[k] = vh;
-    PQ[k] = pq;
+  }
+  __syncthreads();
+
+  // stage 1b: bp, bq (:251-260) into the planes bv and bh held
+  for (int i = tid; i < S1N; i += NT) {
+    const int ly = 3 + i / S1X, lx = 3 + i % S1X;
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    const int k = ly * RSX + lx;
+    float bp = 0.f, bq = 0.f;
+    if (FULL || (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3)) {
+      const float c6 = 6.0f * C(k);
+      bp = grad7(k, w1 + 1, w2 + 2, w3 + 3, c6);
+      bq = grad7(k, w1 - 1, w2 - 2, w3 - 3, c6);
+    }
+    BP[k] = bp;
+    BQ[k] = bq;
+  }
+  __syncthreads();
+
+  // stage 2b: pq (:261-272) on [4, edge-4). With five planes it replaces bp
+  // in place, so every thread first forms its sites' values in registers.
+  auto pq_at = [&](int k) {
+    const float ps = fmaxf(BP[k - w1 - 1] + BP[k] + BP[k + w1 + 1], eps);
+    const float qs = fmaxf(BQ[k - w1 + 1] + BQ[k] + BQ[k + w1 - 1], eps);
+    return __fdiv_rn(ps, ps + qs);
+  };
+  if constexpr (NPL == 7) {
+    for (int i = tid; i < S2N; i += NT) {
+      const int ly = 4 + i / S2X, lx = 4 + i % S2X;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      const int k = ly * RSX + lx;
+      PQ[k] = FULL || (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4) ? pq_at(k) : 0.5f;
+    }
+  } else {
+    constexpr int NPQ = (S2N + NT - 1) / NT;
+    float pqv[NPQ];
+#pragma unroll
+    for (int n = 0; n < NPQ; n++) {
+      const int i = tid + n * NT;
+      pqv[n] = 0.5f;
+      if (i < S2N) {
+        const int ly = 4 + i / S2X, lx = 4 + i % S2X;
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        const int k = ly * RSX + lx;
+        if (FULL || (gx >= 4 && gx < W - 4 && gy >= 4 && gy < H - 4)) pqv[n] = pq_at(k);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int n = 0; n < NPQ; n++) {
+      const int i = tid + n * NT;
+      if (i < S2N) PQ[(4 + i / S2X) * RSX + 4 + i % S2X] = pqv[n];
+    }
   }
   __syncthreads();
 
@@ -326,8 +389,19 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
   // read at the diagonal +-1/+-3 sites of an R (B) site holds native B (R)
   // samples, i.e. c. Interior green sites are never read (4.4 reads R/B
   // sites only); ring green sites keep their MHC values.
-  constexpr int S4Y = RSY - 14, S4H = (RSX - 14) / 2;
-  for (int i = tid; i < S4Y * S4H; i += NT) {  // R/B sites
+  // R43 goes to the lpf plane (retired after stage 3) directly; with five
+  // planes B43 replaces the data plane, which this pass still reads, so each
+  // thread keeps its sites' values in registers until every thread is done
+  // reading.
+  constexpr int S4Y = RSY - 14, S4H = (RSX - 14) / 2, S4N = S4Y * S4H;
+  constexpr int NB4 = (S4N + NT - 1) / NT, NBR = NPL == 5 ? NB4 : 1;
+  float b4[NBR], bg4[RING ? NBR : 1];
+  int k4[NBR], kg4[RING ? NBR : 1];
+#pragma unroll
+  for (int n = 0; n < NB4; n++) {  // R/B sites
+    const int i = tid + n * NT;
+    if constexpr (NPL == 5) k4[n] = -1;
+    if (i >= S4N) continue;
     const int ly = 7 + i / S4H, lx = col_start(ly, 7, false) + 2 * (i % S4H);
     if (lx >= RSX - 7) continue;
     const int gx = gx0 + lx, gy = gy0 + ly;
@@ -357,18 +431,42 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
       b = col == 2 ? C(k) : o2;
     }
     R43[k] = r;
-    B43[k] = b;
+    if constexpr (NPL == 5) {
+      b4[n] = b;
+      k4[n] = k;
+    } else {
+      B43[k] = b;
+    }
   }
-  for (int i = tid; i < (RING ? S4Y * S4H : 0); i += NT) {  // green sites of the ring (RING tiles only)
-    const int ly = 7 + i / S4H, lx = col_start(ly, 7, true) + 2 * (i % S4H);
-    if (lx >= RSX - 7) continue;
-    const int gx = gx0 + lx, gy = gy0 + ly;
-    if (inner(gx, gy)) continue;
-    const int k = ly * RSX + lx;
-    float o0, o1, o2;
-    mhc_at(k, gx, gy, o0, o1, o2);
-    R43[k] = o0;
-    B43[k] = o2;
+  if constexpr (RING) {
+#pragma unroll
+    for (int n = 0; n < NB4; n++) {  // green sites of the ring
+      const int i = tid + n * NT;
+      if constexpr (NPL == 5) kg4[n] = -1;
+      if (i >= S4N) continue;
+      const int ly = 7 + i / S4H, lx = col_start(ly, 7, true) + 2 * (i % S4H);
+      if (lx >= RSX - 7) continue;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      if (inner(gx, gy)) continue;
+      const int k = ly * RSX + lx;
+      float o0, o1, o2;
+      mhc_at(k, gx, gy, o0, o1, o2);
+      R43[k] = o0;
+      if constexpr (NPL == 5) {
+        bg4[n] = o2;
+        kg4[n] = k;
+      } else {
+        B43[k] = o2;
+      }
+    }
+  }
+  if constexpr (NPL == 5) {
+    __syncthreads();
+#pragma unroll
+    for (int n = 0; n < NB4; n++) {
+      if (k4[n] >= 0) B43[k4[n]] = b4[n];
+      if (RING && kg4[n] >= 0) B43[kg4[n]] = bg4[n];
+    }
   }
   __syncthreads();
 
@@ -429,7 +527,7 @@ __device__ __forceinline__ void rcd_tile_body(const Src& src, int W, int H, ds_p
 // One TXT x TYT output tile; see rcd_tile_body. A tile needs the ring code
 // when its stage-3 region (the widest one that can fall back to MHC: local
 // sites [5, edge - 5)) reaches the border ring [0, 4) or [W - 4, W).
-template <class Src, int TXT, int TYT, int NT = RCD_THREADS>
+template <class Src, int TXT, int TYT, int NT = RCD_THREADS, int NPL = 7>
 __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pat, float m0, float m1, float m2,
                                          float* __restrict__ out_rgb, float* __restrict__ out_clip, int tile_x,
                                          int tile_y, float* smem) {
@@ -438,28 +536,28 @@ __device__ __forceinline__ void rcd_tile(const Src& src, int W, int H, ds_pat pa
   const bool ring = gx0 + 5 < 4 || gx0 + RSX - 5 > W - 4 || gy0 + 5 < 4 || gy0 + RSY - 5 > H - 4;
   const bool full = gx0 >= 0 && gx0 + RSX <= W && gy0 >= 0 && gy0 + RSY <= H;
   if (full)
-    rcd_tile_body<Src, TXT, TYT, NT, false, true>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
+    rcd_tile_body<Src, TXT, TYT, NT, NPL, false, true>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
   else if (ring)
-    rcd_tile_body<Src, TXT, TYT, NT, true>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
+    rcd_tile_body<Src, TXT, TYT, NT, NPL, true>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
   else
-    rcd_tile_body<Src, TXT, TYT, NT, false>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
+    rcd_tile_body<Src, TXT, TYT, NT, NPL, false>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, tile_x, tile_y, smem);
 }
 
 template <class Src>
-__global__ void __launch_bounds__(RCD_THREADS_1F, 3) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
+__global__ void __launch_bounds__(RCD_THREADS_1F, 2) rcd_tile_kernel(Src src, int W, int H, ds_pat pat, float m0,
                                                                       float m1, float m2, float* __restrict__ out_rgb,
                                                                       float* __restrict__ out_clip, int ty0) {
   extern __shared__ float4 smem4[];
-  rcd_tile<Src, RTX, RTY, RCD_THREADS_1F>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, blockIdx.x,
+  rcd_tile<Src, RTX, RTY, RCD_THREADS_1F, 5>(src, W, H, pat, m0, m1, m2, out_rgb, out_clip, blockIdx.x,
                                           blockIdx.y + ty0, reinterpret_cast<float*>(smem4));
 }
-
-// Tile shapes of the batched kernel (w x h); all of them fit two CTAs per SM.
+// Tile shapes of the batched kernels (w x h).
 constexpr int RCD_SHAPE_W[DS_RCD_SHAPES] = {32, 64, 48, 24, 16};
 constexpr int RCD_SHAPE_H[DS_RCD_SHAPES] = {32, 16, 24, 48, 64};
 constexpr size_t smax(size_t a, size_t b) { return a > b ? a : b; }
-constexpr size_t RCD_BATCH_SMEM =
-    smax(smax(smax(rcd_smem(32, 32), rcd_smem(64, 16)), smax(rcd_smem(48, 24), rcd_smem(24, 48))), rcd_smem(16, 64));
+constexpr size_t RCD_BATCH_SMEM = smax(smax(smax(rcd_smem(32, 32, 7), rcd_smem(64, 16, 7)),
+                                             smax(rcd_smem(48, 24, 7), rcd_smem(24, 48, 7))),
+                                        rcd_smem(16, 64, 7));
 
 // index of the frame owning global tile t: the last f with tile0(f) <= t
 template <class Get>
@@ -473,6 +571,9 @@ __device__ __forceinline__ int find_frame(int n, int t, Get tile0) {
   return lo;
 }
 
+template <int NT>
+__device__ __noinline__ void rcd_batch_tile(const ds_batch_frame& F, int local, float* smem);
+
 // Persistent RCD over the tiles of all frames; each frame uses its own tile shape.
 __global__ void __launch_bounds__(RCD_THREADS, 2) rcd_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
                                                                    int total) {
@@ -481,17 +582,8 @@ __global__ void __launch_bounds__(RCD_THREADS, 2) rcd_batch_kernel(const ds_batc
   for (int t = blockIdx.x; t < total; t += gridDim.x) {
     const int f = find_frame(n, t, [&](int i) { return frames[i].rcd_tile0; });
     const ds_batch_frame& F = frames[f];
-    const int local = t - F.rcd_tile0;
-    const int ty = local / F.rcd_tiles_x, tx = local - ty * F.rcd_tiles_x;
-    const SrcU16 src{F.src};
     __syncthreads();  // the previous tile is done with shared memory
-    switch (F.rcd_shape) {
-      case 0: rcd_tile<SrcU16, 32, 32>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-      case 1: rcd_tile<SrcU16, 64, 16>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-      case 2: rcd_tile<SrcU16, 48, 24>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-      case 3: rcd_tile<SrcU16, 24, 48>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-      default: rcd_tile<SrcU16, 16, 64>(src, F.w, F.h, F.pat, F.mul[0], F.mul[1], F.mul[2], F.rgb, F.clip, tx, ty, smem); break;
-    }
+    rcd_batch_tile<RCD_THREADS>(F, t - F.rcd_tile0, smem);  // the fused kernel's RCD tile
   }
 }
 
@@ -634,7 +726,7 @@ __device__ __forceinline__ unsigned long long batch_clock_ns() {
 // stamps[f] = the device clock. The tile bodies are those of the one-frame
 // kernels, so every frame's output equals the one-frame path's bit for bit.
 template <int P>
-__global__ void __launch_bounds__(nlmk::NLM_THREADS, 1) batch_fused_kernel(const ds_batch_frame* __restrict__ frames,
+__global__ void __launch_bounds__(nlmk::NLM_THREADS, 2) batch_fused_kernel(const ds_batch_frame* __restrict__ frames,
                                                                      int n, const ds_batch_seg* __restrict__ segs,
                                                                      int nseg, int total, int S, int* counters,
                                                                      int max_frames,
