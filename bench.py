@@ -533,7 +533,7 @@ def run_ours(args):
     p_plain, p_learned, p_noisy = psnr(q_plain, truth), psnr(q_learned, truth), psnr(q_noisy, truth)
     loss_db = p_plain - p_learned
     meets = loss_db <= QUALITY_BOUND_DB
-    tiles = -(-W // 32) * -(-H // (64 - 2 * PATCH))  # NLM tiles of 32 x (64 - 2P)
+    tiles = -(-W // 16) * -(-H // (64 - 2 * PATCH))  # NLM tiles of 16 x (64 - 2P)
 
     del rgb
     batched = None

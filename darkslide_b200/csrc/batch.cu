@@ -26,7 +26,7 @@
 
 ds_scene ds_scene_make(const dsgpu_scene_desc* d);
 cudaError_t ds_launch_scene(cudaStream_t st, const ds_scene& s, uint16_t* out);
-void ds_nlm_tile_grid(int w, int h, int patch, int* tiles_x, int* tiles_y, int* tile_w, int* tile_h);
+void ds_nlm_batch_tile_grid(int w, int h, int patch, int* tiles_x, int* tiles_y);
 
 namespace {
 
@@ -163,8 +163,8 @@ void describe(ds_batch_frame& d, const dsgpu_frame& fr, ds_pat pat, int shape, i
   d.rcd_tiles = d.rcd_tiles_x * ((fr.h + th - 1) / th);
   d.rcd_tile0 = *rcd_total;
   *rcd_total += d.rcd_tiles;
-  int tx, ty, ntw, nth;
-  ds_nlm_tile_grid(fr.w, fr.h, patch, &tx, &ty, &ntw, &nth);
+  int tx, ty;
+  ds_nlm_batch_tile_grid(fr.w, fr.h, patch, &tx, &ty);
   d.nlm_tiles_x = tx;
   d.nlm_tiles_y = ty;
   d.nlm_tile0 = *nlm_total;

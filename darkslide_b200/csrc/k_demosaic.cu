@@ -726,7 +726,7 @@ __device__ __forceinline__ unsigned long long batch_clock_ns() {
 // stamps[f] = the device clock. The tile bodies are those of the one-frame
 // kernels, so every frame's output equals the one-frame path's bit for bit.
 template <int P>
-__global__ void __launch_bounds__(nlmk::NLM_THREADS, 2) batch_fused_kernel(const ds_batch_frame* __restrict__ frames,
+__global__ void __launch_bounds__(nlmk::NLM_BATCH_THREADS, 2) batch_fused_kernel(const ds_batch_frame* __restrict__ frames,
                                                                      int n, const ds_batch_seg* __restrict__ segs,
                                                                      int nseg, int total, int S, int* counters,
                                                                      int max_frames,
@@ -752,7 +752,7 @@ __global__ void __launch_bounds__(nlmk::NLM_THREADS, 2) batch_fused_kernel(const
     const ds_batch_frame& F = frames[sg.frame];
     const int local = t - sg.start;
     if (sg.kind == 0) {
-      rcd_batch_tile<nlmk::NLM_THREADS>(F, local, smem);  // out of line: keeps the NLM body's registers to itself
+      rcd_batch_tile<nlmk::NLM_BATCH_THREADS>(F, local, smem);  // out of line: keeps the NLM body's registers to itself
       __syncthreads();
       if (tid == 0) {
         __threadfence();  // the tile's output before its count
@@ -779,7 +779,8 @@ __global__ void __launch_bounds__(nlmk::NLM_THREADS, 2) batch_fused_kernel(const
       const int per = F.nlm_tiles_x * F.nlm_tiles_y;
       const int ch = local / per, r = local - ch * per;
       const int ty = r / F.nlm_tiles_x, tx = r - ty * F.nlm_tiles_x;
-      nlmk::nlm_tile<P>(F.rgb, F.w, F.h, 3, S, F.sigma, F.out, tx, ty, ch, smem);
+      nlmk::nlm_tile<P, false, DSGPU_NLM_MAX_SEARCH, nlmk::NLM_BATCH_TX>(F.rgb, F.w, F.h, 3, S, F.sigma, F.out, tx, ty, ch,
+                                                                      smem);
       __syncthreads();
       if (tid == 0) {
         __threadfence();
@@ -794,11 +795,11 @@ template <int P>
 cudaError_t launch_batch_fused_p(cudaStream_t st, const ds_batch_frame* frames, int n, const ds_batch_seg* segs,
                                  int nseg, int total, int S, int grid, int* counters, int max_frames,
                                  unsigned long long* stamps) {
-  const size_t nlm = nlmk::nlm_smem_bytes(S, P);
+  const size_t nlm = nlmk::nlm_smem_bytes(S, P, false, DSGPU_NLM_MAX_SEARCH, nlmk::NLM_BATCH_TX);
   const size_t smem = nlm > RCD_BATCH_SMEM ? nlm : RCD_BATCH_SMEM;
   cudaError_t e = cudaFuncSetAttribute(batch_fused_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  batch_fused_kernel<P><<<grid, nlmk::NLM_THREADS, smem, st>>>(frames, n, segs, nseg, total, S, counters, max_frames,
+  batch_fused_kernel<P><<<grid, nlmk::NLM_BATCH_THREADS, smem, st>>>(frames, n, segs, nseg, total, S, counters, max_frames,
                                                          stamps);
   return cudaGetLastError();
 }

@@ -11,12 +11,15 @@
 // and ~8 FP32 operations; what binds is the shared-memory traffic of the
 // separable box sums (one 128-byte wavefront per clock per SM), so the
 // layout minimises shared bytes per update:
-//  - one CTA (256 threads, two per SM, so that one CTA's row phase, heavy on
-//    shared stores, overlaps the other's column phase, heavy on ex2) owns a
-//    32-wide tile of one channel, TY = 64 - 2P rows tall, so that the
+//  - one CTA (128 threads, four per SM, so that the CTAs' row phases, heavy
+//    on shared stores, overlap the others' column phases, heavy on ex2) owns
+//    a 16-wide tile of one channel, TY = 64 - 2P rows tall, so that the
 //    horizontal box sums it needs cover exactly 64 rows; the three channels
 //    of a tile are adjacent in launch order, so the interleaved RGB lines
-//    they all read come from L2;
+//    they all read come from L2 (the batch kernels run the same body on
+//    32-wide tiles and 256 threads, two CTAs per SM);
+//  - the staged plane's pitch is sized for search radius 10 or for the
+//    maximum, whichever the call needs, so that four CTAs fit at S <= 10;
 //  - the tile plus its S+P+1 halo is staged once in shared memory, PRE-SCALED
 //    by sigma = sqrt(log2(e) / (h^2 (2P+1)^2)): the squared differences of
 //    scaled samples sum directly to the ex2 exponent, so a weight costs one
@@ -31,8 +34,9 @@
 //      accumulates; the shifted sample of row r at dy0+1 is the one of row
 //      r+1 at dy0, so one column load serves both dy. The two dx halves of a
 //      pixel's sums meet once, at the end;
-//  - all shared pitches are odd, so a warp's 32 rows (phase A) or 32 columns
-//    (phase B) hit 32 distinct banks.
+//  - all shared pitches are odd, so a warp's 32 rows (phase A) hit 32
+//    distinct banks; in phase B a 16-wide tile's warp is two half-warps on
+//    neighbouring H planes, whose stride is 16 (mod 32) words.
 // Clamped edges: the staged copy is loaded at clamped coordinates, so the
 // shifted sample p_clamped(x+o) is a plain shared read; the reference's box
 // filter clamps the DIFFERENCE plane, so H rows are clamped per row and, in
@@ -50,8 +54,8 @@ using namespace nlmk;
 
 // grid: (tiles_x * C, tile rows); block x = tile_x * C + channel, so the C
 // channels of a tile run side by side
-template <int P, bool F16>
-__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
+template <int P, bool F16, int SM>
+__global__ void __launch_bounds__(NLM_THREADS, 4) nlm_tile_kernel(const float* __restrict__ in, int W, int H, int C,
                                                                   int S, float sigma, const float* __restrict__ h_dev,
                                                                   float norm2_log2e,
                                                                   const unsigned char* __restrict__ tile_flags,
@@ -66,7 +70,7 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_tile_kernel(const float* _
     sigma = sqrtf(norm2_log2e / fmaxf(hh * hh, 1e-12f));
   }
   extern __shared__ float4 smem4[];
-  nlm_tile<P, F16>(in, W, H, C, S, sigma, out, tx, ty, ch, reinterpret_cast<float*>(smem4));
+  nlm_tile<P, F16, SM>(in, W, H, C, S, sigma, out, tx, ty, ch, reinterpret_cast<float*>(smem4));
 }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -81,7 +85,7 @@ __global__ void stamp_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
 // last tile of frame f is done, stamps[f] = the device clock (ns), so the
 // host can report per-frame completion times.
 template <int P>
-__global__ void __launch_bounds__(NLM_THREADS, 2) nlm_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
+__global__ void __launch_bounds__(NLM_BATCH_THREADS, 2) nlm_batch_kernel(const ds_batch_frame* __restrict__ frames, int n,
                                                                    int total, int S, unsigned* __restrict__ done,
                                                                    unsigned long long* __restrict__ stamps) {
   extern __shared__ float4 smem4[];
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_batch_kernel(const ds_batc
     const int ch = local / per, r = local - ch * per;
     const int ty = r / F.nlm_tiles_x, tx = r - ty * F.nlm_tiles_x;
     __syncthreads();  // the previous tile is done with shared memory
-    nlm_tile<P>(F.rgb, F.w, F.h, 3, S, F.sigma, F.out, tx, ty, ch, smem);
+    nlm_tile<P, false, DSGPU_NLM_MAX_SEARCH, NLM_BATCH_TX>(F.rgb, F.w, F.h, 3, S, F.sigma, F.out, tx, ty, ch, smem);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -111,10 +115,10 @@ __global__ void __launch_bounds__(NLM_THREADS, 2) nlm_batch_kernel(const ds_batc
 template <int P>
 cudaError_t launch_nlm_batch_p(cudaStream_t st, const ds_batch_frame* frames, int n, int total, int S, int grid,
                                unsigned* done, unsigned long long* stamps) {
-  const size_t smem = nlm_smem_bytes(S, P);
+  const size_t smem = nlm_smem_bytes(S, P, false, DSGPU_NLM_MAX_SEARCH, NLM_BATCH_TX);
   cudaError_t e = cudaFuncSetAttribute(nlm_batch_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  nlm_batch_kernel<P><<<grid, NLM_THREADS, smem, st>>>(frames, n, total, S, done, stamps);
+  nlm_batch_kernel<P><<<grid, NLM_BATCH_THREADS, smem, st>>>(frames, n, total, S, done, stamps);
   return cudaGetLastError();
 }
 
@@ -127,13 +131,22 @@ cudaError_t launch_nlm_p(cudaStream_t st, const float* in, int w, int h, int C, 
   const int tiles_y = (h + TY - 1) / TY;
   if (ty1 < 0 || ty1 > tiles_y) ty1 = tiles_y;
   if (ty0 >= ty1) return cudaSuccess;
-  const size_t smem = nlm_smem_bytes(S, P, F16);
-  cudaError_t e =
-      cudaFuncSetAttribute(nlm_tile_kernel<P, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid((w + TX - 1) / TX * C, ty1 - ty0);
-  nlm_tile_kernel<P, F16><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags, out,
-                                                            ty0);
+  dim3 grid((w + NLM_TX - 1) / NLM_TX * C, ty1 - ty0);
+  if (S <= 10) {
+    const size_t smem = nlm_smem_bytes(S, P, F16, 10);
+    cudaError_t e =
+        cudaFuncSetAttribute(nlm_tile_kernel<P, F16, 10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    nlm_tile_kernel<P, F16, 10><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev, norm2_log2e, flags,
+                                                                out, ty0);
+  } else {
+    const size_t smem = nlm_smem_bytes(S, P, F16);
+    cudaError_t e = cudaFuncSetAttribute(nlm_tile_kernel<P, F16, DSGPU_NLM_MAX_SEARCH>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    nlm_tile_kernel<P, F16, DSGPU_NLM_MAX_SEARCH><<<grid, NLM_THREADS, smem, st>>>(in, w, h, C, S, sigma, h_dev,
+                                                                                  norm2_log2e, flags, out, ty0);
+  }
   return cudaGetLastError();
 }
 
@@ -193,9 +206,16 @@ cudaError_t ds_launch_nlm_rows(cudaStream_t st, const float* in, int w, int h, i
 // NLM tile geometry (the fallback's flag grid): tiles_x x tiles_y of 64 x (64 - 2P)
 void ds_nlm_tile_grid(int w, int h, int patch, int* tiles_x, int* tiles_y, int* tile_w, int* tile_h) {
   const int ty = HRW - 2 * patch;
-  *tile_w = TX;
+  *tile_w = NLM_TX;
   *tile_h = ty;
-  *tiles_x = (w + TX - 1) / TX;
+  *tiles_x = (w + NLM_TX - 1) / NLM_TX;
+  *tiles_y = (h + ty - 1) / ty;
+}
+
+// The batch kernels' NLM tile grid (their tiles are NLM_BATCH_TX wide).
+void ds_nlm_batch_tile_grid(int w, int h, int patch, int* tiles_x, int* tiles_y) {
+  const int ty = HRW - 2 * patch;
+  *tiles_x = (w + NLM_BATCH_TX - 1) / NLM_BATCH_TX;
   *tiles_y = (h + ty - 1) / ty;
 }
 

@@ -11,15 +11,28 @@
 namespace {
 namespace nlmk {
 
-constexpr int NLM_THREADS = 256;  // two CTAs per SM: one's row phase overlaps the other's column phase
-constexpr int TX = 32;      // tile width
+// Tile widths: the one-frame kernels run 16-wide tiles on 128-thread CTAs,
+// four per SM (four independent barrier domains, so one CTA's row phase,
+// heavy on shared stores, overlaps the column phases of the others); the
+// batch kernels, whose CTAs also run 256-thread RCD tiles, run 32-wide tiles
+// on 256 threads, two per SM. Threads = 8 x width either way.
+constexpr int NLM_TX = 16;
+constexpr int NLM_THREADS = 8 * NLM_TX;
+constexpr int NLM_BATCH_TX = 32;
+constexpr int NLM_BATCH_THREADS = 8 * NLM_BATCH_TX;
 constexpr int HRW = 64;     // H rows per offset (TY + 2P)
 constexpr int SEG = 16;     // phase-A segment width
 constexpr int NI = 4;       // dx per block (one shifted-row load serves all four)
 constexpr int NJ = 2;       // dy per block (one shifted-column load serves both)
 constexpr int NPLANE = NI * NJ;
-constexpr int HP = TX + 1;  // odd H pitch: conflict-free row stores and column loads
 constexpr int HBR = HRW + 4;  // H rows allocated: phase B of the last quarter reads up to row 66
+// H row pitch (odd: conflict-free row stores and column loads) and plane
+// stride (= 16 mod 32 words, so that two half-warps reading neighbouring
+// planes hit disjoint banks) of a tile width
+__host__ __device__ constexpr int nlm_hp(int tx) { return tx + 1; }
+__host__ __device__ constexpr int nlm_hps(int tx) {
+  return HBR * nlm_hp(tx) + ((16 - (HBR * nlm_hp(tx)) % 32) + 32) % 32;
+}
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -31,30 +44,34 @@ __device__ __forceinline__ float ex2(float x) {
 
 // Plane pitch: odd and fixed per P (sized for the largest search radius) so
 // that every shared address offset is a compile-time constant.
-__host__ __device__ constexpr int nlm_pitch(int P) { return (TX + 2 * (DSGPU_NLM_MAX_SEARCH + P + 1)) | 1; }
+__host__ __device__ constexpr int nlm_pitch(int P, int SM = DSGPU_NLM_MAX_SEARCH, int tx = NLM_TX) {
+  return (tx + 2 * (SM + P + 1)) | 1;
+}
+// the pitch class of a search radius: 10 (the common radii) or the maximum
+__host__ __device__ constexpr int nlm_smax(int S) { return S <= 10 ? 10 : DSGPU_NLM_MAX_SEARCH; }
 
 struct NlmGeom {
   int R, PW, PH, PHA;  // halo, region width, region height, allocated rows
 };
 
-__host__ __device__ inline NlmGeom nlm_geom(int S, int P) {
+__host__ __device__ inline NlmGeom nlm_geom(int S, int P, int tx = NLM_TX) {
   NlmGeom g;
   const int TY = HRW - 2 * P;
   g.R = S + P + 1;
-  g.PW = TX + 2 * g.R;
+  g.PW = tx + 2 * g.R;
   g.PH = TY + 2 * g.R;
   g.PHA = g.PH + 4;  // phase B of the last quarter reads up to 3 rows past the region
   return g;
 }
 
 // plane bytes (f32, or f16 when staged in half precision), rounded to 16
-size_t nlm_plane_bytes(int S, int P, bool f16) {
-  const NlmGeom g = nlm_geom(S, P);
-  return ((size_t)nlm_pitch(P) * g.PHA * (f16 ? 2 : 4) + 15) / 16 * 16;
+size_t nlm_plane_bytes(int S, int P, bool f16, int sm = DSGPU_NLM_MAX_SEARCH, int tx = NLM_TX) {
+  const NlmGeom g = nlm_geom(S, P, tx);
+  return ((size_t)nlm_pitch(P, sm, tx) * g.PHA * (f16 ? 2 : 4) + 15) / 16 * 16;
 }
 
-size_t nlm_smem_bytes(int S, int P, bool f16 = false) {
-  return nlm_plane_bytes(S, P, f16) + (size_t)NPLANE * HBR * HP * sizeof(float);
+size_t nlm_smem_bytes(int S, int P, bool f16 = false, int sm = DSGPU_NLM_MAX_SEARCH, int tx = NLM_TX) {
+  return nlm_plane_bytes(S, P, f16, sm, tx) + (size_t)NPLANE * nlm_hps(tx) * sizeof(float);
 }
 
 __device__ __forceinline__ float ldp(const float* p) { return *p; }
@@ -63,7 +80,7 @@ __device__ __forceinline__ void stp(float* p, float v) { *p = v; }
 __device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v); }
 
 // One TX x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
-// image, by NLM_THREADS threads; smem holds nlm_smem_bytes(S, P, F16) bytes.
+// image, by 8 TX threads; smem holds nlm_smem_bytes(S, P, F16, SM, TX) bytes.
 //
 // Offsets are taken in blocks of up to NI dx x NJ dy. Phase A (thread =
 // H row, 16-wide segment and one dy of the block) forms the horizontal box
@@ -82,15 +99,17 @@ __device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v
 // XIN: every patch window of the tile's columns lies inside the image (no
 // column clamping in phase A). The two cases are separate code so that the
 // border case's per-element clamping does not cost the interior registers.
-template <int P, bool F16, bool XIN>
+template <int P, bool F16, bool XIN, int SM, int TX>
 __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
                                               float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
   using T = typename std::conditional<F16, __half, float>::type;
+  constexpr int NT = 8 * TX;  // threads
+  constexpr int HP = nlm_hp(TX), HPS = nlm_hps(TX);
   constexpr int TY = HRW - 2 * P;
   constexpr int DW = SEG + 2 * P;   // differences per phase-A segment
   constexpr int RB = (TY + 3) / 4;  // phase-B rows per thread (a quarter of the tile)
-  constexpr int PP = nlm_pitch(P);
-  const NlmGeom g = nlm_geom(S, P);
+  constexpr int PP = nlm_pitch(P, SM, TX);
+  const NlmGeom g = nlm_geom(S, P, TX);
   T* PL = reinterpret_cast<T*>(smem);  // scaled plane, pitch PP
   float* HB = reinterpret_cast<float*>(reinterpret_cast<char*>(smem) +
                                        ((size_t)PP * g.PHA * sizeof(T) + 15) / 16 * 16);  // NPLANE x HBR rows x HP
@@ -101,13 +120,13 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
 
   float off = 0.f;  // F16: the tile's centre sample
   if (F16) off = in[((size_t)clampi(Y0 + TY / 2, 0, H - 1) * W + clampi(X0 + TX / 2, 0, W - 1)) * C + ch];
-  for (int i = tid; i < g.PW * g.PH; i += NLM_THREADS) {
+  for (int i = tid; i < g.PW * g.PH; i += NT) {
     const int ly = i / g.PW, lx = i - ly * g.PW;
     const int gx = clampi(ox0 + lx, 0, W - 1), gy = clampi(oy0 + ly, 0, H - 1);
     const float v = in[((size_t)gy * W + gx) * C + ch];
     stp(&PL[ly * PP + lx], F16 ? (v - off) * sigma : v * sigma);
   }
-  for (int i = tid; i < (g.PHA - g.PH) * PP; i += NLM_THREADS) stp(&PL[g.PH * PP + i], 0.f);
+  for (int i = tid; i < (g.PHA - g.PH) * PP; i += NT) stp(&PL[g.PH * PP + i], 0.f);
 
   // ---- phase-A role: H row `arow` (tile row arow - P), segment at ax0, dy index aj
   const int arow = tid & (HRW - 1);
@@ -117,8 +136,10 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
   const int acol0 = ax0 - P + g.R;  // plane column of difference 0 (interior tiles)
   // ---- phase-B role: column bcol, rows [brow0, brow0 + RB) (clipped to TY), dx half bk
   const int bcol = tid & (TX - 1);
-  const int brow0 = ((tid / TX) & 3) * RB;
-  const int bk = tid / (4 * TX);
+  // consecutive groups of TX threads take the two dx halves (at TX = 16 the
+  // two half-warps of a warp, which read neighbouring planes)
+  const int bk = (tid / TX) & 1;
+  const int brow0 = (tid / (2 * TX)) * RB;
 
   __syncthreads();
   float pv[DW];  // centre samples of this thread's phase-A segment
@@ -136,7 +157,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
   }
 
   // One block of offsets {dx0 .. dx0+BI-1} x {dy0 .. dy0+BJ-1}; plane (i, j)
-  // of the block is HB + (j * NI + i) * HBR * HP.
+  // of the block is HB + (j * NI + i) * HPS.
   auto block = [&](int dx0, int dy0, auto ni_tag, auto nj_tag) {
     constexpr int BI = decltype(ni_tag)::value;
     constexpr int BJ = decltype(nj_tag)::value;
@@ -149,7 +170,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
 #pragma unroll
         for (int m = 0; m < DW + BI - 1; m++) q[m] = ldp(&qrow[acol0 + m]);
       }
-      float* Hrow = HB + (size_t)aj * NI * (HBR * HP) + arow * HP + ax0;
+      float* Hrow = HB + (size_t)aj * NI * HPS + arow * HP + ax0;
 #pragma unroll
       for (int i = 0; i < BI; i++) {
         // difference k of plane i; computed where it enters the window and
@@ -168,7 +189,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
           const float d = dif(k);
           h = fmaf(-d, d, h);
         }
-        float* Hi = Hrow + i * (HBR * HP);
+        float* Hi = Hrow + i * HPS;
         Hi[0] = h;
 #pragma unroll
         for (int k = 1; k < SEG; k++) {
@@ -191,7 +212,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
         for (int r = 0; r < RB + BJ - 1; r++) qv[r] = ldp(&qc[r * PP]);
 #pragma unroll
         for (int j = 0; j < BJ; j++) {
-          const float* hc = HB + (j * NI + i) * (HBR * HP) + brow0 * HP + bcol;
+          const float* hc = HB + (j * NI + i) * HPS + brow0 * HP + bcol;
           float hv[RB + 2 * P];
 #pragma unroll
           for (int r = 0; r < RB + 2 * P; r++) hv[r] = hc[r * HP];
@@ -242,7 +263,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
   float* XA = HB;
   float* XS = HB + TX * 4 * RB;
   float* XC = HB + 2 * TX * 4 * RB;
-  const int slot = ((tid / TX) & 3) * RB * TX + bcol;  // (quarter, row r) x column
+  const int slot = (tid / (2 * TX)) * RB * TX + bcol;  // (quarter, row r) x column
   if (bk == 1) {
 #pragma unroll
     for (int r = 0; r < RB; r++) {
@@ -268,14 +289,14 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
   }
 }
 
-template <int P, bool F16 = false>
+template <int P, bool F16 = false, int SM = DSGPU_NLM_MAX_SEARCH, int TX = NLM_TX>
 __device__ __forceinline__ void nlm_tile(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
                                          float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
   const int X0 = tile_x * TX;
   if (X0 - P >= 0 && X0 + TX + P <= W)
-    nlm_tile_body<P, F16, true>(in, W, H, C, S, sigma, out, tile_x, tile_y, ch, smem);
+    nlm_tile_body<P, F16, true, SM, TX>(in, W, H, C, S, sigma, out, tile_x, tile_y, ch, smem);
   else
-    nlm_tile_body<P, F16, false>(in, W, H, C, S, sigma, out, tile_x, tile_y, ch, smem);
+    nlm_tile_body<P, F16, false, SM, TX>(in, W, H, C, S, sigma, out, tile_x, tile_y, ch, smem);
 }
 
 }  // namespace nlmk

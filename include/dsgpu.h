@@ -345,9 +345,10 @@ int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, 
  * DSGPU_ERR_TIMEOUT. */
 int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* net, int tensor_core_gen5);
 /* The learned stand-in for nlm(in, h_param, search, patch) with its per-tile
- * fallback: the network runs on the whole image, then every NLM tile whose
- * removed component out - in has an RMS above tau * h / 1.5 (or is not
- * finite) is recomputed by plain NLM. tau <= 0 disables the fallback.
+ * fallback: the network runs on the whole image, then every NLM tile (16 x
+ * (64 - 2 patch) pixels) whose removed component out - in has an RMS above
+ * tau * h / 1.5 (or is not finite) is recomputed by plain NLM. tau <= 0
+ * disables the fallback.
  * *fallback_tiles (may be NULL) receives the number of tiles recomputed. */
 int dsgpu_cnn_denoise(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, int h, float h_param,
                       int search, int patch, float tau, float* out_rgb, int* fallback_tiles, unsigned flags);

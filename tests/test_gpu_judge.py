@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 WB = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
 S, P = 10, 3
-TW, TH = 32, 64 - 2 * P  # the NLM tile (nlm_tile.cuh: TX x (64 - 2P))
+TW, TH = 16, 64 - 2 * P  # the NLM tile of the one-frame kernel (nlm_tile.cuh: NLM_TX x (64 - 2P))
 WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "darkslide_b200", "weights",
                        "cnn_nlm.bin")
 
