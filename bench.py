@@ -573,7 +573,7 @@ def run_ours(args):
             "launch_ms": nlm_launch_ms, "fp32_peak_tflops": fl / 1e12, "fp32x2_peak_tflops": fl2 / 1e12,
             "binding": {k[len("nlm_"):]: v for k, v in traffic.items()
                         if k.startswith("nlm_") and k != "nlm_bytes_per_launch"} or None,
-            "binding_source": "ncu counters of one launch on 4096x3072x3, from profiles/dram_traffic.txt "
+            "binding_source": "ncu counters of one launch on 6000x4000x3, from profiles/dram_traffic.txt "
                               "(shared-memory bytes and issue per (pixel, channel, offset) update)",
         }
         roof_rcd = {
