@@ -36,6 +36,27 @@ __host__ __device__ constexpr int nlm_hps(int tx) {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// two floats as a half2 word (lo in the low half), rounded to nearest and
+// saturated to the largest finite half (a box sum past it gives a weight of 0
+// either way, and a finite value keeps the running sums free of inf - inf)
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
+  float2 r;
+  asm("{\n .reg .b64 ra, rb, rr;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " sub.rn.f32x2 rr, ra, rb;\n mov.b64 {%0, %1}, rr;\n}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ unsigned pack_h2(float lo, float hi) {
+  unsigned r;
+  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+__device__ __forceinline__ float2 unpack_h2(unsigned w) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+
 __device__ __forceinline__ float ex2(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -65,19 +86,19 @@ __host__ __device__ inline NlmGeom nlm_geom(int S, int P, int tx = NLM_TX) {
 }
 
 // plane bytes (f32, or f16 when staged in half precision), rounded to 16
-size_t nlm_plane_bytes(int S, int P, bool f16, int sm = DSGPU_NLM_MAX_SEARCH, int tx = NLM_TX) {
+// FP32 plane bytes, rounded to 16
+size_t nlm_plane_bytes(int S, int P, int sm = DSGPU_NLM_MAX_SEARCH, int tx = NLM_TX) {
   const NlmGeom g = nlm_geom(S, P, tx);
-  return ((size_t)nlm_pitch(P, sm, tx) * g.PHA * (f16 ? 2 : 4) + 15) / 16 * 16;
+  return ((size_t)nlm_pitch(P, sm, tx) * g.PHA * 4 + 15) / 16 * 16;
 }
 
+// plane + H planes: NPLANE of FP32, or (f16) NPLANE / 2 of half2 pairs
 size_t nlm_smem_bytes(int S, int P, bool f16 = false, int sm = DSGPU_NLM_MAX_SEARCH, int tx = NLM_TX) {
-  return nlm_plane_bytes(S, P, f16, sm, tx) + (size_t)NPLANE * nlm_hps(tx) * sizeof(float);
+  return nlm_plane_bytes(S, P, sm, tx) + (size_t)(f16 ? NPLANE / 2 : NPLANE) * nlm_hps(tx) * sizeof(float);
 }
 
 __device__ __forceinline__ float ldp(const float* p) { return *p; }
-__device__ __forceinline__ float ldp(const __half* p) { return __half2float(*p); }
 __device__ __forceinline__ void stp(float* p, float v) { *p = v; }
-__device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v); }
 
 // One TX x (64 - 2P) tile (tile_x, tile_y) of channel ch of a W x H x C
 // image, by 8 TX threads; smem holds nlm_smem_bytes(S, P, F16, SM, TX) bytes.
@@ -89,12 +110,11 @@ __device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v
 // dx) sums them vertically, weights and accumulates. A pixel's sums are
 // split between the two dx halves and added once at the end.
 //
-// F16 (the precision variant): the pre-scaled plane is staged in half
-// precision, centred on the tile's centre sample (NLM weights depend only on
-// differences, so the offset costs nothing there and keeps the half-precision
-// error of the staged values small; it is added back to the result), while
-// distances, weights and sums stay in FP32 and the weight sum (the
-// normalisation) is accumulated with Kahan compensation.
+// F16 (the precision variant): the horizontal box sums handed from phase A
+// to phase B, most of the shared-memory traffic, are staged in half
+// precision: planes i and i + 2 of a block share one half2 word, which a
+// phase-B thread (it owns exactly those two planes) reads with one load and
+// sums as one packed pair. Differences, weights and sums stay in FP32.
 //
 // XIN: every patch window of the tile's columns lies inside the image (no
 // column clamping in phase A). The two cases are separate code so that the
@@ -102,7 +122,7 @@ __device__ __forceinline__ void stp(__half* p, float v) { *p = __float2half_rn(v
 template <int P, bool F16, bool XIN, int SM, int TX>
 __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int W, int H, int C, int S, float sigma,
                                               float* __restrict__ out, int tile_x, int tile_y, int ch, float* smem) {
-  using T = typename std::conditional<F16, __half, float>::type;
+  using T = float;  // the staged plane is FP32 in both variants
   constexpr int NT = 8 * TX;  // threads
   constexpr int HP = nlm_hp(TX), HPS = nlm_hps(TX);
   constexpr int TY = HRW - 2 * P;
@@ -118,13 +138,10 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
   const int tid = threadIdx.x;
   const int ox0 = X0 - g.R, oy0 = Y0 - g.R;  // global site of plane (0,0)
 
-  float off = 0.f;  // F16: the tile's centre sample
-  if (F16) off = in[((size_t)clampi(Y0 + TY / 2, 0, H - 1) * W + clampi(X0 + TX / 2, 0, W - 1)) * C + ch];
   for (int i = tid; i < g.PW * g.PH; i += NT) {
     const int ly = i / g.PW, lx = i - ly * g.PW;
     const int gx = clampi(ox0 + lx, 0, W - 1), gy = clampi(oy0 + ly, 0, H - 1);
-    const float v = in[((size_t)gy * W + gx) * C + ch];
-    stp(&PL[ly * PP + lx], F16 ? (v - off) * sigma : v * sigma);
+    stp(&PL[ly * PP + lx], in[((size_t)gy * W + gx) * C + ch] * sigma);
   }
   for (int i = tid; i < (g.PHA - g.PH) * PP; i += NT) stp(&PL[g.PH * PP + i], 0.f);
 
@@ -148,12 +165,11 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
     const int col = XIN ? acol0 + k : clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
     pv[k] = ldp(&PL[aprow * PP + col]);
   }
-  float a[RB], s[RB], cs[F16 ? RB : 1];  // cs: Kahan compensation of s (F16)
+  float a[RB], s[RB];
 #pragma unroll
   for (int r = 0; r < RB; r++) {
     a[r] = 0.f;
     s[r] = 0.f;
-    if (F16) cs[r] = 0.f;
   }
 
   // One block of offsets {dx0 .. dx0+BI-1} x {dy0 .. dy0+BJ-1}; plane (i, j)
@@ -163,6 +179,55 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
     constexpr int BJ = decltype(nj_tag)::value;
     // phase A: horizontal sums, stored NEGATED (-sum d^2) so that phase B's
     // vertical sum is the ex2 argument itself
+    if constexpr (F16) {
+      // planes i0 and i0 + 2 of the block side by side in one half2 slot
+      // (pair plane j * 2 + i0), saturated to the largest finite half
+      if (aj < BJ) {
+        const T* qrow = PL + (aprow + dy0 + aj) * PP + dx0;
+        float q[DW + BI - 1];
+        if constexpr (XIN) {
+#pragma unroll
+          for (int m = 0; m < DW + BI - 1; m++) q[m] = ldp(&qrow[acol0 + m]);
+        }
+        unsigned* Hrow = reinterpret_cast<unsigned*>(HB) + (size_t)aj * 2 * HPS + arow * HP + ax0;
+#pragma unroll
+        for (int i0 = 0; i0 < 2 && i0 < BI; i0++) {
+          const bool two = i0 + 2 < BI;
+          auto dif = [&](int k, int i) {
+            if constexpr (XIN) {
+              return pv[k] - q[k + i];
+            } else {
+              const int col = clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
+              return pv[k] - ldp(&qrow[col + i]);
+            }
+          };
+          float h0 = 0.f, h1 = 0.f;
+#pragma unroll
+          for (int k = 0; k <= 2 * P; k++) {
+            const float d0 = dif(k, i0);
+            h0 = fmaf(-d0, d0, h0);
+            if (two) {
+              const float d1 = dif(k, i0 + 2);
+              h1 = fmaf(-d1, d1, h1);
+            }
+          }
+          unsigned* Hi = Hrow + i0 * HPS;
+          Hi[0] = pack_h2(h0, h1);
+#pragma unroll
+          for (int k = 1; k < SEG; k++) {
+            const float de0 = dif(k + 2 * P, i0), dl0 = dif(k - 1, i0);
+            h0 = fmaf(-de0, de0, h0);
+            h0 = fmaf(dl0, dl0, h0);
+            if (two) {
+              const float de1 = dif(k + 2 * P, i0 + 2), dl1 = dif(k - 1, i0 + 2);
+              h1 = fmaf(-de1, de1, h1);
+              h1 = fmaf(dl1, dl1, h1);
+            }
+            Hi[k] = pack_h2(h0, h1);
+          }
+        }
+      }
+    } else {
     if (aj < BJ) {
       const T* qrow = PL + (aprow + dy0 + aj) * PP + dx0;
       float q[DW + BI - 1];
@@ -200,7 +265,45 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
         }
       }
     }
+    }
     __syncthreads();
+    // phase B: vertical sums, weights, accumulation for dx0 + i (i = bk, bk + 2)
+    if constexpr (F16) {
+      // both of the thread's planes from one half2 slot; their running sums
+      // side by side in one packed pair
+      if (bk < BI) {
+        const bool two = bk + 2 < BI;
+        const T* qc = PL + (brow0 + g.R + dy0) * PP + bcol + g.R + dx0 + bk;
+        float q0[RB + BJ - 1], q1[RB + BJ - 1];
+#pragma unroll
+        for (int r = 0; r < RB + BJ - 1; r++) {
+          q0[r] = ldp(&qc[r * PP]);
+          q1[r] = two ? ldp(&qc[r * PP + 2]) : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < BJ; j++) {
+          const unsigned* hc = reinterpret_cast<const unsigned*>(HB) + (j * 2 + bk) * HPS + brow0 * HP + bcol;
+          unsigned hv[RB + 2 * P];
+#pragma unroll
+          for (int r = 0; r < RB + 2 * P; r++) hv[r] = hc[r * HP];
+          float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int r = 0; r <= 2 * P; r++) v = f2add(v, unpack_h2(hv[r]));
+#pragma unroll
+          for (int r = 0; r < RB; r++) {
+            if (r > 0) v = f2sub(f2add(v, unpack_h2(hv[r + 2 * P])), unpack_h2(hv[r - 1]));
+            const float w0 = ex2(v.x);
+            a[r] = fmaf(w0, q0[r + j], a[r]);
+            s[r] += w0;
+            if (two) {
+              const float w1 = ex2(v.y);
+              a[r] = fmaf(w1, q1[r + j], a[r]);
+              s[r] += w1;
+            }
+          }
+        }
+      }
+    } else {
     // phase B: vertical sums, weights, accumulation for dx0 + i (i = bk, bk + 2)
 #pragma unroll
     for (int ii = 0; ii < 2; ii++) {
@@ -224,17 +327,11 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
             if (r > 0) v = v + hv[r + 2 * P] - hv[r - 1];
             const float wgt = ex2(v);
             a[r] = fmaf(wgt, qv[r + j], a[r]);
-            if (F16) {  // Kahan: s[r] + cs[r] carries the sum of weights
-              const float y = wgt - cs[r];
-              const float t = s[r] + y;
-              cs[r] = (t - s[r]) - y;
-              s[r] = t;
-            } else {
-              s[r] += wgt;
-            }
+            s[r] += wgt;
           }
         }
       }
+    }
     }
     __syncthreads();
   };
@@ -262,14 +359,12 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
   // through shared memory (the H planes are free now), half 0 adds and writes
   float* XA = HB;
   float* XS = HB + TX * 4 * RB;
-  float* XC = HB + 2 * TX * 4 * RB;
   const int slot = (tid / (2 * TX)) * RB * TX + bcol;  // (quarter, row r) x column
   if (bk == 1) {
 #pragma unroll
     for (int r = 0; r < RB; r++) {
       XA[slot + r * TX] = a[r];
       XS[slot + r * TX] = s[r];
-      if (F16) XC[slot + r * TX] = cs[r];
     }
   }
   __syncthreads();
@@ -281,9 +376,9 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
       const int gx = X0 + bcol, gy = Y0 + y;
       if (y < TY && gx < W && gy < H) {
         const float at = a[r] + XA[slot + r * TX];
-        const float st = F16 ? (s[r] - cs[r]) + (XS[slot + r * TX] - XC[slot + r * TX]) : s[r] + XS[slot + r * TX];
+        const float st = s[r] + XS[slot + r * TX];
         const float o = __fdiv_rn(at * inv_sigma, fmaxf(st, 1e-12f));
-        out[((size_t)gy * W + gx) * C + ch] = F16 ? o + off : o;
+        out[((size_t)gy * W + gx) * C + ch] = o;
       }
     }
   }

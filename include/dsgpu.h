@@ -50,11 +50,12 @@ extern "C" {
 /* flags */
 #define DSGPU_HOST 1u  /* buffers are host memory */
 #define DSGPU_ASYNC 2u /* device buffers: do not synchronise before returning */
-/* dsgpu_nlm / dsgpu_develop_u16: the precision variant of NLM. The tile is
- * staged in shared memory in FP16 (centred on the tile's centre sample);
- * patch distances, weights and sums stay in FP32 and the weight sum is
- * accumulated with Kahan compensation. Not bit-equal to the FP32 path; its
- * error against the FP64 oracle is measured by the tests and the profiles. */
+/* dsgpu_nlm / dsgpu_develop_u16: the precision variant of NLM. The
+ * horizontal patch-distance sums that the kernel hands between its two
+ * phases through shared memory are staged in FP16 (rounded to nearest,
+ * saturated to the largest finite half); differences, weights and sums stay
+ * in FP32. Not bit-equal to the FP32 path; its error against the FP64 oracle
+ * is measured by the tests and the profiles. */
 #define DSGPU_FP16_STAGING 4u
 /* dsgpu_develop_u16: reconstruct highlights between RCD and NLM, as
  * Engine::base does (pipeline/mod.rs:186-187): cfa_clip_levels of the

@@ -63,7 +63,8 @@ def test_crop_512_against_fp64(frame, oracle):
     e16 = errors(out16[y0:y0 + 512, x0:x0 + 512], ref)
     print(f"\n45MP BGGR read 12 DN, 512x512 crop vs FP64: fp32 max-abs {e32[0]:.3e} PSNR {e32[1]:.1f} dB; "
           f"fp16-staged max-abs {e16[0]:.3e} PSNR {e16[1]:.1f} dB")
-    assert e32[0] <= 1e-3 and e16[0] <= 3e-3, (e32, e16)
+    # measured: 5.9e-6 for both (PSNR 145 dB)
+    assert e32[0] <= 6e-5 and e16[0] <= 6e-5, (e32, e16)
 
 
 def test_full_frame_against_fp64(frame, oracle):
@@ -72,12 +73,14 @@ def test_full_frame_against_fp64(frame, oracle):
     e32, e16 = errors(out32, ref), errors(out16, ref)
     print(f"\n45MP BGGR read 12 DN, full frame vs FP64: fp32 max-abs {e32[0]:.3e} PSNR {e32[1]:.1f} dB; "
           f"fp16-staged max-abs {e16[0]:.3e} PSNR {e16[1]:.1f} dB")
-    assert e32[0] <= 1e-3 and e16[0] <= 3e-3, (e32, e16)
+    # measured: 1.33e-4 for both (PSNR 142 dB); the maximum sits at RCD sites
+    # where the FP32 demosaic differs from the FP64 one
+    assert e32[0] <= 1e-3 and e16[0] <= 1e-3, (e32, e16)
 
 
 def test_fp16_variant_on_small_frames(oracle):
-    """Ragged sizes and all four layouts: the variant stays within 3e-3 of
-    the FP64 oracle (the FP32 path's bound is 2e-4)."""
+    """Ragged sizes and all four layouts: the variant stays within the FP32
+    path's bound (2e-4) of the FP64 oracle."""
     import torch
 
     if not torch.cuda.is_available():
@@ -89,4 +92,4 @@ def test_fp16_variant_on_small_frames(oracle):
         got = ds.develop_u16(raw, pat, 512, [16383.0] * 3, MUL, hp, SEARCH, PATCH,
                              fp16_staging=True).data.cpu().numpy()
         ref = oracle64(oracle, raw.cpu().numpy(), hp, pat)
-        assert errors(got, ref)[0] <= 3e-3
+        assert errors(got, ref)[0] <= 2e-4
