@@ -286,12 +286,15 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
           unsigned hv[RB + 2 * P];
 #pragma unroll
           for (int r = 0; r < RB + 2 * P; r++) hv[r] = hc[r * HP];
+          float2 hf[RB + 2 * P];  // each pair unpacked once, used where it enters and where it leaves
+#pragma unroll
+          for (int r = 0; r < RB + 2 * P; r++) hf[r] = unpack_h2(hv[r]);
           float2 v = make_float2(0.f, 0.f);
 #pragma unroll
-          for (int r = 0; r <= 2 * P; r++) v = f2add(v, unpack_h2(hv[r]));
+          for (int r = 0; r <= 2 * P; r++) v = f2add(v, hf[r]);
 #pragma unroll
           for (int r = 0; r < RB; r++) {
-            if (r > 0) v = f2sub(f2add(v, unpack_h2(hv[r + 2 * P])), unpack_h2(hv[r - 1]));
+            if (r > 0) v = f2sub(f2add(v, hf[r + 2 * P]), hf[r - 1]);
             const float w0 = ex2(v.x);
             a[r] = fmaf(w0, q0[r + j], a[r]);
             s[r] += w0;
