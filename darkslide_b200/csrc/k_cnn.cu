@@ -16,6 +16,9 @@
 //   weight grad   conv_wgrad_kernel<CIN, COUTW>: M = out channels, N = in
 //                 channels, K = pixels; per-CTA partial sums reduced in a
 //                 fixed order (deterministic)
+// These form the mma.sync training engine, kept as the cross-check of the
+// default tcgen05 engine, whose forward, data-gradient and weight-gradient
+// kernels (conv_tc_kernel, wgrad_tc_kernel) are in k_cnn_tc.cu.
 #include <cuda_bf16.h>
 
 #include <cstring>
@@ -620,12 +623,12 @@ __global__ void judge_decide_kernel(const float* __restrict__ save, float* __res
   }
 }
 
-// Layout conversions of the tensor-core training engine. A batch of B crops
+// Layout conversion of the tensor-core training engine. A batch of B crops
 // of H x W pixels lives in the tensor-core layout as one frame [C/8][Hp][Wp][8]
 // whose crop b occupies rows b * period .. b * period + H - 1 (period = H +
-// the largest dilation; the rows between crops and the padding are zero);
-// the mma.sync weight-gradient kernels read NHWC [B][H][W][C].
-// NHWC -> tensor-core layout (only the crops' pixels are written).
+// the largest dilation; the rows between crops and the padding are zero).
+// NHWC -> tensor-core layout (only the crops' pixels are written): the packed
+// input and the loss gradient, which the NHWC kernels produce.
 template <int C>
 __global__ void nhwc_to_tc_kernel(const bf16* __restrict__ x, int B, int H, int W, int period, int wp, size_t plane,
                                   bf16* __restrict__ y) {
@@ -638,21 +641,6 @@ __global__ void nhwc_to_tc_kernel(const bf16* __restrict__ x, int B, int H, int 
   const int r = (int)(p - (size_t)b * H * W), py = r / W, px = r - py * W;
   const uint4 v = reinterpret_cast<const uint4*>(x)[i];
   reinterpret_cast<uint4*>(y)[(size_t)cb * plane + (size_t)(b * period + py) * wp + px] = v;
-}
-
-// tensor-core layout -> NHWC
-template <int C>
-__global__ void tc_to_nhwc_kernel(const bf16* __restrict__ y, int B, int H, int W, int period, int wp, size_t plane,
-                                  bf16* __restrict__ x) {
-  const size_t n = (size_t)B * H * W * (C / 8);
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int cb = (int)(i % (C / 8));
-  const size_t p = i / (C / 8);
-  const int b = (int)(p / ((size_t)H * W));
-  const int r = (int)(p - (size_t)b * H * W), py = r / W, px = r - py * W;
-  reinterpret_cast<uint4*>(x)[i] =
-      reinterpret_cast<const uint4*>(y)[(size_t)cb * plane + (size_t)(b * period + py) * wp + px];
 }
 
 // ------------------------------------------------------------------ host side
@@ -741,6 +729,8 @@ int ds_cnn_halo_rows() { return cnn_reach(); }
 cudaError_t ds_tc_layer(cudaStream_t st, int kind, int dil, const void* x, int H, int W, const void* wt,
                         const float* bias, void* y, const float* resid, float* yf, const void* mask, int period,
                         int valid, int* err);
+cudaError_t ds_tc_wgrad(cudaStream_t st, int kind, int dil, const void* x, const void* dy, int H, int W,
+                        float* wpart, float* bpart, int max_grid, int* grid, int* err);
 cudaError_t ds_cnn_forward_tc(cudaStream_t st, const void* x16, void* a, void* b, int H, int W,
                               const void* const* wf, const float* const* bias, const int* dil, const float* rgb,
                               float* out, int* err, cudaEvent_t hidden_begin, cudaEvent_t hidden_end);
@@ -939,8 +929,8 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
   if (e != cudaSuccess) return e;
   pack_input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rgb, B, H, W, strength_map, strength,
                                                                   net->act[0]);
-  // the tensor-core engine: forward and data gradients on tcgen05 over the batch frame; the
-  // weight gradients read NHWC copies of its activations and gradients
+  // the tensor-core engine: forward, data and weight gradients on tcgen05 over the batch laid out
+  // as one frame of crops
   const bool tc = net->use_tc;
   const int period = net->t_period, HF = B * period, wp = net->t_wp;
   const size_t tplane = (size_t)wp * ((HF + 11) / 12 * 12);  // pixels of an 8-channel block of the frame
@@ -948,11 +938,6 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
     const size_t m = n * (C / 8);
     if (C == 16) nhwc_to_tc_kernel<16><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(x, B, H, W, period, wp, tplane, y);
     else nhwc_to_tc_kernel<48><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(x, B, H, W, period, wp, tplane, y);
-    return cudaGetLastError();
-  };
-  auto to_nhwc = [&](const bf16* y, bf16* x) {
-    const size_t m = n * 6;
-    tc_to_nhwc_kernel<48><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(y, B, H, W, period, wp, tplane, x);
     return cudaGetLastError();
   };
   if (tc) {
@@ -976,62 +961,72 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
   const int grid = sms * 3;
-  // layer 8: dW from (act7, dy8); dA7 = dgrad(dy8) * [act7 > 0]
-  auto reduce = [&](int l, int coutw, int cinp, int cb) {
+  // a layer's weight and bias gradients from nw / nb partial sums
+  auto reduce = [&](int l, int coutw, int cinp, int cb, int nw, int nb) {
     const LayerSpec L = LAYERS[l];
     const int nreal = 9 * L.cout * L.cin + L.cout;
-    reduce_grads_kernel<<<(nreal + 255) / 256, 256, 0, st>>>(net->wpart, net->wgrid, coutw, cinp, net->bpart,
-                                                            net->bgrid, cb, L.cout, L.cin, net->grads + net->off[l]);
+    reduce_grads_kernel<<<(nreal + 255) / 256, 256, 0, st>>>(net->wpart, nw, coutw, cinp, net->bpart, nb, cb, L.cout,
+                                                            L.cin, net->grads + net->off[l]);
   };
-  if (tc && (e = to_nhwc(net->tact[7], net->act[7])) != cudaSuccess) return e;
-  if ((e = launch_wgrad<48, 16>(st, net->wgrid, LAYERS[7].dil, net->act[7], net->dy8, B, H, W, net->wpart)) !=
-      cudaSuccess)
-    return e;
-  bias_grad_kernel<16><<<net->bgrid, CNN_THREADS, 0, st>>>(net->dy8, n, net->bpart);
-  reduce(7, 16, 48, 16);
-  bf16* g = net->gA;
-  bf16* gnext = net->gB;
-  int tgi = 0;  // tensor-core engine: the data gradient is in net->tg[tgi]
   if (tc) {
+    // per layer, top down: weight and bias gradients of layer l from (tact[l], its output
+    // gradient), then the data gradient below it; every tensor stays in the frame layout
+    int wg = 0;
     if ((e = to_tc(net->dy8, 16, net->tdy8)) != cudaSuccess) return e;
+    if ((e = ds_tc_wgrad(st, 2, LAYERS[7].dil, net->tact[7], net->tdy8, HF, W, net->wpart, net->bpart, net->wgrid,
+                         &wg, net->err)) != cudaSuccess)
+      return e;
+    reduce(7, 16, 48, 16, wg, wg);
     if ((e = ds_tc_layer(st, 3, LAYERS[7].dil, net->tdy8, HF, W, net->wd[7], nullptr, net->tg[0], nullptr, nullptr,
                          net->tact[7], period, H, net->err)) != cudaSuccess)
       return e;
-  } else if ((e = launch_fwd<16, 48, EPI_MASK>(st, grid, LAYERS[7].dil, net->dy8, B, H, W, net->wd[7], nullptr, g,
-                                               net->act[7], nullptr, nullptr)) != cudaSuccess) {
-    return e;
-  }
-  for (int l = 6; l >= 1; l--) {  // layers 7..2 (index l): dW from (act[l], g); g_next = dgrad(g) * [act[l] > 0]
-    if (tc) {
-      if ((e = to_nhwc(net->tg[tgi], g)) != cudaSuccess) return e;
-      if ((e = to_nhwc(net->tact[l], net->act[l])) != cudaSuccess) return e;
-    }
-    if ((e = launch_wgrad<48, 48>(st, net->wgrid, LAYERS[l].dil, net->act[l], g, B, H, W, net->wpart)) !=
-        cudaSuccess)
-      return e;
-    bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
-    reduce(l, 48, 48, 48);
-    if (tc) {
+    int tgi = 0;  // the data gradient is in net->tg[tgi]
+    for (int l = 6; l >= 1; l--) {
+      if ((e = ds_tc_wgrad(st, 1, LAYERS[l].dil, net->tact[l], net->tg[tgi], HF, W, net->wpart, net->bpart,
+                           net->wgrid, &wg, net->err)) != cudaSuccess)
+        return e;
+      reduce(l, 48, 48, 48, wg, wg);
       if ((e = ds_tc_layer(st, 4, LAYERS[l].dil, net->tg[tgi], HF, W, net->wd[l], nullptr, net->tg[tgi ^ 1], nullptr,
                            nullptr, net->tact[l], period, H, net->err)) != cudaSuccess)
         return e;
       tgi ^= 1;
-      continue;
     }
-    if ((e = launch_fwd<48, 48, EPI_MASK>(st, grid, LAYERS[l].dil, g, B, H, W, net->wd[l], nullptr, gnext,
-                                          net->act[l], nullptr, nullptr)) != cudaSuccess)
+    if ((e = ds_tc_wgrad(st, 0, LAYERS[0].dil, net->tact[0], net->tg[tgi], HF, W, net->wpart, net->bpart, net->wgrid,
+                         &wg, net->err)) != cudaSuccess)
       return e;
-    bf16* tmp = g;
-    g = gnext;
-    gnext = tmp;
+    reduce(0, 48, 16, 48, wg, wg);
+  } else {
+    // mma.sync: layer 8: dW from (act7, dy8); dA7 = dgrad(dy8) * [act7 > 0]
+    if ((e = launch_wgrad<48, 16>(st, net->wgrid, LAYERS[7].dil, net->act[7], net->dy8, B, H, W, net->wpart)) !=
+        cudaSuccess)
+      return e;
+    bias_grad_kernel<16><<<net->bgrid, CNN_THREADS, 0, st>>>(net->dy8, n, net->bpart);
+    reduce(7, 16, 48, 16, net->wgrid, net->bgrid);
+    bf16* g = net->gA;
+    bf16* gnext = net->gB;
+    if ((e = launch_fwd<16, 48, EPI_MASK>(st, grid, LAYERS[7].dil, net->dy8, B, H, W, net->wd[7], nullptr, g,
+                                          net->act[7], nullptr, nullptr)) != cudaSuccess)
+      return e;
+    for (int l = 6; l >= 1; l--) {  // layers 7..2 (index l): dW from (act[l], g); g_next = dgrad(g) * [act[l] > 0]
+      if ((e = launch_wgrad<48, 48>(st, net->wgrid, LAYERS[l].dil, net->act[l], g, B, H, W, net->wpart)) !=
+          cudaSuccess)
+        return e;
+      bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
+      reduce(l, 48, 48, 48, net->wgrid, net->bgrid);
+      if ((e = launch_fwd<48, 48, EPI_MASK>(st, grid, LAYERS[l].dil, g, B, H, W, net->wd[l], nullptr, gnext,
+                                            net->act[l], nullptr, nullptr)) != cudaSuccess)
+        return e;
+      bf16* tmp = g;
+      g = gnext;
+      gnext = tmp;
+    }
+    // layer 1: dW from (packed input, g)
+    if ((e = launch_wgrad<16, 48>(st, net->wgrid, LAYERS[0].dil, net->act[0], g, B, H, W, net->wpart)) !=
+        cudaSuccess)
+      return e;
+    bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
+    reduce(0, 48, 16, 48, net->wgrid, net->bgrid);
   }
-  if (tc && (e = to_nhwc(net->tg[tgi], g)) != cudaSuccess) return e;
-  // layer 1: dW from (packed input, g)
-  if ((e = launch_wgrad<16, 48>(st, net->wgrid, LAYERS[0].dil, net->act[0], g, B, H, W, net->wpart)) !=
-      cudaSuccess)
-    return e;
-  bias_grad_kernel<48><<<net->bgrid, CNN_THREADS, 0, st>>>(g, n, net->bpart);
-  reduce(0, 48, 16, 48);
   if (loss_sum_host) {
     float part[512];
     if ((e = cudaMemcpyAsync(part, net->lpart, lgrid * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess)

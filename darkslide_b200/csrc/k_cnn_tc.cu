@@ -493,6 +493,220 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
 }
 
+// ------------------------------------------------------------ weight gradients
+// Weight and bias gradients of one layer of a training batch (the frame of
+// crops of the forward and data-gradient kernels). For tap (ky, kx) at
+// dilation D, substituting q = p + (ky - 1) D rows,
+//   dW[ky][kx][co][ci] = sum_p dY[p][co] X[p + ((ky - 1) D, (kx - 1) D)][ci]
+//                      = sum_q dY[q - (ky - 1) D rows][co] X[q + (kx - 1) D px][ci],
+// so the row shift rides on dY and the column shift on X. A chunk of TK
+// pixels of frame row q is staged as three row-shifted copies of dY (rows
+// q + D, q, q - D: the A operand, M = (ky, co)) and three column-shifted
+// copies of X (the B operand, N = (kx, ci)), each [8-channel block][pixel][8]
+// as the TMA box lands, which is the canonical no-swizzle MN-major layout
+// (core matrices of 8 pixels x 8 channels, 128 contiguous bytes; the next 8
+// pixels 128 bytes on, the next channel block one block on). One MMA per
+// (16-pixel K step, 128 rows of A) covers all nine taps at once. A 48 -> 48
+// layer has 144 rows of A: a second M = 128 MMA starts 16 rows before their
+// end, and of its rows only the last 16 are read out. Sixteen more columns of
+// B, a block of ones and a block of zeros, give the bias gradient
+// sum_q dY[q][co] in the ky = 1 rows. Rows outside the frame and pixels past
+// a row's ends read as zero (TMA fill), and the frame's rows between crops and
+// its padding columns are zero, so every chunk is summed whole, unmasked.
+// A CTA accumulates its contiguous range of chunks in TMEM (FP32) and writes
+// one partial sum per weight; the host adds the CTAs' partials in a fixed
+// order, so the result is deterministic.
+template <int CIN, int COUTW>
+struct WgShape {
+  static constexpr int TK = 64;                   // pixels per chunk
+  static constexpr int STAGES = 4;
+  static constexpr int GB = TK * 16;              // bytes of one 8-channel block of a chunk
+  static constexpr int CBI = CIN / 8, CBO = COUTW / 8;
+  static constexpr int NGA = 3 * CBO;             // A blocks (ky, co block)
+  static constexpr int NM = (NGA + 15) / 16;      // M = 128 MMAs per K step
+  static constexpr int AG = NGA < 16 ? 16 : NGA;  // A blocks an MMA may address
+  static constexpr int NGB = 3 * CBI + 2;         // B blocks (kx, ci block), then ones and zeros
+  static constexpr int N = NGB * 8;
+  static constexpr int STAGE = (AG + NGB) * GB;
+  static constexpr int TMEM_COLS = NM * N <= 256 ? 256 : 512;
+  static constexpr unsigned TX = (unsigned)(3 * CBO + 3 * CBI) * GB;  // bytes the loads of a chunk bring
+  static_assert(N % 16 == 0 && N <= 256 && NM * N <= 512, "MMA and TMEM shapes");
+  static_assert(GB % 128 == 0, "TMA destinations stay 128-byte aligned");
+  // first A block of MMA m: 16 m, the last one ending at the last real block
+  static __host__ __device__ constexpr int a_first(int m) { return NGA <= 16 ? 0 : (16 * m < NGA - 16 ? 16 * m : NGA - 16); }
+};
+constexpr int WG_THREADS = 192;  // warps 0-3 read TMEM out, warp 4 issues the MMAs, warp 5 loads
+
+// TMA load of one 4-D box (channel, pixel, row, 8-channel block) at pixel x,
+// row y, channel 0, block 0
+__device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(x), "r"(y), "r"(0), "r"(bar)
+      : "memory");
+}
+
+// tcgen05.mma with the accumulate flag taken at run time
+__device__ __forceinline__ void mma_bf16_pred(unsigned tmem_d, unsigned long long a, unsigned long long b,
+                                              unsigned idesc, int acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+// x: [CIN/8][Hp][Wp][8] through xmap, dy: [COUTW/8][Hp][Wp][8] through dmap
+// (boxes of 8 channels x TK pixels x 1 row x every block); H: frame rows;
+// wpart: [grid][9][COUTW][CIN], bpart: [grid][COUTW] (one partial sum per CTA).
+template <int CIN, int COUTW>
+__global__ void __launch_bounds__(WG_THREADS, 1)
+    wgrad_tc_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dmap, int H,
+                    int Wp, int dil, float* __restrict__ wpart, float* __restrict__ bpart, int* __restrict__ err) {
+  typedef WgShape<CIN, COUTW> S;
+  extern __shared__ __align__(128) unsigned char sm[];
+  // bars: full[STAGES], empty[STAGES], done, drain
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + (size_t)S::STAGES * S::STAGE);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * S::STAGES + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot) + 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned bar0 = smem_u32(bars);
+  auto full = [&](int s) { return bar0 + 8u * s; };
+  auto empty = [&](int s) { return bar0 + 8u * (S::STAGES + s); };
+  const unsigned done = bar0 + 8u * (2 * S::STAGES), drain = done + 8u;
+  auto a_of = [&](int s) { return sm + (size_t)s * S::STAGE; };
+  auto b_of = [&](int s) { return sm + (size_t)s * S::STAGE + (size_t)S::AG * S::GB; };
+
+  // the blocks no load writes: A blocks past the real ones (zero), B's ones and zeros
+  for (int s = 0; s < S::STAGES; s++) {
+    uint4* az = reinterpret_cast<uint4*>(a_of(s) + (size_t)S::NGA * S::GB);
+    for (int i = tid; i < (S::AG - S::NGA) * S::GB / 16; i += WG_THREADS) az[i] = make_uint4(0u, 0u, 0u, 0u);
+    uint4* bo = reinterpret_cast<uint4*>(b_of(s) + (size_t)3 * S::CBI * S::GB);
+    const unsigned one2 = 0x3F803F80u;  // two BF16 ones
+    for (int i = tid; i < 2 * S::GB / 16; i += WG_THREADS)
+      bo[i] = i < S::GB / 16 ? make_uint4(one2, one2, one2, one2) : make_uint4(0u, 0u, 0u, 0u);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(S::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S::STAGES; s++) {
+      mbar_init(full(s), 1);
+      mbar_init(empty(s), 1);
+    }
+    mbar_init(done, 1);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // ones and zeros -> async proxy
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = *tmem_slot;
+
+  // this CTA's chunks: a contiguous range of (row, TK-pixel run) in row-major order
+  const int cpr = (Wp + S::TK - 1) / S::TK;
+  const long long total = (long long)H * cpr;
+  const int c0 = (int)(total * blockIdx.x / gridDim.x);
+  const int nch = (int)(total * (blockIdx.x + 1) / gridDim.x) - c0;
+
+  if (warp == 5) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&xmap)) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&dmap)) : "memory");
+      int c = 0;
+      for (; c < nch; c++) {
+        const int s = c % S::STAGES;
+        if (!mbar_wait(empty(s), ((c / S::STAGES) & 1) ^ 1, abort_flag)) break;
+        mbar_expect_tx(full(s), S::TX);
+        const int g = c0 + c, q = g / cpr, x0 = (g - q * cpr) * S::TK;
+        const unsigned a = smem_u32(a_of(s)), b = smem_u32(b_of(s));
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          tma_load_4d(a + (unsigned)(k * S::CBO * S::GB), &dmap, x0, q - (k - 1) * dil, full(s));  // ky = k
+          tma_load_4d(b + (unsigned)(k * S::CBI * S::GB), &xmap, x0 + (k - 1) * dil, q, full(s));  // kx = k
+        }
+      }
+      // loads issued but maybe never consumed (abort only): wait for them to land
+      for (int h = c - S::STAGES < 0 ? 0 : c - S::STAGES; h < c; h++)
+        mbar_drain(full(h % S::STAGES), (h / S::STAGES) & 1);
+    }
+  } else if (warp == 4) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      const unsigned idesc = umma_idesc(TC_M, S::N) | (1u << 15) | (1u << 16);  // A and B MN-major
+      int c = 0;
+      bool ok = true;
+      for (; c < nch; c++) {
+        const int s = c % S::STAGES;
+        if (!(ok = mbar_wait(full(s), (c / S::STAGES) & 1, abort_flag))) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned a = smem_u32(a_of(s)), b = smem_u32(b_of(s));
+#pragma unroll
+        for (int k = 0; k < S::TK / 16; k++) {  // 16 pixels = 256 bytes of every block
+          const unsigned long long bd = umma_desc(b + (unsigned)(k * 256), 128, S::GB);
+#pragma unroll
+          for (int m = 0; m < S::NM; m++) {
+            const unsigned long long ad = umma_desc(a + (unsigned)(S::a_first(m) * S::GB + k * 256), 128, S::GB);
+            mma_bf16_pred(tmem + (unsigned)(m * S::N), ad, bd, idesc, c > 0 || k > 0);
+          }
+        }
+        mma_commit(empty(s));  // stage s free once these MMAs have read it
+      }
+      if (ok && nch > 0) mma_commit(done);
+      if (c > 0) {  // MMAs still in flight (after an abort): one commit covers them all
+        mma_commit(drain);
+        const unsigned long long t0 = globaltimer_ns();
+        while (!mbar_test(drain, 0) && globaltimer_ns() - t0 < TC_WAIT_NS) {
+        }
+      }
+    }
+  } else {
+    // ---------------- read-out: warp w owns TMEM lanes 32 w .. 32 w + 31 (rows of A)
+    bool ok = true;
+    if (lane == 0 && nch > 0) ok = mbar_wait(done, 0, abort_flag);
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    if (ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int L = warp * 32 + lane;
+      float* wp = wpart + (size_t)blockIdx.x * 9 * COUTW * CIN;
+#pragma unroll
+      for (int m = 0; m < S::NM; m++) {
+        const int R = 8 * S::a_first(m) + L;  // row of A: (ky, co)
+        const bool live = R >= 128 * m && R < 8 * S::NGA;
+        const int ky = R / COUTW, co = R - ky * COUTW;
+#pragma unroll 1
+        for (int c16 = 0; c16 < S::N; c16 += 16) {
+          unsigned u[16];
+          tmem_ld16_async(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(m * S::N + c16), u);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (!live) continue;
+          float f[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++) f[j] = nch > 0 ? __uint_as_float(u[j]) : 0.f;
+          if (c16 < 3 * CIN) {
+            const int kx = c16 / CIN, ci0 = c16 - kx * CIN;
+            float4* dst = reinterpret_cast<float4*>(wp + ((size_t)(ky * 3 + kx) * COUTW + co) * CIN + ci0);
+#pragma unroll
+            for (int j = 0; j < 4; j++) dst[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+          } else if (c16 == 3 * CIN && ky == 1) {
+            bpart[(size_t)blockIdx.x * COUTW + co] = f[0];
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && *abort_flag) atomicExch(err, DSGPU_ERR_TIMEOUT);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS));
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -557,7 +771,64 @@ cudaError_t launch_tc(cudaStream_t st, int dil, const bf16* x, int H, int W, con
   }
 }
 
+template <int CIN, int COUTW>
+cudaError_t launch_wgrad_tc(cudaStream_t st, int dil, const bf16* x, const bf16* dy, int H, int W, float* wpart,
+                            float* bpart, int max_grid, int* grid_out, int* err) {
+  typedef WgShape<CIN, COUTW> S;
+  constexpr size_t smem = (size_t)S::STAGES * S::STAGE + (2 * S::STAGES + 2) * 8 + 16;
+  static_assert(smem <= 227 * 1024, "shared memory");
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return cudaErrorNotSupported;
+  if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(dy)) & 15) != 0 || H < 1 || W < 1 || dil < 1 ||
+      max_grid < 1)
+    return cudaErrorInvalidValue;
+  const int Wp = (W + TC_PG - 1) / TC_PG * TC_PG, Hp = (H + 11) / 12 * 12;
+  auto make = [&](CUtensorMap* m, const bf16* p, int blocks) {
+    const cuuint64_t dims[4] = {8, (cuuint64_t)Wp, (cuuint64_t)Hp, (cuuint64_t)blocks};
+    const cuuint64_t strides[3] = {16, (cuuint64_t)Wp * 16, (cuuint64_t)Wp * Hp * 16};
+    const cuuint32_t box[4] = {8, (cuuint32_t)S::TK, 1, (cuuint32_t)blocks};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(p), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  CUtensorMap xmap, dmap;
+  if (!make(&xmap, x, S::CBI) || !make(&dmap, dy, S::CBO)) return cudaErrorInvalidValue;
+  cudaError_t e =
+      cudaFuncSetAttribute(wgrad_tc_kernel<CIN, COUTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long chunks = (long long)H * ((Wp + S::TK - 1) / S::TK);
+  int grid = sms < max_grid ? sms : max_grid;
+  if (chunks < grid) grid = (int)chunks;
+  wgrad_tc_kernel<CIN, COUTW><<<grid, WG_THREADS, smem, st>>>(xmap, dmap, H, Wp, dil, wpart, bpart, err);
+  *grid_out = grid;
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+// Weight and bias gradients of one layer of a training batch on the tensor
+// cores, as per-CTA partial sums (see wgrad_tc_kernel). kind: 0 the input
+// layer (16 input, 48 output channels), 1 a hidden layer (48, 48), 2 the
+// output layer (48 input channels, a 16-channel gradient). x: the layer's
+// input, dy: the gradient at its output (ReLU mask applied), both in the
+// tensor-core layout of an H-row frame W pixels wide; wpart[grid][9][cout][cin]
+// and bpart[grid][cout] receive the partials of the *grid CTAs used (at most
+// max_grid).
+cudaError_t ds_tc_wgrad(cudaStream_t st, int kind, int dil, const void* x, const void* dy, int H, int W,
+                        float* wpart, float* bpart, int max_grid, int* grid, int* err) {
+  const bf16* xi = static_cast<const bf16*>(x);
+  const bf16* di = static_cast<const bf16*>(dy);
+  switch (kind) {
+    case 0: return launch_wgrad_tc<16, 48>(st, dil, xi, di, H, W, wpart, bpart, max_grid, grid, err);
+    case 1: return launch_wgrad_tc<48, 48>(st, dil, xi, di, H, W, wpart, bpart, max_grid, grid, err);
+    case 2: return launch_wgrad_tc<48, 16>(st, dil, xi, di, H, W, wpart, bpart, max_grid, grid, err);
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 // One conv layer of a training batch on the tensor cores (the batch is a frame
 // of crops `valid` rows tall stacked `period` rows apart; see conv_tc_kernel).

@@ -53,12 +53,13 @@ def test_forward_matches_fp64(torch_dev):
 
 
 @pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
-@pytest.mark.parametrize("crop", [16, 20])
+@pytest.mark.parametrize("crop", [16, 18, 20])
 def test_gradients_match_fp64(torch_dev, crop, engine):
     """Per-layer weight and bias gradients of a batch against the FP64
-    reference, on either engine: tcgen05 (forward and data gradients on the
-    5th-generation tensor cores over the batch laid out as one frame of
-    crops, weight gradients on mma.sync) or mma.sync throughout."""
+    reference, on either engine: tcgen05 (forward, data and weight gradients
+    on the 5th-generation tensor cores over the batch laid out as one frame
+    of crops; crop 18 leaves two zero padding columns per frame row) or
+    mma.sync throughout."""
     import cnn_ref as C
     from darkslide_b200 import cnn
 
