@@ -165,11 +165,14 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
     const int col = XIN ? acol0 + k : clampi(X0 + ax0 - P + k, 0, W - 1) - ox0;
     pv[k] = ldp(&PL[aprow * PP + col]);
   }
-  float a[RB], s[RB];
+  // weighted sums, and weight sums as two halves added at the end (FP32:
+  // packed pairs over the two dy planes of a block; FP16: the first half only)
+  float a[RB];
+  float2 s2[RB];
 #pragma unroll
   for (int r = 0; r < RB; r++) {
     a[r] = 0.f;
-    s[r] = 0.f;
+    s2[r] = make_float2(0.f, 0.f);
   }
 
   // One block of offsets {dx0 .. dx0+BI-1} x {dy0 .. dy0+BJ-1}; plane (i, j)
@@ -297,11 +300,11 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
             if (r > 0) v = f2sub(f2add(v, hf[r + 2 * P]), hf[r - 1]);
             const float w0 = ex2(v.x);
             a[r] = fmaf(w0, q0[r + j], a[r]);
-            s[r] += w0;
+            s2[r].x += w0;  // one scalar sum here: a second half costs registers this variant lacks
             if (two) {
               const float w1 = ex2(v.y);
               a[r] = fmaf(w1, q1[r + j], a[r]);
-              s[r] += w1;
+              s2[r].x += w1;
             }
           }
         }
@@ -316,9 +319,27 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
         float qv[RB + BJ - 1];
 #pragma unroll
         for (int r = 0; r < RB + BJ - 1; r++) qv[r] = ldp(&qc[r * PP]);
+        if constexpr (BJ == 2) {
+          // both dy of the block at once: their vertical sums and weight sums
+          // run as packed pairs (the same sums, half the instructions)
+          const float* hc0 = HB + i * HPS + brow0 * HP + bcol;
+          const float* hc1 = hc0 + NI * HPS;
+          float2 hv[RB + 2 * P];
 #pragma unroll
-        for (int j = 0; j < BJ; j++) {
-          const float* hc = HB + (j * NI + i) * HPS + brow0 * HP + bcol;
+          for (int r = 0; r < RB + 2 * P; r++) hv[r] = make_float2(hc0[r * HP], hc1[r * HP]);
+          float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int r = 0; r <= 2 * P; r++) v = f2add(v, hv[r]);
+#pragma unroll
+          for (int r = 0; r < RB; r++) {
+            if (r > 0) v = f2sub(f2add(v, hv[r + 2 * P]), hv[r - 1]);
+            const float w0 = ex2(v.x), w1 = ex2(v.y);
+            a[r] = fmaf(w0, qv[r], a[r]);
+            a[r] = fmaf(w1, qv[r + 1], a[r]);
+            s2[r] = f2add(s2[r], make_float2(w0, w1));
+          }
+        } else {
+          const float* hc = HB + i * HPS + brow0 * HP + bcol;
           float hv[RB + 2 * P];
 #pragma unroll
           for (int r = 0; r < RB + 2 * P; r++) hv[r] = hc[r * HP];
@@ -329,8 +350,8 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
           for (int r = 0; r < RB; r++) {
             if (r > 0) v = v + hv[r + 2 * P] - hv[r - 1];
             const float wgt = ex2(v);
-            a[r] = fmaf(wgt, qv[r + j], a[r]);
-            s[r] += wgt;
+            a[r] = fmaf(wgt, qv[r], a[r]);
+            s2[r].x += wgt;
           }
         }
       }
@@ -367,7 +388,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
 #pragma unroll
     for (int r = 0; r < RB; r++) {
       XA[slot + r * TX] = a[r];
-      XS[slot + r * TX] = s[r];
+      XS[slot + r * TX] = s2[r].x + s2[r].y;
     }
   }
   __syncthreads();
@@ -379,7 +400,7 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
       const int gx = X0 + bcol, gy = Y0 + y;
       if (y < TY && gx < W && gy < H) {
         const float at = a[r] + XA[slot + r * TX];
-        const float st = s[r] + XS[slot + r * TX];
+        const float st = (s2[r].x + s2[r].y) + XS[slot + r * TX];
         const float o = __fdiv_rn(at * inv_sigma, fmaxf(st, 1e-12f));
         out[((size_t)gy * W + gx) * C + ch] = o;
       }
