@@ -665,7 +665,7 @@ def run_ours(args):
     return 0
 
 
-CASES = ("nlm", "rcd", "develop", "denoise", "cnn", "learned", "batch")
+CASES = ("nlm", "rcd", "develop", "denoise", "cnn", "learned", "batch", "train")
 
 
 def run_case(args):
@@ -680,7 +680,11 @@ def run_case(args):
       denoise  dsgpu_denoise (enhance::denoise), amount 50
       cnn      dsgpu_cnn_infer, the 8 conv layers
       learned  dsgpu_develop_u16_cnn with the committed weights, tau 3
-      batch    dsgpu_rcd_nlm_batch of --frames equal frames, the 4 CFA layouts"""
+      batch    dsgpu_rcd_nlm_batch of --frames equal frames, the 4 CFA layouts
+      train    one training step of the learned path's network (forward,
+               loss, data, weight and bias gradients, Adam) on a batch of 32
+               crops of 128 x 128 of the demosaiced frame, target the plain
+               NLM of the frame; tcgen05 engine (--mma-sync: the other one)"""
     import ctypes
 
     import torch
@@ -722,13 +726,29 @@ def run_case(args):
                                     torch.empty((h, w, 3), dtype=torch.float32, device=dev))
                       for k in range(args.frames)]
         st.synchronize()
-    if args.case in ("nlm", "denoise", "cnn"):  # these stages take the demosaiced frame
+    if args.case in ("nlm", "denoise", "cnn", "train"):  # these stages take the demosaiced frame
         ctx.check(L.dsgpu_demosaic(ctx.handle, vp(cfa.data_ptr()), w, h, vp(pat.ctypes.data), vp(WB.ctypes.data),
                                    _lib.DSGPU_QUALITY_FULL, vp(rgb.data_ptr()), vp(0), 0), "dsgpu_demosaic")
     A = _lib.DSGPU_ASYNC
+    if args.case == "train":
+        B, crop = 32, 128
+        ctx.check(L.dsgpu_nlm(ctx.handle, vp(rgb.data_ptr()), w, h, 3, float(hp), SEARCH, PATCH, vp(out.data_ptr()),
+                              0), "dsgpu_nlm")
+        pos = np.random.default_rng(5).integers(0, [h - crop + 1, w - crop + 1], (B, 2))
+        with torch.cuda.stream(st):
+            xb = torch.stack([rgb[y:y + crop, x:x + crop] for y, x in pos]).contiguous()
+            tb = torch.stack([out[y:y + crop, x:x + crop] for y, x in pos]).contiguous()
+        st.synchronize()
+        net = cnn.ResidualCNN(ctx, max_batch=B, crop=crop, seed=1)
+        net.set_engine(not args.mma_sync)
+        w, h = crop, crop * B  # Mpix/s below: training pixels per step
 
     def call():
         c = args.case
+        if c == "train":
+            with torch.cuda.stream(st):
+                net.train_step(xb, float(hp), tb, 1e-4, want_loss=False)
+            return
         if c == "batch":
             with torch.cuda.stream(st):
                 ds.develop_batch(frames, args.search, args.patch, ctx=ctx, sync=False)
@@ -764,7 +784,9 @@ def run_case(args):
     ms = e0.elapsed_time(e1) / args.reps
     px = w * h * (args.frames if args.case == "batch" else 1)
     print(json.dumps({"case": args.case, "w": w, "h": h, "ms_per_call": ms, "mpix_per_s": px / ms / 1e3,
-                      "reps": args.reps, "fp16_staging": bool(args.fp16)}), flush=True)
+                      "reps": args.reps, "fp16_staging": bool(args.fp16),
+                      **({"engine": "mma.sync" if args.mma_sync else "tcgen05"} if args.case == "train" else {})}),
+          flush=True)
     return 0
 
 
@@ -784,6 +806,7 @@ def main():
     ap.add_argument("--search", type=int, default=SEARCH, help="--case: NLM search radius")
     ap.add_argument("--patch", type=int, default=PATCH, help="--case: NLM patch radius")
     ap.add_argument("--fp16", action="store_true", help="--case nlm/develop: the FP16-staging variant")
+    ap.add_argument("--mma-sync", action="store_true", help="--case train: the mma.sync training engine")
     args = ap.parse_args()
     if args.case:
         return run_case(args)

@@ -233,7 +233,8 @@ class ResidualCNN:
 
     def set_engine(self, tensor_core_gen5: bool) -> None:
         """Inference and training on tcgen05 (default; training runs its
-        forward and data gradients there) or on the mma.sync kernels."""
+        forward pass, data, weight and bias gradients there) or on the
+        mma.sync kernels."""
         self.ctx.check(lib().dsgpu_cnn_set_engine(self.ctx.handle, self.handle, int(bool(tensor_core_gen5))),
                        "dsgpu_cnn_set_engine")
 

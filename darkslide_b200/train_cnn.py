@@ -97,8 +97,8 @@ def psnr(a, b, peak=1.0):
 def train(crops=200000, batch=32, crop=128, lr=5e-4, frame=512, crops_per_frame=64, mix=8, warmup=500,
           clip_factor=3.0, seed=0, out=None, resume=None, log_every=200, verbose=True, dataset=200000,
           relative=False, scenes="any", engine="tcgen05"):
-    """engine: "tcgen05" (forward and data gradients on the 5th-generation
-    tensor cores, weight gradients on mma.sync) or "mma.sync" throughout."""
+    """engine: "tcgen05" (forward, data and weight gradients on the
+    5th-generation tensor cores) or "mma.sync" throughout."""
     import torch
 
     dev = torch.device("cuda", 0)

@@ -339,9 +339,9 @@ int dsgpu_cnn_set_loss(dsgpu_ctx* ctx, dsgpu_cnn* net, int relative);
 int dsgpu_cnn_infer(dsgpu_ctx* ctx, dsgpu_cnn* net, const float* in_rgb, int w, int h, float strength,
                     float* out_rgb, unsigned flags);
 /* Engine: 1 (default) the tcgen05 tensor cores with TMEM accumulators for
- * inference and for training's forward pass and data gradients (the batch
- * laid out as one frame of crops with zero rows between them; the weight
- * gradients stay on mma.sync); 0 the warp-level mma.sync kernels
+ * inference and for all of training's convolutions: forward pass, data
+ * gradients, weight and bias gradients (the batch laid out as one frame of
+ * crops with zero rows between them); 0 the warp-level mma.sync kernels
  * throughout. A bounded device wait that gives up makes the call return
  * DSGPU_ERR_TIMEOUT. */
 int dsgpu_cnn_set_engine(dsgpu_ctx* ctx, dsgpu_cnn* net, int tensor_core_gen5);
