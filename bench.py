@@ -298,6 +298,37 @@ def psnr(a, b) -> float:
     return 10.0 * float(np.log10(1.0 / max(mse, 1e-30)))
 
 
+def time_training(ctx, stream, rgb, tgt, steps: int = 20, warmup: int = 5) -> dict:
+    """One Adam step of the learned path's network (forward, loss, data,
+    weight and bias gradients, Adam: dsgpu_cnn_train_step) on the training
+    batch, 32 crops of 128 x 128 of rgb with target tgt, on the tcgen05
+    engine; CUDA events on the launching stream."""
+    import torch
+
+    from darkslide_b200 import cnn
+
+    B, crop = 32, 128
+    h, w = rgb.shape[:2]
+    pos = np.random.default_rng(5).integers(0, [h - crop + 1, w - crop + 1], (B, 2))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        xb = torch.stack([rgb[y:y + crop, x:x + crop] for y, x in pos]).contiguous()
+        tb = torch.stack([tgt[y:y + crop, x:x + crop] for y, x in pos]).contiguous()
+        net = cnn.ResidualCNN(ctx, max_batch=B, crop=crop, seed=1)
+        for _ in range(warmup):
+            net.train_step(xb, 0.5, tb, 1e-4, want_loss=False)
+        e0.record(stream)
+        for _ in range(steps):
+            net.train_step(xb, 0.5, tb, 1e-4, want_loss=False)
+        e1.record(stream)
+    e1.synchronize()
+    net.close()
+    ms = e0.elapsed_time(e1) / steps
+    return {"engine": "tcgen05", "batch": f"{B} crops of {crop}x{crop}", "ms_per_step": ms,
+            "mpix_per_s": B * crop * crop / ms / 1e3, "steps": steps,
+            "what": "forward, loss, data, weight and bias gradients, Adam (dsgpu_cnn_train_step)"}
+
+
 BATCH_SIZES = [(4000, 3000), (6000, 4000), (8256, 5504), (9504, 6336)]
 BATCH_FRAMES = 64
 
@@ -530,6 +561,8 @@ def run_ours(args):
         ctx.check(L.dsgpu_cnn_denoise(ctx.handle, net.handle, vp(rgb.data_ptr()), W, H, float(hp), SEARCH, PATCH,
                                       float(TAU), vp(out.data_ptr()), ctypes.byref(nf), 0), "dsgpu_cnn_denoise")
     stream.synchronize()
+    training = time_training(ctx, stream, rgb, out)  # target: the learned output of the same frame
+    ctx.set_stream(stream.cuda_stream)
     p_plain, p_learned, p_noisy = psnr(q_plain, truth), psnr(q_learned, truth), psnr(q_noisy, truth)
     loss_db = p_plain - p_learned
     meets = loss_db <= QUALITY_BOUND_DB
@@ -627,7 +660,7 @@ def run_ours(args):
                       "ms_per_step": learned_judged["ms_per_step"],
                       "cost_ms_per_step": learned_judged["ms_per_step"] - learned["ms_per_step"], **judge},
             "roofline": roof_conv, "weights": "darkslide_b200/weights/cnn_nlm.bin", "dtype": "bf16 (fp32 accumulate)",
-            "clocks": learned["clocks"],
+            "clocks": learned["clocks"], "training_step": training,
         }
         plain_info = {
             "value": plain["value"], "ms_per_step": plain["ms_per_step"], "e2e": plain_e2e,
