@@ -295,33 +295,33 @@ __global__ void __launch_bounds__(CNN_THREADS) bias_grad_kernel(const bf16* __re
   }
 }
 
-// sum of p[k * stride], k < n, in eight interleaved partial sums (eight
-// loads in flight per thread) added in a fixed order
-__device__ __forceinline__ float sum_strided(const float* __restrict__ p, size_t stride, int n) {
-  float a[8];
-#pragma unroll
-  for (int j = 0; j < 8; j++) a[j] = 0.f;
-  int k = 0;
-  for (; k + 8 <= n; k += 8) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) a[j] += p[(size_t)(k + j) * stride];
-  }
-  for (; k < n; k++) a[0] += p[(size_t)k * stride];
-  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-}
-
-// grads[layer] (real shape [9][cout][cin] then [cout]) from the partials
-__global__ void reduce_grads_kernel(const float* __restrict__ wpart, int nw, int coutw, int cinp,
-                                    const float* __restrict__ bpart, int nb, int cb, int cout, int cin,
-                                    float* __restrict__ gw) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// grads[layer] (real shape [9][cout][cin] then [cout]) from the per-CTA
+// partials: a CTA takes RG_X consecutive parameters; thread row y sums the
+// partials y, y + RG_Y, ... (its loads coalesced across the parameters), and
+// the RG_Y row sums are added in a fixed order, so the result is
+// deterministic.
+constexpr int RG_X = 128, RG_Y = 8;
+__global__ void __launch_bounds__(RG_X * RG_Y) reduce_grads_kernel(const float* __restrict__ wpart, int nw, int coutw,
+                                                                    int cinp, const float* __restrict__ bpart, int nb,
+                                                                    int cb, int cout, int cin, float* __restrict__ gw) {
+  __shared__ float red[RG_Y][RG_X];
+  const int i = blockIdx.x * RG_X + threadIdx.x;
   const int nwreal = 9 * cout * cin;
+  float acc = 0.f;
   if (i < nwreal) {
     const int tap = i / (cout * cin), r = i - tap * cout * cin, co = r / cin, ci = r - co * cin;
     const size_t off = ((size_t)tap * coutw + co) * cinp + ci, stride = (size_t)9 * coutw * cinp;
-    gw[i] = sum_strided(wpart + off, stride, nw);
+    for (int k = threadIdx.y; k < nw; k += RG_Y) acc += wpart[off + (size_t)k * stride];
   } else if (i < nwreal + cout) {
-    gw[i] = sum_strided(bpart + (i - nwreal), (size_t)cb, nb);
+    for (int k = threadIdx.y; k < nb; k += RG_Y) acc += bpart[(i - nwreal) + (size_t)k * cb];
+  }
+  red[threadIdx.y][threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.y == 0 && i < nwreal + cout) {
+    float sum = 0.f;
+#pragma unroll
+    for (int y = 0; y < RG_Y; y++) sum += red[y][threadIdx.x];
+    gw[i] = sum;
   }
 }
 
@@ -965,8 +965,8 @@ cudaError_t ds_cnn_gradients(DsCnn* net, cudaStream_t st, const float* rgb, cons
   auto reduce = [&](int l, int coutw, int cinp, int cb, int nw, int nb) {
     const LayerSpec L = LAYERS[l];
     const int nreal = 9 * L.cout * L.cin + L.cout;
-    reduce_grads_kernel<<<(nreal + 255) / 256, 256, 0, st>>>(net->wpart, nw, coutw, cinp, net->bpart, nb, cb, L.cout,
-                                                            L.cin, net->grads + net->off[l]);
+    reduce_grads_kernel<<<(nreal + RG_X - 1) / RG_X, dim3(RG_X, RG_Y), 0, st>>>(
+        net->wpart, nw, coutw, cinp, net->bpart, nb, cb, L.cout, L.cin, net->grads + net->off[l]);
   };
   if (tc) {
     // per layer, top down: weight and bias gradients of layer l from (tact[l], its output

@@ -1,6 +1,8 @@
-// Inference convolutions of the learned path on the 5th-generation tensor
-// cores (tcgen05). Same network and tensors as k_cnn.cu (NHWC bf16
-// activations, [9][cout][cin] bf16 weights); the difference is the engine.
+// The learned path's convolutions on the 5th-generation tensor cores
+// (tcgen05): inference, and training's forward pass, data gradients
+// (conv_tc_kernel) and weight and bias gradients (wgrad_tc_kernel, at the end
+// of the file). Same network and weights as k_cnn.cu ([9][cout][cin] bf16);
+// the difference is the engine and the activation layout.
 //
 // Layout. Activations live in HBM channel-block-major, [C/8][H][Wp][8] bf16
 // (16 bytes per pixel and block; Wp = W rounded up to 4, padding columns
@@ -556,13 +558,20 @@ __device__ __forceinline__ void mma_bf16_pred(unsigned tmem_d, unsigned long lon
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
-// x: [CIN/8][Hp][Wp][8] through xmap, dy: [COUTW/8][Hp][Wp][8] through dmap
-// (boxes of 8 channels x TK pixels x 1 row x every block); H: frame rows;
-// wpart: [grid][9][COUTW][CIN], bpart: [grid][COUTW] (one partial sum per CTA).
+// x: [CIN/8][Hp][Wp][8], dy: [COUTW/8][Hp][Wp][8]. The loads that start at a
+// chunk's first pixel (every dY copy, the unshifted X copy) go through xmap4 /
+// dmap4, which see a block row as 64-byte groups of 4 pixels (boxes of 4
+// pixels x 8 channels x TK / 4 groups x 1 row x every block); the two
+// column-shifted X copies, which start at any pixel, through xmap (16-byte box
+// rows of one pixel; such a row moves a 32-byte sector, so these are the only
+// loads that fetch twice their bytes). Both forms land in shared memory as
+// [block][pixel][8]. H: frame rows; wpart: [grid][9][COUTW][CIN], bpart:
+// [grid][COUTW] (one partial sum per CTA).
 template <int CIN, int COUTW>
 __global__ void __launch_bounds__(WG_THREADS, 1)
-    wgrad_tc_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dmap, int H,
-                    int Wp, int dil, float* __restrict__ wpart, float* __restrict__ bpart, int* __restrict__ err) {
+    wgrad_tc_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap xmap4,
+                    const __grid_constant__ CUtensorMap dmap4, int H, int Wp, int dil, float* __restrict__ wpart,
+                    float* __restrict__ bpart, int* __restrict__ err) {
   typedef WgShape<CIN, COUTW> S;
   extern __shared__ __align__(128) unsigned char sm[];
   // bars: full[STAGES], empty[STAGES], done, drain
@@ -617,7 +626,8 @@ __global__ void __launch_bounds__(WG_THREADS, 1)
     // ---------------- TMA producer
     if (lane == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&xmap)) : "memory");
-      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&dmap)) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&xmap4)) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&dmap4)) : "memory");
       int c = 0;
       for (; c < nch; c++) {
         const int s = c % S::STAGES;
@@ -625,10 +635,14 @@ __global__ void __launch_bounds__(WG_THREADS, 1)
         mbar_expect_tx(full(s), S::TX);
         const int g = c0 + c, q = g / cpr, x0 = (g - q * cpr) * S::TK;
         const unsigned a = smem_u32(a_of(s)), b = smem_u32(b_of(s));
+        // x0 is a multiple of TK, so the unshifted loads start on a 4-pixel group
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-          tma_load_4d(a + (unsigned)(k * S::CBO * S::GB), &dmap, x0, q - (k - 1) * dil, full(s));  // ky = k
-          tma_load_4d(b + (unsigned)(k * S::CBI * S::GB), &xmap, x0 + (k - 1) * dil, q, full(s));  // kx = k
+          tma_load_4d(a + (unsigned)(k * S::CBO * S::GB), &dmap4, x0 / TC_PG, q - (k - 1) * dil, full(s));  // ky = k
+          if (k == 1)
+            tma_load_4d(b + (unsigned)(S::CBI * S::GB), &xmap4, x0 / TC_PG, q, full(s));  // kx = 1
+          else
+            tma_load_4d(b + (unsigned)(k * S::CBI * S::GB), &xmap, x0 + (k - 1) * dil, q, full(s));  // kx = 0, 2
         }
       }
       // loads issued but maybe never consumed (abort only): wait for them to land
@@ -783,17 +797,20 @@ cudaError_t launch_wgrad_tc(cudaStream_t st, int dil, const bf16* x, const bf16*
       max_grid < 1)
     return cudaErrorInvalidValue;
   const int Wp = (W + TC_PG - 1) / TC_PG * TC_PG, Hp = (H + 11) / 12 * 12;
-  auto make = [&](CUtensorMap* m, const bf16* p, int blocks) {
-    const cuuint64_t dims[4] = {8, (cuuint64_t)Wp, (cuuint64_t)Hp, (cuuint64_t)blocks};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)Wp * 16, (cuuint64_t)Wp * Hp * 16};
-    const cuuint32_t box[4] = {8, (cuuint32_t)S::TK, 1, (cuuint32_t)blocks};
+  static_assert(S::TK % TC_PG == 0, "chunks start on a 4-pixel group");
+  // px: pixels per innermost element group (1: any start pixel; TC_PG: 64-byte rows)
+  auto make = [&](CUtensorMap* m, const bf16* p, int blocks, int px) {
+    const cuuint64_t dims[4] = {(cuuint64_t)(8 * px), (cuuint64_t)(Wp / px), (cuuint64_t)Hp, (cuuint64_t)blocks};
+    const cuuint64_t strides[3] = {(cuuint64_t)(16 * px), (cuuint64_t)Wp * 16, (cuuint64_t)Wp * Hp * 16};
+    const cuuint32_t box[4] = {(cuuint32_t)(8 * px), (cuuint32_t)(S::TK / px), 1, (cuuint32_t)blocks};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(p), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   };
-  CUtensorMap xmap, dmap;
-  if (!make(&xmap, x, S::CBI) || !make(&dmap, dy, S::CBO)) return cudaErrorInvalidValue;
+  CUtensorMap xmap, xmap4, dmap4;
+  if (!make(&xmap, x, S::CBI, 1) || !make(&xmap4, x, S::CBI, TC_PG) || !make(&dmap4, dy, S::CBO, TC_PG))
+    return cudaErrorInvalidValue;
   cudaError_t e =
       cudaFuncSetAttribute(wgrad_tc_kernel<CIN, COUTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -803,7 +820,7 @@ cudaError_t launch_wgrad_tc(cudaStream_t st, int dil, const bf16* x, const bf16*
   const long long chunks = (long long)H * ((Wp + S::TK - 1) / S::TK);
   int grid = sms < max_grid ? sms : max_grid;
   if (chunks < grid) grid = (int)chunks;
-  wgrad_tc_kernel<CIN, COUTW><<<grid, WG_THREADS, smem, st>>>(xmap, dmap, H, Wp, dil, wpart, bpart, err);
+  wgrad_tc_kernel<CIN, COUTW><<<grid, WG_THREADS, smem, st>>>(xmap, xmap4, dmap4, H, Wp, dil, wpart, bpart, err);
   *grid_out = grid;
   return cudaGetLastError();
 }
