@@ -190,6 +190,32 @@ def test_tensor_core_training_matches_mma_sync(torch_dev):
             assert cos >= 0.995, (i, sl, cos)
 
 
+@pytest.mark.parametrize("crop", [72, 128])
+def test_tensor_core_gradients_at_wide_crops(torch_dev, crop):
+    """Crops wider than the weight-gradient kernel's 64-pixel chunk: a frame
+    row then holds two chunks (the second one ragged at 72, whole at the
+    training crop 128), loaded at a non-zero start pixel. Both engines agree
+    on the loss and every layer's weight and bias gradients up to BF16
+    rounding of the activations."""
+    from darkslide_b200 import cnn
+
+    torch, dev = torch_dev
+    p = cnn.init_params(21)
+    p[-1299:] = np.random.default_rng(21).normal(0, 0.05, 1299)
+    net = cnn.ResidualCNN(max_batch=2, crop=crop, params=p)
+    rgb, tgt, trgb, ttgt = _batch(torch, dev, 2, crop, 22)
+    g_tc, l_tc = net.gradients(trgb, 0.4, ttgt)
+    net.set_engine(False)
+    g_ms, l_ms = net.gradients(trgb, 0.4, ttgt)
+    g_tc, g_ms = g_tc.cpu().numpy(), g_ms.cpu().numpy()
+    assert abs(l_tc - l_ms) <= 1e-2 * l_ms
+    for i, (ws, bs, _) in enumerate(cnn.layer_slices()):
+        for sl in (ws, bs):
+            a, b = g_tc[sl], g_ms[sl]
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30))
+            assert cos >= 0.995, (crop, i, sl, cos)
+
+
 def test_training_reduces_loss(torch_dev):
     from darkslide_b200 import cnn
 
