@@ -22,7 +22,7 @@ WB = np.array([2.0, 1.0, 1.0 / 0.7], np.float32)
 LEVELS = [(2.0, 0.25), (6.0, 0.5), (12.0, 1.0)]
 # the NLM bound against the f32 oracle over the whole frame: about ten times
 # the measured maximum (1.6e-6 to 1.7e-6 at the three levels), so that a
-# regression shows; the north-star bound against the reference is 1e-3
+# regression shows; the path's bound against the reference is 1e-3
 NLM_TOL_FULL = 2e-5
 
 
