@@ -187,7 +187,8 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
       // (pair plane j * 2 + i0), saturated to the largest finite half
       if (aj < BJ) {
         const T* qrow = PL + (aprow + dy0 + aj) * PP + dx0;
-        float q[DW + BI - 1];
+        float q[DW + BI - 1];  // the shifted row in registers (interior tiles only)
+        (void)q;
         if constexpr (XIN) {
 #pragma unroll
           for (int m = 0; m < DW + BI - 1; m++) q[m] = ldp(&qrow[acol0 + m]);
@@ -233,7 +234,8 @@ __device__ __forceinline__ void nlm_tile_body(const float* __restrict__ in, int 
     } else {
     if (aj < BJ) {
       const T* qrow = PL + (aprow + dy0 + aj) * PP + dx0;
-      float q[DW + BI - 1];
+      float q[DW + BI - 1];  // the shifted row in registers (interior tiles only)
+      (void)q;
       if constexpr (XIN) {
 #pragma unroll
         for (int m = 0; m < DW + BI - 1; m++) q[m] = ldp(&qrow[acol0 + m]);
