@@ -17,7 +17,9 @@ demosaiced, 288 MB output, 2.3 GB of CNN activations) is larger than the
 The line also carries "batched": 64 mosaics of four camera sizes, four CFA
 layouts and two bit depths through dsgpu_rcd_nlm_batch (one CUDA graph launch
 per batch), after the tile autotuner, with aggregate Mpix/s and per-frame
-p50/p99 completion times (--no-batched skips it).
+p50/p99 completion times (--no-batched skips it), and "learned.training_step":
+one Adam step of the network on its training batch (32 crops of 128 x 128)
+on the tcgen05 engine, timed with CUDA events.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
